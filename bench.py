@@ -1,0 +1,406 @@
+#!/usr/bin/env python
+"""Signature-kernel throughput benchmark on B200.
+
+Default workload (the headline configuration): SigPDE.gram(x, y) with the
+linear static kernel, X and Y each 256 Brownian paths of length 128 in 8
+dimensions, dyadic order 2, float32 inputs, float64 PDE cells (the default,
+"accurate" precision).  One step = one full 256x256 Gram = 65,536 entries =
+1.69e10 refined-grid cell updates.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|fp32]
+    python bench.py --impl reference ...   # the float64 CPU oracle (C/OpenMP) on the host cores
+
+Multi-GPU (one process per GPU, launched by torchrun): every rank solves its
+own Gram (weak scaling, replicas: the entries are independent and no data
+crosses GPUs); `value` = all ranks' entries / the slowest rank's time.
+Prints ONE JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # SigPDE.gram(x, y), LinearKernel, X,Y 256 Brownian paths, L=128, d=8, dyadic order 2
+    "gram256": dict(nx=256, ny=256, L=128, d=8, order=2, seed_x=2001, seed_y=2002),
+}
+
+L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="gram256", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target length of the CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------- workload
+def workload_units(w):
+    n = (w["L"] - 1) << w["order"]
+    entries = w["nx"] * w["ny"]
+    cells = entries * n * n
+    coarse = entries * (w["L"] - 1) ** 2
+    # algorithmic FLOPs: 4 per refined cell ((a+b)*A - c*B), 2d + 8 per coarse cell
+    # (the increment dot product and the stencil coefficients)
+    flops = 4 * cells + (2 * w["d"] + 8) * coarse
+    return entries, cells, flops
+
+
+def make_inputs(w, device=None, dtype=None):
+    from sigpde_b200 import synthetic
+    x = synthetic.brownian(w["nx"], w["L"], w["d"], w["seed_x"], dtype=dtype, device=device)
+    y = synthetic.brownian(w["ny"], w["L"], w["d"], w["seed_y"], dtype=dtype, device=device)
+    return x, y
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu_index = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu_index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+
+        def num(v):
+            try:
+                return float(v)
+            except ValueError:
+                return None
+
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        mx = [num(r[2]) for r in rows if num(r[2]) is not None]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for name, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# ----------------------------------------------------------------------------- timing
+def device_peak_tflops(torch, dtype, n=4096, reps=5):
+    """Measured dense GEMM rate for `dtype` (cuBLAS through torch.matmul); the
+    float64 figure is the denominator of the float64 wavefront's roofline."""
+    a = torch.randn(n, n, dtype=dtype, device="cuda")
+    b = torch.randn(n, n, dtype=dtype, device="cuda")
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        for _ in range(2):
+            torch.matmul(a, b)
+        torch.cuda.synchronize()
+        best = math.inf
+        for _ in range(reps):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            torch.matmul(a, b)
+            e.record()
+            e.synchronize()
+            best = min(best, s.elapsed_time(e))
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+    del a, b
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def timed_steps(torch, step, K, W, flush_buf, barrier):
+    for _ in range(W):
+        step()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    evs = []
+    for _ in range(K):
+        flush_buf.zero_()  # L2 flush between timed steps (outside the events)
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        step()
+        e.record(stream)
+        evs.append((s, e))
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    return [s.elapsed_time(e) for s, e in evs]
+
+
+def percentile(v, q):
+    v = sorted(v)
+    if not v:
+        return None
+    k = (len(v) - 1) * q
+    f, c = math.floor(k), math.ceil(k)
+    return v[f] + (v[c] - v[f]) * (k - f)
+
+
+def read_traffic(kernel_key):
+    """Per-launch DRAM bytes from the committed ncu summary (profiles/traffic.txt)."""
+    p = os.path.join(ROOT, "profiles", "traffic.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        line = line.strip()
+        if line.startswith(kernel_key + "="):
+            try:
+                return float(line.split("=", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# ----------------------------------------------------------------------------- CPU legs
+def cpu_oracle_rate(w, target_s, seed=7, max_entries=None):
+    """Float64 oracle (C, OpenMP over entries, all host threads) on a sample of
+    the Gram's entries; returns (entries/s, cores, sample description)."""
+    import numpy as np
+
+    from oracle import oracle
+    from sigpde_b200 import synthetic
+    oracle.build()
+    x = synthetic.brownian_np(w["nx"], w["L"], w["d"], w["seed_x"]).astype(np.float32).astype(np.float64)
+    y = synthetic.brownian_np(w["ny"], w["L"], w["d"], w["seed_y"]).astype(np.float32).astype(np.float64)
+    rng = np.random.default_rng(seed)
+    cores = oracle.num_threads()
+    n = max(cores, 8)
+    while True:
+        flat = rng.choice(w["nx"] * w["ny"], n, replace=False)
+        t0 = time.perf_counter()
+        oracle.gram(x, y, w["order"], pairs=flat)
+        dt = time.perf_counter() - t0
+        if dt >= target_s or n >= w["nx"] * w["ny"] or (max_entries and n >= max_entries):
+            break
+        n = min(w["nx"] * w["ny"], max(n * 2, int(n * target_s / max(dt, 1e-3) * 1.1)))
+        if max_entries:
+            n = min(n, max_entries)
+    return n / dt, cores, f"{n} random entries of the {w['nx']}x{w['ny']} Gram in {dt:.1f} s"
+
+
+def run_reference(args, w, rank):
+    if rank != 0:
+        return
+    entries, cells, _ = workload_units(w)
+    per_step = []
+    cores = None
+    sample = None
+    step_s = max(1.0, args.cpu_seconds / 2)
+    for i in range(args.warmup + args.steps):
+        rate, cores, sample = cpu_oracle_rate(w, step_s, seed=100 + i)
+        if i >= args.warmup:
+            per_step.append(rate)
+    value = statistics.mean(per_step)
+    line = {
+        "impl": "reference",
+        "metric": "gram_entries_per_s",
+        "value": value,
+        "unit": "entries/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": entries / value * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic Brownian paths (seeded), float32 inputs upcast to float64",
+        "config": {"workload": "SigPDE.gram 256x256, L=128, d=8, dyadic_order=2, LinearKernel", "global_batch":
+                   entries, "seq_len": w["L"], "parallelism": "cpu", "l2": "n/a (CPU)"},
+        "cells_per_s": value * cells / entries,
+        "cpu_baseline": {"value": value, "unit": "entries/s", "cores": cores, "kind": "port",
+                         "sample": f"per step: {sample}; float64 C restatement of the reference solver"},
+        "e2e": {"value": value, "unit": "entries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- our arm
+def run_ours(args, w):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    import sigpde_b200.torch as sig
+    from sigpde_b200 import _lib
+
+    entries, cells, flops = workload_units(w)
+    X, Y = make_inputs(w, device=dev)
+    k = sig.SigPDE(sig.kernels.LinearKernel(), w["order"], precision=args.precision)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+
+    out = k.gram(X, Y)  # also loads libsigk.so
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    times = timed_steps(torch, lambda: k.gram(X, Y), args.steps, args.warmup, flush, barrier)
+    clk = clocks.stop()
+    total_ms = sum(times)
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * entries * args.steps / (total_ms * 1e-3)
+
+    # end to end through the public API: pinned host paths -> device -> Gram -> pinned host result
+    Xh = X.cpu().pin_memory()
+    Yh = Y.cpu().pin_memory()
+    Rh = torch.empty((w["nx"], w["ny"]), dtype=X.dtype).pin_memory()
+
+    def e2e_step():
+        Xd = Xh.to(dev, non_blocking=True)
+        Yd = Yh.to(dev, non_blocking=True)
+        Rh.copy_(k.gram(Xd, Yd), non_blocking=True)
+
+    e2e_times = timed_steps(torch, e2e_step, args.steps, args.warmup, flush, barrier)
+    e2e_ms = sum(e2e_times)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * entries * args.steps / (e2e_ms * 1e-3)
+
+    line = None
+    if rank == 0:
+        ms = statistics.mean(times)
+        fp64 = args.precision == "fp64"
+        peak = device_peak_tflops(torch, torch.float64 if fp64 else torch.float32)
+        achieved = flops / (ms * 1e-3) / 1e12
+        traffic = read_traffic(f"gram256_{args.precision}")
+        # accuracy of this run on a sample of entries against the float64 oracle
+        acc = None
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            from oracle import oracle
+            G = out.double().cpu().numpy()
+            rng = np.random.default_rng(1)
+            flat = rng.choice(entries, 64, replace=False)
+            xin, yin = X.double().cpu().numpy(), Y.double().cpu().numpy()
+            want = oracle.gram(xin, yin, w["order"], pairs=flat)
+            got = G.reshape(-1)[flat]
+            kxx = oracle.pairwise(xin[flat // w["ny"]], None, w["order"])
+            kyy = oracle.pairwise(yin[flat % w["ny"]], None, w["order"])
+            acc = {"max_rel_err": float(np.max(np.abs(got - want) / np.abs(want))),
+                   "max_cs_err": float(np.max(np.abs(got - want) / np.sqrt(kxx * kyy))),
+                   "sample": "64 random entries vs the float64 oracle"}
+            rate, cores, sample = cpu_oracle_rate(w, args.cpu_seconds)
+            cpu = {"value": rate, "unit": "entries/s", "cores": cores, "kind": "port",
+                   "sample": f"{sample}; float64 C restatement of the reference solver (OpenMP)"}
+        line = {
+            "metric": "gram_entries_per_s",
+            "value": value,
+            "unit": "entries/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms,
+            "p50_ms": percentile(times, 0.5),
+            "p99_ms": percentile(times, 0.99),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64" if fp64 else "f32",
+            "data": "synthetic Brownian paths (seeded PCG64), float32",
+            "config": {"workload": "SigPDE.gram 256x256, L=128, d=8, dyadic_order=2, LinearKernel",
+                       "global_batch": entries * world, "seq_len": w["L"], "parallelism": f"replicas x{world}",
+                       "precision": args.precision, "l2": "flushed between timed steps (256 MB write)"},
+            "cells_per_s": value * cells / entries,
+            "accuracy": acc,
+            "roofline": {"bound": "fp64" if fp64 else "fp32", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": ("measured cuBLAS " + ("DGEMM" if fp64 else "SGEMM (no TF32)") +
+                                         " 4096^3 on this device (the wavefront is bound by the "
+                                         + ("FP64" if fp64 else "FP32") + " pipe, not HBM or tensor cores)"),
+                         "algorithmic_flops_per_launch": flops},
+            "e2e": {"value": e2e_value, "unit": "entries/s", "h2d_bytes_per_step": X.numel() * X.element_size()
+                    + Y.numel() * Y.element_size(), "d2h_bytes_per_step": Rh.numel() * Rh.element_size(),
+                    "ms_per_step": statistics.mean(e2e_times)},
+            "gpu_launches": args.steps,
+            "clocks": clk,
+            "lib": _lib.version(),
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+    if world > 1:
+        barrier()
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        run_reference(args, w, int(os.environ.get("RANK", "0")))
+        return
+    run_ours(args, w)
+
+
+if __name__ == "__main__":
+    main()

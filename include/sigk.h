@@ -1,0 +1,194 @@
+/*
+ * sigk.h -- C ABI of libsigk.so, the B200 (sm_100a) signature-kernel engine.
+ *
+ * The library solves the Goursat PDE of the untruncated signature kernel
+ * (Salvi et al. 2021) on a dyadically refined grid, and the per-path
+ * Chandrupatla root-find of the robust (tensor-normalised) signature kernel
+ * (Chevyrev & Oberhauser 2022).  It is the native back end of the
+ * `sigpde_b200.torch` package, which keeps stojl/SigPDE's `sigpde.torch` API.
+ *
+ * Conventions shared by every entry point
+ *   - Pointers are DEVICE pointers unless a name says otherwise.  Paths are
+ *     C-contiguous (count, length, dim) arrays of `dtype`; outputs are written
+ *     in `dtype` too (the reference returns results in the dtype of x).
+ *   - Nothing is allocated.  Scratch, when an entry point needs it, comes from
+ *     the caller through (workspace, workspace_bytes); sigk_workspace_size()
+ *     returns the byte count.  A NULL workspace with workspace_bytes == 0 is
+ *     valid whenever the size query returns 0.
+ *   - Work is enqueued asynchronously on `stream` (a cudaStream_t; 0 is the
+ *     legacy default stream).  No entry point synchronises the device.
+ *   - Every entry point returns a sigk_status; sigk_last_error_string() holds
+ *     a description of the last failure on the calling host thread.
+ *   - Entry points are re-entrant and thread-safe; concurrent calls on
+ *     different streams with disjoint outputs and workspaces do not interact.
+ *
+ * Precision modes (sigk_precision)
+ *   SIGK_PREC_FP64  increments <dx_i,dy_j> and PDE cells in float64 (default;
+ *                   no worse than the reference's GPU path, which does float64
+ *                   arithmetic with float32 storage, and far better).
+ *   SIGK_PREC_FP32  increments and cells in float32 (fastest; its error grows
+ *                   with |K| along the grid and is reported by the tests).
+ */
+#ifndef SIGK_H_
+#define SIGK_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(SIGK_BUILD) && defined(__GNUC__)
+#define SIGK_API __attribute__((visibility("default")))
+#else
+#define SIGK_API
+#endif
+
+typedef void *sigk_stream_t; /* cudaStream_t */
+
+typedef enum {
+    SIGK_OK = 0,
+    SIGK_EINVAL = 1,      /* bad argument (shape, dtype, pointer, size)            */
+    SIGK_ENOMEM = 2,      /* workspace too small                                   */
+    SIGK_ETIMEDOUT = 3,   /* a bounded device wait gave up                         */
+    SIGK_ELAUNCH = 4,     /* CUDA launch or runtime error                          */
+    SIGK_EUNSUPPORTED = 5 /* valid request that this build does not implement      */
+} sigk_status;
+
+typedef enum { SIGK_F32 = 0, SIGK_F64 = 1 } sigk_dtype;
+
+typedef enum { SIGK_PREC_FP64 = 0, SIGK_PREC_FP32 = 1 } sigk_precision;
+
+typedef enum {
+    SIGK_OP_PAIRWISE = 0,     /* out[b]    = k(x_b, y_b)                                */
+    SIGK_OP_GRAM = 1,         /* out[i][j] = k(x_i, y_j)                                */
+    SIGK_OP_GRAM_SYM = 2,     /* out[i][j] = k(x_i, x_j), lower triangle solved, mirrored */
+    SIGK_OP_NORMALIZE = 3     /* robust lambda per path                                 */
+} sigk_op;
+
+/* Library version string, e.g. "sigk 0.1.0 sm_100a". */
+SIGK_API const char *sigk_version(void);
+
+/* Description of the last error on this host thread ("" if none). */
+SIGK_API const char *sigk_last_error_string(void);
+
+/*
+ * Bytes of caller-provided scratch an entry point needs for the given shape.
+ * `op` is a sigk_op; len_x / len_y are path lengths before refinement; for
+ * SIGK_OP_PAIRWISE n_x is the batch, for the Gram ops n_x / n_y are the path
+ * counts.  Pass dim = 0 for the *_inc entry points (len_x / len_y are then
+ * nc_x + 1 / nc_y + 1).  Returns 0 when no scratch is needed.  The size
+ * depends on the current device's SM count.
+ */
+SIGK_API size_t sigk_workspace_size(int op, int64_t n_x, int64_t n_y, int64_t len_x, int64_t len_y, int64_t dim,
+                           int order, int dtype, int precision);
+
+/*
+ * Pairwise signature kernel with the linear static kernel.
+ * Replaces SigPDE.pairwise's increment build + PairwisePDESolver.solve /
+ * solve_scaled (sigpde/torch/kernel.py:31-65, sigpde/torch/kernel.py:13-16,
+ * sigpde/PDESolvers.py:56-84, sigpde/cuda_pairwise_kernels.py:8-97).
+ *   x: (batch, len_x, dim), y: (batch, len_y, dim); out: (batch,)
+ *   static_scale: LinearKernel(scale) factor (sigpde/torch/static_kernels.py:4-8)
+ *   scale_x / scale_y: (batch,) per-pair path scales or NULL (NULL = 1)
+ */
+SIGK_API int sigk_pairwise(const void *x, const void *y, int64_t batch, int64_t len_x, int64_t len_y, int64_t dim,
+                  int dtype, int order, double static_scale, const void *scale_x, const void *scale_y, void *out,
+                  int precision, void *workspace, size_t workspace_bytes, sigk_stream_t stream);
+
+/*
+ * Gram matrix with the linear static kernel.
+ * Replaces SigPDE._gram's tile loop, gram_inner_product and
+ * GramPDESolver.solve / solve_scaled (sigpde/torch/kernel.py:75-126,
+ * sigpde/torch/kernel.py:18-21, sigpde/PDESolvers.py:160-190,
+ * sigpde/cuda_gram_kernels.py:8-76).
+ *   x: (n_x, len_x, dim), y: (n_y, len_y, dim); out: (n_x, n_y) row-major
+ *   scale_x: (n_x,) or NULL, scale_y: (n_y,) or NULL
+ */
+SIGK_API int sigk_gram(const void *x, const void *y, int64_t n_x, int64_t n_y, int64_t len_x, int64_t len_y, int64_t dim,
+              int dtype, int order, double static_scale, const void *scale_x, const void *scale_y, void *out,
+              int precision, void *workspace, size_t workspace_bytes, sigk_stream_t stream);
+
+/*
+ * Symmetric Gram matrix k(x_i, x_j): only the lower triangle i >= j is solved
+ * and each entry is written to [i][j] and [j][i].
+ * Replaces SigPDE._gram_sym + SymmetricGramPDESolver.solve / solve_scaled
+ * (sigpde/torch/kernel.py:128-171, sigpde/PDESolvers.py:192-245,
+ * sigpde/cuda_gram_kernels.py:79-164).
+ *   x: (n, len, dim); scale: (n,) or NULL; out: (n, n)
+ */
+SIGK_API int sigk_gram_sym(const void *x, int64_t n, int64_t len, int64_t dim, int dtype, int order, double static_scale,
+                  const void *scale, void *out, int precision, void *workspace, size_t workspace_bytes,
+                  sigk_stream_t stream);
+
+/*
+ * Self norms k(x_b, x_b) in float64, NaN mapped to +inf.
+ * First half of RobustSigPDE._norm_factors (sigpde/torch/kernel.py:181-183);
+ * used when the normaliser is a user callable that the host applies.
+ *   x: (n, len, dim); knorm: (n,) float64
+ */
+SIGK_API int sigk_self_norms(const void *x, int64_t n, int64_t len, int64_t dim, int dtype, int order, double static_scale,
+                    double *knorm, void *workspace, size_t workspace_bytes, sigk_stream_t stream);
+
+/*
+ * Robust normalisation lambda per path: the Chandrupatla root-find of
+ * g(l) = k(l x, l x) - f(k(x,x)) on [0,1], every iteration re-solving the PDE
+ * on-chip with float64 cells and float64 bracket arithmetic, then lambda = 0
+ * where k(x,x) < 1.
+ * Replaces RobustSigPDE._norm_factors + PairwisePDESolver.solve_norms
+ * (sigpde/torch/kernel.py:180-195, sigpde/PDESolvers.py:86-101,
+ * sigpde/cuda_pairwise_kernels.py:100-178).
+ *   fnorm == NULL: the default normaliser f(s) = 2 - 1/(1 + log s)
+ *                  (sigpde/torch/kernel.py:23-24) is applied on the device and
+ *                  knorm receives k(x,x) (if knorm != NULL).
+ *   fnorm != NULL: knorm (input, float64, from sigk_self_norms) and fnorm
+ *                  (input, float64, f(knorm) computed by the caller) are used.
+ *   lam: (n,) in dtype.  iters (int32, may be NULL) receives iteration counts.
+ */
+SIGK_API int sigk_normalize(const void *x, int64_t n, int64_t len, int64_t dim, int dtype, int order, double static_scale,
+                   double *knorm, const double *fnorm, double tol, int maxit, void *lam, int *iters,
+                   void *workspace, size_t workspace_bytes, sigk_stream_t stream);
+
+/*
+ * Generic-increment entry points, for static kernels other than the linear
+ * one (RBF, L1-RBF, any duck-typed kernel).  The caller computes the coarse
+ * increments (the 4-term second difference of the static Gram divided by
+ * 4^order, sigpde/torch/kernel.py:13-21) and the library solves the PDE.
+ *
+ * sigk_pairwise_inc replaces PairwisePDESolver.solve / solve_scaled
+ * (sigpde/PDESolvers.py:56-84):
+ *   inc: (batch, nc_x, nc_y) with element strides (s0, s1, s2); out: (batch,)
+ */
+SIGK_API int sigk_pairwise_inc(const void *inc, int64_t batch, int64_t nc_x, int64_t nc_y, int64_t s0, int64_t s1, int64_t s2,
+                      int dtype, int order, const void *scale_x, const void *scale_y, void *out, int precision,
+                      void *workspace, size_t workspace_bytes, sigk_stream_t stream);
+
+/*
+ * sigk_gram_inc replaces GramPDESolver.solve / solve_scaled and, with
+ * symmetric != 0, SymmetricGramPDESolver.solve / solve_scaled
+ * (sigpde/PDESolvers.py:160-245):
+ *   inc: (n_x, n_y, nc_x, nc_y) with element strides (s0, s1, s2, s3);
+ *   out: (n_x, n_y) row-major with row stride out_ld (elements).
+ *   symmetric: solve only i >= j and mirror (requires n_x == n_y).
+ */
+SIGK_API int sigk_gram_inc(const void *inc, int64_t n_x, int64_t n_y, int64_t nc_x, int64_t nc_y, int64_t s0, int64_t s1,
+                  int64_t s2, int64_t s3, int dtype, int order, const void *scale_x, const void *scale_y,
+                  int symmetric, void *out, int64_t out_ld, int precision, void *workspace, size_t workspace_bytes,
+                  sigk_stream_t stream);
+
+/*
+ * sigk_normalize_inc replaces PairwisePDESolver.solve_norms
+ * (sigpde/PDESolvers.py:86-101, sigpde/cuda_pairwise_kernels.py:100-178) for
+ * precomputed self-increments inc: (n, nc, nc) with strides (s0, s1, s2).
+ * knorm and fnorm are float64 inputs (k(x,x) and f(k(x,x))).
+ */
+SIGK_API int sigk_normalize_inc(const void *inc, int64_t n, int64_t nc, int64_t s0, int64_t s1, int64_t s2, int dtype,
+                       int order, const double *knorm, const double *fnorm, double tol, int maxit, void *lam,
+                       int *iters, void *workspace, size_t workspace_bytes, sigk_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SIGK_H_ */

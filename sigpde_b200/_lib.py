@@ -1,0 +1,105 @@
+"""ctypes binding of libsigk.so (the C ABI declared in include/sigk.h).
+
+The shared library is built in-tree by ``python -m sigpde_b200.build`` (or
+``__graft_entry__.build()``).  There is no fallback: if the library is
+missing or cannot be loaded, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsigk.so")
+
+SIGK_OK = 0
+SIGK_EINVAL = 1
+SIGK_ENOMEM = 2
+SIGK_ETIMEDOUT = 3
+SIGK_ELAUNCH = 4
+SIGK_EUNSUPPORTED = 5
+_STATUS_NAMES = {0: "SIGK_OK", 1: "SIGK_EINVAL", 2: "SIGK_ENOMEM", 3: "SIGK_ETIMEDOUT", 4: "SIGK_ELAUNCH",
+                 5: "SIGK_EUNSUPPORTED"}
+
+SIGK_F32 = 0
+SIGK_F64 = 1
+SIGK_PREC_FP64 = 0
+SIGK_PREC_FP32 = 1
+SIGK_OP_PAIRWISE = 0
+SIGK_OP_GRAM = 1
+SIGK_OP_GRAM_SYM = 2
+SIGK_OP_NORMALIZE = 3
+
+# Exported symbol -> (restype, argtypes).  Kept in the order of include/sigk.h.
+_vp = ctypes.c_void_p
+_i64 = ctypes.c_int64
+_int = ctypes.c_int
+_dbl = ctypes.c_double
+_sz = ctypes.c_size_t
+
+SIGNATURES = {
+    "sigk_version": (ctypes.c_char_p, []),
+    "sigk_last_error_string": (ctypes.c_char_p, []),
+    "sigk_workspace_size": (_sz, [_int, _i64, _i64, _i64, _i64, _i64, _int, _int, _int]),
+    "sigk_pairwise": (_int, [_vp, _vp, _i64, _i64, _i64, _i64, _int, _int, _dbl, _vp, _vp, _vp, _int, _vp, _sz,
+                             _vp]),
+    "sigk_gram": (_int, [_vp, _vp, _i64, _i64, _i64, _i64, _i64, _int, _int, _dbl, _vp, _vp, _vp, _int, _vp, _sz,
+                         _vp]),
+    "sigk_gram_sym": (_int, [_vp, _i64, _i64, _i64, _int, _int, _dbl, _vp, _vp, _int, _vp, _sz, _vp]),
+    "sigk_self_norms": (_int, [_vp, _i64, _i64, _i64, _int, _int, _dbl, _vp, _vp, _sz, _vp]),
+    "sigk_normalize": (_int, [_vp, _i64, _i64, _i64, _int, _int, _dbl, _vp, _vp, _dbl, _int, _vp, _vp, _vp, _sz,
+                              _vp]),
+    "sigk_pairwise_inc": (_int, [_vp, _i64, _i64, _i64, _i64, _i64, _i64, _int, _int, _vp, _vp, _vp, _int, _vp, _sz,
+                                 _vp]),
+    "sigk_gram_inc": (_int, [_vp, _i64, _i64, _i64, _i64, _i64, _i64, _i64, _i64, _int, _int, _vp, _vp, _int, _vp,
+                             _i64, _int, _vp, _sz, _vp]),
+    "sigk_normalize_inc": (_int, [_vp, _i64, _i64, _i64, _i64, _i64, _int, _int, _vp, _vp, _dbl, _int, _vp, _vp, _vp,
+                                  _sz, _vp]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+class SigkError(RuntimeError):
+    """A libsigk entry point returned a non-zero status."""
+
+    def __init__(self, status: int, func: str, message: str):
+        super().__init__(f"{func} failed with {_STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+def lib() -> ctypes.CDLL:
+    """Load libsigk.so once; raise if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(
+                    f"libsigk.so is missing at {LIB_PATH}; build it with `python -m sigpde_b200.build` "
+                    "(this package has no CPU fallback)")
+            L = ctypes.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(L, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    return lib().sigk_last_error_string().decode()
+
+
+def call(name: str, *args) -> None:
+    """Call an entry point and raise SigkError on a non-zero status."""
+    st = getattr(lib(), name)(*args)
+    if st != SIGK_OK:
+        raise SigkError(st, name, last_error())
+
+
+def version() -> str:
+    return lib().sigk_version().decode()

@@ -1,0 +1,532 @@
+// sigk_api.cu -- C ABI of libsigk.so (declared in include/sigk.h).
+//
+// Validates arguments on the host, picks a kernel variant from the problem
+// shape (rows per lane R, dyadic order O, cell precision T, input dtype TIN),
+// sizes a persistent grid to the device's resident capacity and enqueues the
+// launch on the caller's stream.  Nothing here allocates device memory.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+
+#include "../../include/sigk.h"
+#include "sigk_kernels.cuh"
+
+namespace sigk {
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *where)
+{
+    return fail(SIGK_ELAUNCH, "%s: %s (%s)", where, cudaGetErrorString(e), cudaGetErrorName(e));
+}
+
+constexpr int kMaxBlocksPerSM = 8;
+constexpr size_t kMaxStageBytesPerWarp = 24 * 1024;
+
+int sm_count()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) return 148;
+    return n;
+}
+
+int64_t warp_cap() { return (int64_t)sm_count() * kMaxBlocksPerSM * kWarpsPerBlock; }
+
+// Rows per lane: the smallest power of two in {2,4,8,16} that covers the
+// refined rows with one band of 32*R rows, else 16 (several bands).
+int pick_rows(int64_t n)
+{
+    if (n <= 64) return 2;
+    if (n <= 128) return 4;
+    if (n <= 256) return 8;
+    return 16;
+}
+
+int rows_per_coarse_lane(int R, int order)
+{
+    if (order >= 4) return 1;
+    int rc = R >> order;
+    return rc > 0 ? rc : 1;
+}
+
+struct Plan {
+    int R;
+    int O;
+    int nbands;
+    int64_t n, m;
+    size_t stage_bytes_per_warp; // 0 = no staging
+    size_t bnd_bytes;            // total boundary scratch
+    int64_t bnd_stride;          // elements per warp
+};
+
+Plan make_plan(int64_t ncx, int64_t ncy, int64_t d, int order, size_t tsize, bool from_inc)
+{
+    Plan pl;
+    pl.n = ncx << order;
+    pl.m = ncy << order;
+    pl.O = order >= 4 ? 4 : order;
+    pl.R = pick_rows(pl.n);
+    pl.stage_bytes_per_warp = 0;
+    if (!from_inc) {
+        // shrink R (more bands) until the dx staging fits; if even R=2 does not fit, read dx from global
+        int R = pl.R;
+        while (true) {
+            size_t bytes = (size_t)rows_per_coarse_lane(R, order) * (size_t)d * 32 * tsize;
+            if (bytes <= kMaxStageBytesPerWarp) {
+                pl.R = R;
+                pl.stage_bytes_per_warp = bytes;
+                break;
+            }
+            if (R == 2) break;
+            R >>= 1;
+        }
+    }
+    pl.nbands = (int)((pl.n + 32 * pl.R - 1) / (32 * pl.R));
+    pl.bnd_stride = 0;
+    pl.bnd_bytes = 0;
+    if (pl.nbands > 1) {
+        pl.bnd_stride = ((pl.m + 1 + 31) / 32) * 32;
+        pl.bnd_bytes = (size_t)warp_cap() * (size_t)pl.bnd_stride * tsize;
+    }
+    return pl;
+}
+
+// ------------------------------------------------------------------ kernel tables
+using PairFn = void (*)(PairParams);
+using NormFn = void (*)(NormParams);
+
+template <typename T, typename TIN, int R, bool FI>
+PairFn pair_by_o(int O)
+{
+    switch (O) {
+    case 0: return pair_kernel<T, TIN, R, 0, FI>;
+    case 1: return pair_kernel<T, TIN, R, 1, FI>;
+    case 2: return pair_kernel<T, TIN, R, 2, FI>;
+    case 3: return pair_kernel<T, TIN, R, 3, FI>;
+    default: return pair_kernel<T, TIN, R, 4, FI>;
+    }
+}
+
+template <typename T, typename TIN, bool FI>
+PairFn pair_by_r(int R, int O)
+{
+    switch (R) {
+    case 2: return pair_by_o<T, TIN, 2, FI>(O);
+    case 4: return pair_by_o<T, TIN, 4, FI>(O);
+    case 8: return pair_by_o<T, TIN, 8, FI>(O);
+    default: return pair_by_o<T, TIN, 16, FI>(O);
+    }
+}
+
+PairFn pick_pair(int precision, int dtype, bool from_inc, int R, int O)
+{
+    const bool f64cells = (precision == SIGK_PREC_FP64);
+    const bool in64 = (dtype == SIGK_F64);
+    if (f64cells) {
+        if (in64) return from_inc ? pair_by_r<double, double, true>(R, O) : pair_by_r<double, double, false>(R, O);
+        return from_inc ? pair_by_r<double, float, true>(R, O) : pair_by_r<double, float, false>(R, O);
+    }
+    if (in64) return from_inc ? pair_by_r<float, double, true>(R, O) : pair_by_r<float, double, false>(R, O);
+    return from_inc ? pair_by_r<float, float, true>(R, O) : pair_by_r<float, float, false>(R, O);
+}
+
+template <typename TIN, int R, bool FI>
+NormFn norm_by_o(int O)
+{
+    switch (O) {
+    case 0: return normalize_kernel<TIN, R, 0, FI>;
+    case 1: return normalize_kernel<TIN, R, 1, FI>;
+    case 2: return normalize_kernel<TIN, R, 2, FI>;
+    case 3: return normalize_kernel<TIN, R, 3, FI>;
+    default: return normalize_kernel<TIN, R, 4, FI>;
+    }
+}
+
+template <typename TIN, bool FI>
+NormFn norm_by_r(int R, int O)
+{
+    switch (R) {
+    case 2: return norm_by_o<TIN, 2, FI>(O);
+    case 4: return norm_by_o<TIN, 4, FI>(O);
+    case 8: return norm_by_o<TIN, 8, FI>(O);
+    default: return norm_by_o<TIN, 16, FI>(O);
+    }
+}
+
+NormFn pick_norm(int dtype, bool from_inc, int R, int O)
+{
+    if (dtype == SIGK_F64) return from_inc ? norm_by_r<double, true>(R, O) : norm_by_r<double, false>(R, O);
+    return from_inc ? norm_by_r<float, true>(R, O) : norm_by_r<float, false>(R, O);
+}
+
+// ------------------------------------------------------------------ launching
+struct OccKey {
+    const void *fn;
+    size_t smem;
+    int dev;
+    bool operator==(const OccKey &o) const { return fn == o.fn && smem == o.smem && dev == o.dev; }
+};
+struct OccHash {
+    size_t operator()(const OccKey &k) const
+    {
+        return std::hash<const void *>()(k.fn) ^ (k.smem * 1315423911u) ^ ((size_t)k.dev << 48);
+    }
+};
+std::mutex g_occ_mu;
+std::unordered_map<OccKey, int, OccHash> g_occ;
+
+int blocks_per_sm(const void *fn, size_t smem, int *out)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    OccKey key{fn, smem, dev};
+    {
+        std::lock_guard<std::mutex> lk(g_occ_mu);
+        auto it = g_occ.find(key);
+        if (it != g_occ.end()) {
+            *out = it->second;
+            return SIGK_OK;
+        }
+    }
+    if (smem > 48 * 1024) {
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+    }
+    int nb = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kWarpsPerBlock * 32, smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (nb <= 0) return fail(SIGK_ELAUNCH, "kernel cannot be resident (smem=%zu bytes)", smem);
+    if (nb > kMaxBlocksPerSM) nb = kMaxBlocksPerSM;
+    {
+        std::lock_guard<std::mutex> lk(g_occ_mu);
+        g_occ[key] = nb;
+    }
+    *out = nb;
+    return SIGK_OK;
+}
+
+template <class P>
+int launch(void (*fn)(P), P params, int64_t nitems, size_t smem, cudaStream_t stream)
+{
+    int nb = 0;
+    int st = blocks_per_sm((const void *)fn, smem, &nb);
+    if (st != SIGK_OK) return st;
+    const int64_t want = (nitems + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    const int64_t cap = (int64_t)sm_count() * nb;
+    const int64_t blocks = want < cap ? want : cap;
+    if (blocks <= 0) return SIGK_OK;
+    fn<<<(unsigned)blocks, kWarpsPerBlock * 32, smem, stream>>>(params);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+    return SIGK_OK;
+}
+
+bool is_device_ptr(const void *p)
+{
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+int check_common(int dtype, int precision, int order)
+{
+    if (dtype != SIGK_F32 && dtype != SIGK_F64) return fail(SIGK_EINVAL, "dtype must be SIGK_F32 or SIGK_F64");
+    if (precision != SIGK_PREC_FP64 && precision != SIGK_PREC_FP32)
+        return fail(SIGK_EINVAL, "precision must be SIGK_PREC_FP64 or SIGK_PREC_FP32");
+    if (order < 0 || order > 12) return fail(SIGK_EINVAL, "dyadic order %d outside [0, 12]", order);
+    return SIGK_OK;
+}
+
+int check_dev(const void *p, const char *name, bool nullable)
+{
+    if (!p) return nullable ? SIGK_OK : fail(SIGK_EINVAL, "%s is NULL", name);
+    if (!is_device_ptr(p)) return fail(SIGK_EINVAL, "%s is not a device pointer", name);
+    return SIGK_OK;
+}
+
+size_t tsize_of(int precision) { return precision == SIGK_PREC_FP64 ? 8 : 4; }
+
+int check_ws(const Plan &pl, void *ws, size_t ws_bytes)
+{
+    if (pl.bnd_bytes == 0) return SIGK_OK;
+    if (!ws || ws_bytes < pl.bnd_bytes)
+        return fail(SIGK_ENOMEM, "workspace of %zu bytes needed (got %zu)", pl.bnd_bytes, ws ? ws_bytes : 0);
+    if (((uintptr_t)ws & 15) != 0) return fail(SIGK_EINVAL, "workspace must be 16-byte aligned");
+    return SIGK_OK;
+}
+
+int run_pairs(int op, const void *x, const void *y, int64_t nx, int64_t ny, int64_t lx, int64_t ly, int64_t d,
+              int dtype, int order, double static_scale, const void *sx, const void *sy, void *out, int64_t out_ld,
+              int precision, void *ws, size_t ws_bytes, cudaStream_t stream)
+{
+    int st = check_common(dtype, precision, order);
+    if (st) return st;
+    if (nx < 1 || ny < 1) return fail(SIGK_EINVAL, "path counts must be >= 1 (got %lld, %lld)", (long long)nx,
+                                      (long long)ny);
+    if (lx < 2 || ly < 2) return fail(SIGK_EINVAL, "path lengths must be >= 2 (got %lld, %lld)", (long long)lx,
+                                      (long long)ly);
+    if (d < 1) return fail(SIGK_EINVAL, "dim must be >= 1");
+    if ((st = check_dev(x, "x", false)) || (st = check_dev(y, "y", false)) || (st = check_dev(out, "out", false)) ||
+        (st = check_dev(sx, "scale_x", true)) || (st = check_dev(sy, "scale_y", true)))
+        return st;
+    const size_t ts = tsize_of(precision);
+    Plan pl = make_plan(lx - 1, ly - 1, d, order, ts, false);
+    if ((st = check_ws(pl, ws, ws_bytes))) return st;
+
+    PairParams p{};
+    p.op = op;
+    p.x = x;
+    p.y = y;
+    p.nx = nx;
+    p.ny = ny;
+    p.ncx = lx - 1;
+    p.ncy = ly - 1;
+    p.d = d;
+    p.order = order;
+    p.fscale = static_scale * std::ldexp(1.0, -2 * order);
+    p.sx = sx;
+    p.sy = sy;
+    p.out = out;
+    p.out_ld = out_ld;
+    p.nitems = op == kOpPairwise ? nx : (op == kOpGram ? nx * ny : nx * (nx + 1) / 2);
+    p.bnd = pl.bnd_bytes ? ws : nullptr;
+    p.bnd_stride = pl.bnd_stride;
+    p.stage_smem = pl.stage_bytes_per_warp > 0;
+    PairFn fn = pick_pair(precision, dtype, false, pl.R, pl.O);
+    return launch(fn, p, p.nitems, pl.stage_bytes_per_warp * kWarpsPerBlock, stream);
+}
+
+} // namespace
+} // namespace sigk
+
+using namespace sigk;
+
+extern "C" {
+
+const char *sigk_version(void) { return "sigk 0.1.0 sm_100a"; }
+
+const char *sigk_last_error_string(void) { return g_last_error.c_str(); }
+
+size_t sigk_workspace_size(int op, int64_t n_x, int64_t n_y, int64_t len_x, int64_t len_y, int64_t dim, int order,
+                           int dtype, int precision)
+{
+    (void)n_x;
+    (void)n_y;
+    (void)dtype;
+    if (len_x < 2 || len_y < 2 || order < 0 || order > 12 || dim < 0) return 0;
+    if (op == SIGK_OP_NORMALIZE) precision = SIGK_PREC_FP64;
+    if (op == SIGK_OP_GRAM_SYM || op == SIGK_OP_NORMALIZE) len_y = len_x;
+    // dim == 0 selects the plan of the *_inc entry points (no dx staging)
+    Plan pl = make_plan(len_x - 1, len_y - 1, dim > 0 ? dim : 1, order, tsize_of(precision), dim == 0);
+    return pl.bnd_bytes;
+}
+
+int sigk_pairwise(const void *x, const void *y, int64_t batch, int64_t len_x, int64_t len_y, int64_t dim, int dtype,
+                  int order, double static_scale, const void *scale_x, const void *scale_y, void *out, int precision,
+                  void *workspace, size_t workspace_bytes, sigk_stream_t stream)
+{
+    return run_pairs(kOpPairwise, x, y, batch, batch, len_x, len_y, dim, dtype, order, static_scale, scale_x, scale_y,
+                     out, 1, precision, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+int sigk_gram(const void *x, const void *y, int64_t n_x, int64_t n_y, int64_t len_x, int64_t len_y, int64_t dim,
+              int dtype, int order, double static_scale, const void *scale_x, const void *scale_y, void *out,
+              int precision, void *workspace, size_t workspace_bytes, sigk_stream_t stream)
+{
+    return run_pairs(kOpGram, x, y, n_x, n_y, len_x, len_y, dim, dtype, order, static_scale, scale_x, scale_y, out,
+                     n_y, precision, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+int sigk_gram_sym(const void *x, int64_t n, int64_t len, int64_t dim, int dtype, int order, double static_scale,
+                  const void *scale, void *out, int precision, void *workspace, size_t workspace_bytes,
+                  sigk_stream_t stream)
+{
+    return run_pairs(kOpGramSym, x, x, n, n, len, len, dim, dtype, order, static_scale, scale, scale, out, n,
+                     precision, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+static int run_normalize(const void *x, const void *inc, int64_t n, int64_t nc, int64_t d, int64_t s0, int64_t s1,
+                         int64_t s2, int dtype, int order, double static_scale, double *knorm, const double *fnorm,
+                         double tol, int maxit, void *lam, int *iters, void *ws, size_t ws_bytes,
+                         cudaStream_t stream)
+{
+    int st = check_common(dtype, SIGK_PREC_FP64, order);
+    if (st) return st;
+    if (n < 1) return fail(SIGK_EINVAL, "path count must be >= 1");
+    if (nc < 1) return fail(SIGK_EINVAL, "path length must be >= 2");
+    if (maxit < 0) return fail(SIGK_EINVAL, "maxit must be >= 0");
+    if (!(tol >= 0)) return fail(SIGK_EINVAL, "tol must be >= 0");
+    const bool from_inc = inc != nullptr;
+    if (from_inc) {
+        if ((st = check_dev(inc, "inc", false))) return st;
+        if (!knorm || !fnorm) return fail(SIGK_EINVAL, "increment mode needs knorm and fnorm");
+    } else {
+        if (d < 1) return fail(SIGK_EINVAL, "dim must be >= 1");
+        if ((st = check_dev(x, "x", false))) return st;
+    }
+    if ((st = check_dev(lam, "lam", false)) || (st = check_dev(knorm, "knorm", true)) ||
+        (st = check_dev(fnorm, "fnorm", true)) || (st = check_dev(iters, "iters", true)))
+        return st;
+    if (fnorm && !knorm) return fail(SIGK_EINVAL, "fnorm given without knorm");
+    Plan pl = make_plan(nc, nc, from_inc ? 1 : d, order, 8, from_inc);
+    if ((st = check_ws(pl, ws, ws_bytes))) return st;
+    NormParams p{};
+    p.x = x;
+    p.n = n;
+    p.nc = nc;
+    p.d = d;
+    p.order = order;
+    p.fscale = from_inc ? 1.0 : static_scale * std::ldexp(1.0, -2 * order);
+    p.inc = inc;
+    p.is0 = s0;
+    p.is1 = s1;
+    p.is2 = s2;
+    p.knorm = knorm;
+    p.fnorm = fnorm;
+    p.tol = tol;
+    p.maxit = maxit;
+    p.lam = lam;
+    p.iters = iters;
+    p.bnd = pl.bnd_bytes ? ws : nullptr;
+    p.bnd_stride = pl.bnd_stride;
+    p.stage_smem = pl.stage_bytes_per_warp > 0;
+    NormFn fn = pick_norm(dtype, from_inc, pl.R, pl.O);
+    return launch(fn, p, n, pl.stage_bytes_per_warp * kWarpsPerBlock, stream);
+}
+
+int sigk_self_norms(const void *x, int64_t n, int64_t len, int64_t dim, int dtype, int order, double static_scale,
+                    double *knorm, void *workspace, size_t workspace_bytes, sigk_stream_t stream)
+{
+    // k(x,x) with float64 cells, written as float64; NaN -> +inf is applied by
+    // the normalisation kernel with maxit = 0 (no bracket iterations).
+    int st = check_dev(knorm, "knorm", false);
+    if (st) return st;
+    if (!x) return fail(SIGK_EINVAL, "x is NULL");
+    // lam output is required by the kernel; reuse knorm's storage would alias,
+    // so run the pair kernel directly with float64 output instead.
+    st = check_common(dtype, SIGK_PREC_FP64, order);
+    if (st) return st;
+    if (n < 1 || len < 2 || dim < 1) return fail(SIGK_EINVAL, "bad shape (n=%lld len=%lld dim=%lld)",
+                                                 (long long)n, (long long)len, (long long)dim);
+    if ((st = check_dev(x, "x", false))) return st;
+    Plan pl = make_plan(len - 1, len - 1, dim, order, 8, false);
+    if ((st = check_ws(pl, workspace, workspace_bytes))) return st;
+    NormParams p{};
+    p.x = x;
+    p.n = n;
+    p.nc = len - 1;
+    p.d = dim;
+    p.order = order;
+    p.fscale = static_scale * std::ldexp(1.0, -2 * order);
+    p.knorm = knorm;
+    p.fnorm = nullptr;
+    p.tol = 0;
+    p.maxit = 0;
+    p.lam = nullptr;
+    p.bnd = pl.bnd_bytes ? workspace : nullptr;
+    p.bnd_stride = pl.bnd_stride;
+    p.stage_smem = pl.stage_bytes_per_warp > 0;
+    NormFn fn = pick_norm(dtype, false, pl.R, pl.O);
+    return launch(fn, p, n, pl.stage_bytes_per_warp * kWarpsPerBlock, (cudaStream_t)stream);
+}
+
+int sigk_normalize(const void *x, int64_t n, int64_t len, int64_t dim, int dtype, int order, double static_scale,
+                   double *knorm, const double *fnorm, double tol, int maxit, void *lam, int *iters, void *workspace,
+                   size_t workspace_bytes, sigk_stream_t stream)
+{
+    if (len < 2) return fail(SIGK_EINVAL, "path length must be >= 2");
+    return run_normalize(x, nullptr, n, len - 1, dim, 0, 0, 0, dtype, order, static_scale, knorm, fnorm, tol, maxit,
+                         lam, iters, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+int sigk_normalize_inc(const void *inc, int64_t n, int64_t nc, int64_t s0, int64_t s1, int64_t s2, int dtype,
+                       int order, const double *knorm, const double *fnorm, double tol, int maxit, void *lam,
+                       int *iters, void *workspace, size_t workspace_bytes, sigk_stream_t stream)
+{
+    if (!inc) return fail(SIGK_EINVAL, "inc is NULL");
+    return run_normalize(nullptr, inc, n, nc, 1, s0, s1, s2, dtype, order, 1.0, const_cast<double *>(knorm), fnorm,
+                         tol, maxit, lam, iters, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+static int run_inc(int op, const void *inc, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, int64_t s0, int64_t s1,
+                   int64_t s2, int64_t s3, int dtype, int order, const void *sx, const void *sy, void *out,
+                   int64_t out_ld, int precision, void *ws, size_t ws_bytes, cudaStream_t stream)
+{
+    int st = check_common(dtype, precision, order);
+    if (st) return st;
+    if (nx < 1 || ny < 1 || ncx < 1 || ncy < 1) return fail(SIGK_EINVAL, "empty increment tensor");
+    if ((st = check_dev(inc, "inc", false)) || (st = check_dev(out, "out", false)) ||
+        (st = check_dev(sx, "scale_x", true)) || (st = check_dev(sy, "scale_y", true)))
+        return st;
+    Plan pl = make_plan(ncx, ncy, 1, order, tsize_of(precision), true);
+    if ((st = check_ws(pl, ws, ws_bytes))) return st;
+    PairParams p{};
+    p.op = op;
+    p.nx = nx;
+    p.ny = ny;
+    p.ncx = ncx;
+    p.ncy = ncy;
+    p.d = 1;
+    p.order = order;
+    p.fscale = 1.0;
+    p.sx = sx;
+    p.sy = sy;
+    p.inc = inc;
+    p.is0 = s0;
+    p.is1 = s1;
+    p.is2 = s2;
+    p.is3 = s3;
+    p.out = out;
+    p.out_ld = out_ld;
+    p.nitems = op == kOpPairwise ? nx : (op == kOpGram ? nx * ny : nx * (nx + 1) / 2);
+    p.bnd = pl.bnd_bytes ? ws : nullptr;
+    p.bnd_stride = pl.bnd_stride;
+    p.stage_smem = 0;
+    PairFn fn = pick_pair(precision, dtype, true, pl.R, pl.O);
+    return launch(fn, p, p.nitems, 0, stream);
+}
+
+int sigk_pairwise_inc(const void *inc, int64_t batch, int64_t nc_x, int64_t nc_y, int64_t s0, int64_t s1, int64_t s2,
+                      int dtype, int order, const void *scale_x, const void *scale_y, void *out, int precision,
+                      void *workspace, size_t workspace_bytes, sigk_stream_t stream)
+{
+    return run_inc(kOpPairwise, inc, batch, batch, nc_x, nc_y, s0, s1, s2, 0, dtype, order, scale_x, scale_y, out, 1,
+                   precision, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+int sigk_gram_inc(const void *inc, int64_t n_x, int64_t n_y, int64_t nc_x, int64_t nc_y, int64_t s0, int64_t s1,
+                  int64_t s2, int64_t s3, int dtype, int order, const void *scale_x, const void *scale_y, int symmetric,
+                  void *out, int64_t out_ld, int precision, void *workspace, size_t workspace_bytes,
+                  sigk_stream_t stream)
+{
+    if (symmetric && n_x != n_y) return fail(SIGK_EINVAL, "symmetric Gram needs n_x == n_y");
+    return run_inc(symmetric ? kOpGramSym : kOpGram, inc, n_x, n_y, nc_x, nc_y, s0, s1, s2, s3, dtype, order,
+                   scale_x, scale_y, out, out_ld, precision, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+} // extern "C"

@@ -1,0 +1,240 @@
+// sigk_kernels.cuh -- persistent-warp kernels built on warp_solve (wave.cuh).
+//
+//   pair_kernel       pairwise / Gram / symmetric-Gram signature kernels
+//   normalize_kernel  robust normalisation: per-path Chandrupatla root-find
+//                     whose every iteration re-solves the PDE on-chip
+//
+// Each kernel is a grid of 4-warp blocks sized to the resident capacity of
+// the device; warp w handles work items w, w + W, w + 2W, ... (W = warps in
+// the grid).  Gram items are numbered row-major, so neighbouring warps share
+// x_i and read neighbouring y_j (L1/L2 reuse).
+#pragma once
+
+#include "wave.cuh"
+
+namespace sigk {
+
+enum : int { kOpPairwise = 0, kOpGram = 1, kOpGramSym = 2 };
+
+constexpr int kWarpsPerBlock = 4;
+
+struct PairParams {
+    int op;
+    const void *x;
+    const void *y;
+    int64_t nx, ny;     // path counts (pairwise: batch in both)
+    int64_t ncx, ncy;   // coarse cells per side (len - 1)
+    int64_t d;
+    int order;
+    double fscale;      // static_scale * 4^-order (path mode) or 1 (increment mode)
+    const void *sx;
+    const void *sy;
+    const void *inc;    // increment mode only
+    int64_t is0, is1, is2, is3;
+    void *out;
+    int64_t out_ld;
+    int64_t nitems;
+    void *bnd;          // per-warp boundary rows (multi-band pairs only)
+    int64_t bnd_stride; // elements per warp
+    int stage_smem;     // 1: dx rows staged in shared memory
+};
+
+// Lower-triangle index w -> (i, j), i >= j, w = i*(i+1)/2 + j.
+__device__ __forceinline__ void tri_decode(int64_t w, int64_t &i, int64_t &j)
+{
+    int64_t r = (int64_t)((sqrt(8.0 * (double)w + 1.0) - 1.0) * 0.5);
+    while (r * (r + 1) / 2 > w) --r;
+    while ((r + 1) * (r + 2) / 2 <= w) ++r;
+    i = r;
+    j = w - r * (r + 1) / 2;
+}
+
+template <typename TIN>
+__device__ __forceinline__ double scale_at(const void *s, int64_t i)
+{
+    return s ? (double)reinterpret_cast<const TIN *>(s)[i] : 1.0;
+}
+
+template <typename T, typename TIN, int R, int O, bool FROM_INC>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) pair_kernel(PairParams p)
+{
+    using BS = BlockShape<R, O>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int64_t gwarp = (int64_t)blockIdx.x * kWarpsPerBlock + wib;
+    const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
+    const SolveGeom g = make_geom<R, O>(p.ncx, p.ncy, p.order);
+    T *bnd = p.bnd ? reinterpret_cast<T *>(p.bnd) + gwarp * p.bnd_stride : nullptr;
+    TIN *out = reinterpret_cast<TIN *>(p.out);
+
+    for (int64_t item = gwarp; item < p.nitems; item += nwarps) {
+        int64_t xi, yj;
+        if (p.op == kOpPairwise) {
+            xi = item;
+            yj = item;
+        } else if (p.op == kOpGram) {
+            xi = item / p.ny;
+            yj = item - xi * p.ny;
+        } else {
+            tri_decode(item, xi, yj);
+        }
+        double s = p.fscale;
+        if (p.sx) s *= scale_at<TIN>(p.sx, xi);
+        if (p.sy) s *= scale_at<TIN>(p.sy, yj);
+
+        T val;
+        if constexpr (FROM_INC) {
+            GivenIncs<T, TIN, BS::RC> src;
+            const TIN *base = reinterpret_cast<const TIN *>(p.inc);
+            if (p.op == kOpPairwise) {
+                src.inc = base + item * p.is0;
+                src.si = p.is1;
+                src.sj = p.is2;
+            } else {
+                src.inc = base + xi * p.is0 + yj * p.is1;
+                src.si = p.is2;
+                src.sj = p.is3;
+            }
+            src.fscale = T(s);
+            val = warp_solve<T, R, O>(g, src, bnd);
+        } else {
+            PathIncs<T, TIN, BS::RC> src;
+            src.X = reinterpret_cast<const TIN *>(p.x) + xi * (p.ncx + 1) * p.d;
+            src.Y = reinterpret_cast<const TIN *>(p.y) + yj * (p.ncy + 1) * p.d;
+            src.d = p.d;
+            src.dxs = p.stage_smem ? reinterpret_cast<T *>(smem_raw) + (int64_t)wib * BS::RC * p.d * 32 : nullptr;
+            src.fscale = T(s);
+            val = warp_solve<T, R, O>(g, src, bnd);
+        }
+        if (lane == 0) {
+            if (p.op == kOpPairwise) {
+                out[item] = TIN(val);
+            } else {
+                out[xi * p.out_ld + yj] = TIN(val);
+                if (p.op == kOpGramSym && xi != yj) out[yj * p.out_ld + xi] = TIN(val);
+            }
+        }
+    }
+}
+
+struct NormParams {
+    const void *x;
+    int64_t n;
+    int64_t nc;
+    int64_t d;
+    int order;
+    double fscale;      // static_scale * 4^-order (path mode) or 1
+    const void *inc;    // increment mode only
+    int64_t is0, is1, is2;
+    double *knorm;      // builtin: output (may be null); external: input
+    const double *fnorm; // null: builtin f(s) = 2 - 1/(1 + log s)
+    double tol;
+    int maxit;
+    void *lam;
+    int *iters;
+    void *bnd;
+    int64_t bnd_stride;
+    int stage_smem;
+};
+
+// The Chandrupatla iteration of sigpde/cuda_pairwise_kernels.py:100-178 with
+// the argument order of sigpde/torch/kernel.py:186-193: g(l) = k(l x) - f(k),
+// g(0) = 1 - f(k), g(1) = k - f(k).  All bracket state is float64 and
+// warp-uniform; the PDE solve returns the same value in every lane.
+template <typename TIN, int R, int O, bool FROM_INC>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) normalize_kernel(NormParams p)
+{
+    using T = double;
+    using BS = BlockShape<R, O>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int64_t gwarp = (int64_t)blockIdx.x * kWarpsPerBlock + wib;
+    const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
+    const SolveGeom g = make_geom<R, O>(p.nc, p.nc, p.order);
+    T *bnd = p.bnd ? reinterpret_cast<T *>(p.bnd) + gwarp * p.bnd_stride : nullptr;
+    TIN *lam_out = reinterpret_cast<TIN *>(p.lam);
+
+    for (int64_t b = gwarp; b < p.n; b += nwarps) {
+        PathIncs<T, TIN, BS::RC> psrc;
+        GivenIncs<T, TIN, BS::RC> gsrc;
+        if constexpr (FROM_INC) {
+            gsrc.inc = reinterpret_cast<const TIN *>(p.inc) + b * p.is0;
+            gsrc.si = p.is1;
+            gsrc.sj = p.is2;
+        } else {
+            psrc.X = reinterpret_cast<const TIN *>(p.x) + b * (p.nc + 1) * p.d;
+            psrc.Y = psrc.X;
+            psrc.d = p.d;
+            psrc.dxs = p.stage_smem ? reinterpret_cast<T *>(smem_raw) + (int64_t)wib * BS::RC * p.d * 32 : nullptr;
+        }
+        auto solve = [&](double scale) -> double {
+            if constexpr (FROM_INC) {
+                gsrc.fscale = p.fscale * scale;
+                return warp_solve<T, R, O>(g, gsrc, bnd);
+            } else {
+                psrc.fscale = p.fscale * scale;
+                return warp_solve<T, R, O>(g, psrc, bnd);
+            }
+        };
+
+        double k, fk;
+        if (p.fnorm == nullptr) {
+            k = solve(1.0);
+            if (isnan(k)) k = __longlong_as_double(0x7ff0000000000000LL); // NaN -> +inf (kernel.py:183)
+            fk = 2.0 - 1.0 / (1.0 + log(k));                              // kernel.py:23-24
+            if (p.knorm && lane == 0) p.knorm[b] = k;
+        } else {
+            k = p.knorm[b];
+            fk = p.fnorm[b];
+        }
+
+        double out = 0.0;
+        int it = 0;
+        if (k >= 1.0) { // lambda is forced to 0 for k < 1 (kernel.py:195), so the loop is skipped
+            double a = 0.0, c = 0.0, bb = 1.0;
+            double fa = 1.0 - fk;
+            double fb = k - fk;
+            double fc = fa;
+            double t = 0.5;
+            for (it = 0; it < p.maxit;) {
+                const double xt = a + t * (bb - a);
+                const double sol = solve(xt * xt);
+                const double ft = isnan(sol) ? __longlong_as_double(0x7ff0000000000000LL) : sol - fk;
+                ++it;
+                if (ft * fa >= 0) {
+                    c = a;
+                    fc = fa;
+                } else {
+                    c = bb;
+                    bb = a;
+                    fc = fb;
+                    fb = fa;
+                }
+                a = xt;
+                fa = ft;
+                if (fabs(fa) < fabs(fb)) {
+                    out = a;
+                    if (fabs(fa) < p.tol) break;
+                } else {
+                    out = bb;
+                    if (fabs(fb) < p.tol) break;
+                }
+                const double xi = (a - bb) / (c - bb);
+                const double phi = (fa - fb) / (fc - fb);
+                if (phi * phi < xi && (1 - phi) * (1 - phi) < 1 - xi)
+                    t = fa / (fb - fa) * fc / (fb - fc) + (c - a) / (bb - a) * fa / (fc - fa) * fb / (fc - fb);
+                else
+                    t = 0.5;
+                if (!(0 < t && t < 1)) t = 0.5;
+            }
+        }
+        if (lane == 0) {
+            if (lam_out) lam_out[b] = TIN(out);
+            if (p.iters) p.iters[b] = it;
+        }
+    }
+}
+
+} // namespace sigk

@@ -1,0 +1,259 @@
+// wave.cuh -- warp-synchronous anti-diagonal Goursat wavefront for sm_100a.
+//
+// One warp solves one (x, y) pair.  The refined grid has n = (len_x-1)*2^order
+// rows and m = (len_y-1)*2^order columns; K = 1 on row 0 and column 0 and
+//   K[i][j] = (K[i][j-1] + K[i-1][j]) * A - K[i-1][j-1] * B,
+//   A = 1 + c/2 + c^2/12,  B = 1 - c^2/12,
+// with c the coarse increment of cell (i,j) (sigpde/cuda_device_functions.py:3-5
+// restated with the coefficients hoisted per coarse cell).
+//
+// Layout of the work in registers (no global scratch, no __syncthreads):
+//   * rows are cut into bands of 32*R; lane l of the warp owns R consecutive
+//     rows of the band and keeps their current column in registers;
+//   * every step the lane advances its rows by C = 2^order columns (C = 8 for
+//     order >= 4): an R x C block whose cells share one coarse column, so each
+//     step needs R/2^order increments and R/2^order (A, B) pairs;
+//   * lane l runs one step behind lane l-1 and receives lane l-1's bottom row
+//     of the same column block through __shfl_up_sync (C values per step);
+//   * a band that is not the last writes its bottom row to a per-warp
+//     boundary buffer that the next band's lane 0 reads.
+// The R x C block is straight-line code, so the compiler overlaps its cells
+// along anti-diagonals (critical path R + C - 1 cells, 3 FP ops per cell).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sigk {
+
+constexpr unsigned kFullMask = 0xffffffffu;
+
+template <typename T>
+__device__ __forceinline__ T ld_in(const T *p)
+{
+    return __ldg(p);
+}
+
+// A = 1 + c/2 + c^2/12, B = 1 - c^2/12
+template <typename T>
+__device__ __forceinline__ void stencil_coefs(T c, T &A, T &B)
+{
+    const T c2 = c * c;
+    A = fma(c2, T(1.0 / 12.0), fma(c, T(0.5), T(1)));
+    B = fma(c2, T(-1.0 / 12.0), T(1));
+}
+
+// Compile-time shape of one lane's block.
+template <int R, int O>
+struct BlockShape {
+    static constexpr int C = (O <= 3) ? (1 << O) : 8;                       // fine columns per step
+    static constexpr int RC = (O <= 3) ? ((R >> O) > 0 ? (R >> O) : 1) : 1; // coarse rows per lane
+    static constexpr int ROWS_PER_COARSE = (O <= 3) ? (1 << O) : 1 << 30;
+    __host__ __device__ static constexpr int rc_of(int r) { return (RC == 1) ? 0 : r / ROWS_PER_COARSE; }
+};
+
+// Geometry of one solve.
+struct SolveGeom {
+    int64_t ncx, ncy; // coarse cells per side (len - 1)
+    int order;
+    int64_t n, m;     // refined rows / columns
+    int nbands;
+    int64_t nsteps;   // column blocks per band
+};
+
+template <int R, int O>
+__device__ __forceinline__ SolveGeom make_geom(int64_t ncx, int64_t ncy, int order)
+{
+    SolveGeom g;
+    g.ncx = ncx;
+    g.ncy = ncy;
+    g.order = order;
+    g.n = ncx << order;
+    g.m = ncy << order;
+    g.nbands = (int)((g.n + 32 * R - 1) / (32 * R));
+    g.nsteps = g.m / BlockShape<R, O>::C;
+    return g;
+}
+
+// Source of increments computed from the two paths (linear static kernel):
+// c(ci, cj) = fscale * <x[ci+1]-x[ci], y[cj+1]-y[cj]>, differences taken in T
+// (exact for float32 paths when T is double).  Computing the differences
+// first avoids the cancellation of the reference's 4-term difference of the
+// static Gram (sigpde/torch/kernel.py:13-21); both are equal in exact
+// arithmetic.  The lane's dx rows live in shared memory as [rc][k][lane]
+// (conflict-free); without a staging area they are re-read from global.
+template <typename T, typename TIN, int RC>
+struct PathIncs {
+    const TIN *X;
+    const TIN *Y;
+    int64_t d;
+    T *dxs;      // this warp's staging area: RC * d * 32 values, or null
+    T fscale;
+    int64_t ci0 = 0, ncx = 0;
+    bool rc_per_row = false;
+
+    __device__ __forceinline__ void stage(int64_t ci0_, int64_t ncx_, int lane, bool rc_per_row_)
+    {
+        ci0 = ci0_;
+        ncx = ncx_;
+        rc_per_row = rc_per_row_;
+        if (!dxs) return;
+        __syncwarp();
+        for (int rc = 0; rc < RC; ++rc) {
+            const int64_t ci = ci0 + (rc_per_row ? rc : 0);
+            const bool ok = ci < ncx;
+            const TIN *x0 = X + ci * d;
+            for (int64_t k = 0; k < d; ++k) {
+                T v = T(0);
+                if (ok) v = T(ld_in(x0 + d + k)) - T(ld_in(x0 + k));
+                dxs[(rc * d + k) * 32 + lane] = v;
+            }
+        }
+        __syncwarp();
+    }
+
+    __device__ __forceinline__ void column(int64_t cj, int lane, T (&c)[RC]) const
+    {
+#pragma unroll
+        for (int rc = 0; rc < RC; ++rc) c[rc] = T(0);
+        const TIN *y0 = Y + cj * d;
+        if (dxs) {
+            for (int64_t k = 0; k < d; ++k) {
+                const T dy = T(ld_in(y0 + d + k)) - T(ld_in(y0 + k));
+#pragma unroll
+                for (int rc = 0; rc < RC; ++rc) c[rc] = fma(dxs[(rc * d + k) * 32 + lane], dy, c[rc]);
+            }
+        } else {
+            for (int64_t k = 0; k < d; ++k) {
+                const T dy = T(ld_in(y0 + d + k)) - T(ld_in(y0 + k));
+#pragma unroll
+                for (int rc = 0; rc < RC; ++rc) {
+                    const int64_t ci = ci0 + (rc_per_row ? rc : 0);
+                    if (ci < ncx) {
+                        const TIN *x0 = X + ci * d;
+                        c[rc] = fma(T(ld_in(x0 + d + k)) - T(ld_in(x0 + k)), dy, c[rc]);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int rc = 0; rc < RC; ++rc) c[rc] *= fscale;
+    }
+};
+
+// Source of precomputed coarse increments (generic static kernels): strided
+// reads of inc[ci][cj] in TIN, times fscale.
+template <typename T, typename TIN, int RC>
+struct GivenIncs {
+    const TIN *inc;
+    int64_t si, sj;
+    T fscale;
+    int64_t ci0;
+    bool rc_per_row;
+    int64_t ncx;
+
+    __device__ __forceinline__ void stage(int64_t ci0_, int64_t ncx_, int, bool rc_per_row_)
+    {
+        ci0 = ci0_;
+        ncx = ncx_;
+        rc_per_row = rc_per_row_;
+    }
+
+    __device__ __forceinline__ void column(int64_t cj, int, T (&c)[RC]) const
+    {
+#pragma unroll
+        for (int rc = 0; rc < RC; ++rc) {
+            const int64_t ci = ci0 + (rc_per_row ? rc : 0);
+            c[rc] = (ci < ncx) ? T(ld_in(inc + ci * si + cj * sj)) * fscale : T(0);
+        }
+    }
+};
+
+// Solve one pair with the warp.  Returns K[n][m] in every lane.
+// bnd: per-warp boundary row buffer of m + 1 values (only touched when the
+// pair has more than one band).
+template <typename T, int R, int O, class Src>
+__device__ T warp_solve(const SolveGeom &g, Src &src, T *bnd)
+{
+    using BS = BlockShape<R, O>;
+    constexpr int C = BS::C;
+    constexpr int RC = BS::RC;
+    const int lane = threadIdx.x & 31;
+    const bool rc_per_row = (RC > 1);
+    T result = T(1);
+
+    for (int b = 0; b < g.nbands; ++b) {
+        const int64_t row0 = (int64_t)b * 32 * R + (int64_t)lane * R; // first refined row (0-based)
+        src.stage(row0 >> g.order, g.ncx, lane, rc_per_row);
+
+        T left[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) left[r] = T(1);
+        T bot[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) bot[c] = T(1);
+        T corner_next = T(1);
+        const bool first_band = (b == 0);
+        const bool write_bnd = (lane == 31) && (b + 1 < g.nbands);
+
+        const int64_t total = g.nsteps + 31;
+        for (int64_t s = 0; s < total; ++s) {
+            const int64_t q = s - lane;
+            T top[C];
+#pragma unroll
+            for (int c = 0; c < C; ++c) top[c] = __shfl_up_sync(kFullMask, bot[c], 1);
+            const bool active = (q >= 0) && (q < g.nsteps);
+            if (lane == 0) {
+                if (first_band) {
+#pragma unroll
+                    for (int c = 0; c < C; ++c) top[c] = T(1);
+                } else if (active) {
+#pragma unroll
+                    for (int c = 0; c < C; ++c) top[c] = bnd[q * C + 1 + c];
+                }
+            }
+            if (active) {
+                const T corner = (q == 0) ? T(1) : corner_next;
+                corner_next = top[C - 1];
+                T cc[RC];
+                src.column((q * C) >> g.order, lane, cc);
+                T A[RC], B[RC];
+#pragma unroll
+                for (int rc = 0; rc < RC; ++rc) stencil_coefs(cc[rc], A[rc], B[rc]);
+#pragma unroll
+                for (int c = 0; c < C; ++c) {
+                    T up = top[c];
+                    T dg = (c == 0) ? corner : top[c - 1];
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        const T l = left[r];
+                        const T v = fma(l + up, A[BS::rc_of(r)], -(dg * B[BS::rc_of(r)]));
+                        dg = l;
+                        up = v;
+                        left[r] = v;
+                    }
+                    bot[c] = up;
+                }
+                if (write_bnd) {
+#pragma unroll
+                    for (int c = 0; c < C; ++c) bnd[q * C + 1 + c] = bot[c];
+                }
+            }
+        }
+        __syncwarp(); // orders lane 31's boundary stores before the next band's loads
+
+        if (b == g.nbands - 1) {
+            const int64_t last = g.n - 1 - (int64_t)b * 32 * R; // row index within the band
+            const int lstar = (int)(last / R);
+            const int rstar = (int)(last % R);
+            T v = left[0];
+#pragma unroll
+            for (int r = 1; r < R; ++r)
+                if (r == rstar) v = left[r];
+            result = __shfl_sync(kFullMask, v, lstar);
+        }
+    }
+    return result;
+}
+
+} // namespace sigk

@@ -1,0 +1,335 @@
+"""`SigPDE` and `RobustSigPDE` with the API of sigpde/torch/kernel.py, backed
+by libsigk.so (hand-written sm_100a CUDA).
+
+Differences from the reference that a caller can observe:
+  * the work is enqueued on torch's current CUDA stream and the call returns
+    without a device-wide synchronise (the reference calls
+    numba.cuda.synchronize(), kernel.py:56-63,124,169,228,289); results are
+    ordinary torch tensors, so stream order keeps every later torch op correct;
+  * PDE cells are float64 by default (`precision="fp64"`), also for float32
+    inputs, and the robust normalisation always runs in float64, including
+    k(x,x) and f(k(x,x)); the reference rounds every cell to the input dtype
+    and overflows k(x,x) to inf in float32 (SURVEY: 17.6% of the robust
+    benchmark paths).  `precision="fp32"` gives float32 cells;
+  * `max_batch` / `max_threads` are accepted and only bound the memory of the
+    generic-increment path (non-linear static kernels); the linear kernel runs
+    any batch in one launch.
+"""
+from __future__ import annotations
+
+import math
+
+import torch
+
+from .. import _lib
+from . import static_kernels
+
+_PREC = {"fp64": _lib.SIGK_PREC_FP64, "fp32": _lib.SIGK_PREC_FP32}
+
+
+def _dtype_code(t: torch.Tensor) -> int:
+    if t.dtype == torch.float32:
+        return _lib.SIGK_F32
+    if t.dtype == torch.float64:
+        return _lib.SIGK_F64
+    raise TypeError(f"signature kernels take float32 or float64 paths, got {t.dtype}")
+
+
+def _check_paths(x: torch.Tensor, name: str) -> None:
+    if not isinstance(x, torch.Tensor):
+        raise TypeError(f"{name} must be a torch.Tensor")
+    if not x.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor (this package has no CPU path)")
+    if x.dim() != 3:
+        raise ValueError(f"{name} must have shape (batch, length, dim), got {tuple(x.shape)}")
+    if x.shape[1] < 2:
+        raise ValueError(f"{name} needs at least 2 points per path, got length {x.shape[1]}")
+    _dtype_code(x)
+
+
+def _stream() -> int:
+    return torch.cuda.current_stream().cuda_stream
+
+
+def _ptr(t):
+    return None if t is None else t.data_ptr()
+
+
+def _workspace(op, nx, ny, lx, ly, d, order, dtype_code, prec, device):
+    n = _lib.lib().sigk_workspace_size(op, nx, ny, lx, ly, d, order, dtype_code, prec)
+    if n == 0:
+        return None, 0
+    return torch.empty(n, dtype=torch.uint8, device=device), n
+
+
+def _broadcast_scale(s, n, like: torch.Tensor):
+    """Scale broadcast of sigpde/torch/kernel.py:38-41 ([1] -> [n])."""
+    if s is None:
+        return None
+    if not isinstance(s, torch.Tensor):
+        s = torch.as_tensor(s, dtype=like.dtype, device=like.device)
+    s = s.reshape(-1).to(device=like.device, dtype=like.dtype)
+    if s.shape[0] == 1:
+        s = s.repeat(n)
+    if s.shape[0] != n:
+        raise ValueError(f"scale has {s.shape[0]} entries, expected 1 or {n}")
+    return s.contiguous()
+
+
+def _is_fused_linear(static_kernel) -> bool:
+    """The linear kernel (ours, or any object named LinearKernel with a float
+    `scale`, such as the reference's) is contracted on the device."""
+    if isinstance(static_kernel, static_kernels.LinearKernel):
+        return True
+    return type(static_kernel).__name__ == "LinearKernel" and isinstance(getattr(static_kernel, "scale", None),
+                                                                          (int, float))
+
+
+def pairwise_inner_product(x, y, static_kernel, dyadic_order):
+    """Coarse increments of each pair: 4-term second difference of the static
+    Gram divided by 4^order (sigpde/torch/kernel.py:13-16)."""
+    ip = static_kernel.pairwise(x, y)
+    ip = ip[:, 1:, 1:] + ip[:, :-1, :-1] - ip[:, 1:, :-1] - ip[:, :-1, 1:]
+    return ip / float(4 ** dyadic_order)
+
+
+def gram_inner_product(x, y, static_kernel, dyadic_order):
+    """Gram version of pairwise_inner_product (sigpde/torch/kernel.py:18-21)."""
+    ip = static_kernel.gram(x, y)
+    ip = ip[:, :, 1:, 1:] + ip[:, :, :-1, :-1] - ip[:, :, 1:, :-1] - ip[:, :, :-1, 1:]
+    return ip / float(4 ** dyadic_order)
+
+
+def log_normalizer(x):
+    """Default robust normaliser f(s) = 2 - 1/(1 + log s) (sigpde/torch/kernel.py:23-24)."""
+    return 2 - 1 / (1 + x.log())
+
+
+def _batches(n, size):
+    size = max(1, int(size))
+    for start in range(0, n, size):
+        yield start, min(n, start + size)
+
+
+class SigPDE:
+    """Untruncated signature kernel by the Goursat PDE (sigpde/torch/kernel.py:26-171)."""
+
+    def __init__(self, static_kernel, dyadic_order=0, precision="fp64"):
+        if precision not in _PREC:
+            raise ValueError(f"precision must be one of {sorted(_PREC)}")
+        if int(dyadic_order) < 0:
+            raise ValueError("dyadic_order must be >= 0")
+        self.static_kernel = static_kernel
+        self.dyadic_order = int(dyadic_order)
+        self.precision = precision
+
+    # ------------------------------------------------------------------ pairwise
+    def pairwise(self, x, y=None, x_scale=None, y_scale=None, max_batch=1000, max_threads=1024):
+        y_scale = x_scale if y is None else y_scale
+        y = x if y is None else y
+        _check_paths(x, "x")
+        _check_paths(y, "y")
+        if y.dtype != x.dtype or y.device != x.device:
+            raise ValueError("x and y must share dtype and device")
+        B = x.shape[0]
+        if y.shape[0] != B:
+            raise ValueError(f"pairwise needs equal batch sizes, got {B} and {y.shape[0]}")
+        if y.shape[2] != x.shape[2]:
+            raise ValueError("x and y must have the same dimension")
+        scaled = x_scale is not None or y_scale is not None
+        sx = _broadcast_scale(x_scale, B, x) if scaled else None
+        sy = _broadcast_scale(y_scale, B, y) if scaled else None
+        result = torch.empty(B, device=x.device, dtype=x.dtype)
+        if B == 0:
+            return result
+        dt = _dtype_code(x)
+        prec = _PREC[self.precision]
+        with torch.cuda.device(x.device):
+            if _is_fused_linear(self.static_kernel):
+                x = x.contiguous()
+                y = y.contiguous()
+                ws, nws = _workspace(_lib.SIGK_OP_PAIRWISE, B, B, x.shape[1], y.shape[1], x.shape[2],
+                                     self.dyadic_order, dt, prec, x.device)
+                _lib.call("sigk_pairwise", _ptr(x), _ptr(y), B, x.shape[1], y.shape[1], x.shape[2], dt,
+                          self.dyadic_order, float(self.static_kernel.scale), _ptr(sx), _ptr(sy), _ptr(result),
+                          prec, _ptr(ws), nws, _stream())
+                return result
+            for s0, s1 in _batches(B, max_batch):
+                inc = pairwise_inner_product(x[s0:s1], y[s0:s1], self.static_kernel, self.dyadic_order)
+                self._solve_pairwise_inc(inc, None if sx is None else sx[s0:s1],
+                                         None if sy is None else sy[s0:s1], result[s0:s1])
+        return result
+
+    def _solve_pairwise_inc(self, inc, sx, sy, out):
+        inc = inc.to(out.dtype)
+        nb, ncx, ncy = inc.shape
+        dt = _dtype_code(inc)
+        prec = _PREC[self.precision]
+        ws, nws = _workspace(_lib.SIGK_OP_PAIRWISE, nb, nb, ncx + 1, ncy + 1, 0, self.dyadic_order, dt, prec,
+                             inc.device)
+        _lib.call("sigk_pairwise_inc", _ptr(inc), nb, ncx, ncy, inc.stride(0), inc.stride(1), inc.stride(2), dt,
+                  self.dyadic_order, _ptr(sx), _ptr(sy), _ptr(out), prec, _ptr(ws), nws, _stream())
+
+    # ------------------------------------------------------------------ gram
+    def gram(self, x, y=None, x_scale=None, y_scale=None, max_batch=1000, max_threads=1024):
+        if y is None:
+            return self._gram_sym(x, x_scale, max_batch)
+        return self._gram(x, y, x_scale, y_scale, max_batch)
+
+    def _gram(self, x, y, x_scale, y_scale, max_batch):
+        _check_paths(x, "x")
+        _check_paths(y, "y")
+        if y.dtype != x.dtype or y.device != x.device:
+            raise ValueError("x and y must share dtype and device")
+        if y.shape[2] != x.shape[2]:
+            raise ValueError("x and y must have the same dimension")
+        Nx, Ny = x.shape[0], y.shape[0]
+        scaled = x_scale is not None or y_scale is not None
+        sx = _broadcast_scale(x_scale, Nx, x) if scaled else None
+        sy = _broadcast_scale(y_scale, Ny, y) if scaled else None
+        result = torch.empty((Nx, Ny), device=x.device, dtype=x.dtype)
+        if Nx == 0 or Ny == 0:
+            return result
+        dt = _dtype_code(x)
+        prec = _PREC[self.precision]
+        with torch.cuda.device(x.device):
+            if _is_fused_linear(self.static_kernel):
+                x = x.contiguous()
+                y = y.contiguous()
+                ws, nws = _workspace(_lib.SIGK_OP_GRAM, Nx, Ny, x.shape[1], y.shape[1], x.shape[2],
+                                     self.dyadic_order, dt, prec, x.device)
+                _lib.call("sigk_gram", _ptr(x), _ptr(y), Nx, Ny, x.shape[1], y.shape[1], x.shape[2], dt,
+                          self.dyadic_order, float(self.static_kernel.scale), _ptr(sx), _ptr(sy), _ptr(result),
+                          prec, _ptr(ws), nws, _stream())
+                return result
+            tile = math.ceil(math.sqrt(max_batch))  # sigpde/torch/kernel.py:68
+            for y0, y1 in _batches(Ny, tile):
+                for x0, x1 in _batches(Nx, tile):
+                    inc = gram_inner_product(x[x0:x1], y[y0:y1], self.static_kernel, self.dyadic_order)
+                    self._solve_gram_inc(inc, None if sx is None else sx[x0:x1], None if sy is None else sy[y0:y1],
+                                         result, x0, y0, False)
+        return result
+
+    def _gram_sym(self, x, x_scale, max_batch):
+        _check_paths(x, "x")
+        N = x.shape[0]
+        sx = _broadcast_scale(x_scale, N, x)
+        result = torch.empty((N, N), device=x.device, dtype=x.dtype)
+        if N == 0:
+            return result
+        dt = _dtype_code(x)
+        prec = _PREC[self.precision]
+        with torch.cuda.device(x.device):
+            if _is_fused_linear(self.static_kernel):
+                x = x.contiguous()
+                ws, nws = _workspace(_lib.SIGK_OP_GRAM_SYM, N, N, x.shape[1], x.shape[1], x.shape[2],
+                                     self.dyadic_order, dt, prec, x.device)
+                _lib.call("sigk_gram_sym", _ptr(x), N, x.shape[1], x.shape[2], dt, self.dyadic_order,
+                          float(self.static_kernel.scale), _ptr(sx), _ptr(result), prec, _ptr(ws), nws, _stream())
+                return result
+            tile = math.ceil(math.sqrt(max_batch))
+            for y0, y1 in _batches(N, tile):
+                for x0, x1 in _batches(N, tile):
+                    if x0 < y0:
+                        continue  # upper tiles are mirrored from the lower ones
+                    inc = gram_inner_product(x[x0:x1], x[y0:y1], self.static_kernel, self.dyadic_order)
+                    self._solve_gram_inc(inc, None if sx is None else sx[x0:x1], None if sx is None else sx[y0:y1],
+                                         result, x0, y0, x0 == y0)
+                    if x0 != y0:
+                        result[y0:y1, x0:x1] = result[x0:x1, y0:y1].t()
+        return result
+
+    def _solve_gram_inc(self, inc, sx, sy, result, x0, y0, symmetric):
+        inc = inc.to(result.dtype)
+        nx, ny, ncx, ncy = inc.shape
+        dt = _dtype_code(inc)
+        prec = _PREC[self.precision]
+        out = result[x0:, y0:]
+        op = _lib.SIGK_OP_GRAM_SYM if symmetric else _lib.SIGK_OP_GRAM
+        ws, nws = _workspace(op, nx, ny, ncx + 1, ncy + 1, 0, self.dyadic_order, dt, prec, inc.device)
+        _lib.call("sigk_gram_inc", _ptr(inc), nx, ny, ncx, ncy, inc.stride(0), inc.stride(1), inc.stride(2),
+                  inc.stride(3), dt, self.dyadic_order, _ptr(sx), _ptr(sy), int(symmetric), _ptr(out),
+                  result.stride(0), prec, _ptr(ws), nws, _stream())
+
+
+class RobustSigPDE:
+    """Robust (tensor-normalised) signature kernel (sigpde/torch/kernel.py:174-301)."""
+
+    def __init__(self, static_kernel, dyadic_order=0, normalizer=None, precision="fp64"):
+        if precision not in _PREC:
+            raise ValueError(f"precision must be one of {sorted(_PREC)}")
+        self.static_kernel = static_kernel
+        self.dyadic_order = int(dyadic_order)
+        self.normalizer = log_normalizer if normalizer is None else normalizer
+        self.precision = precision
+
+    def normalization(self, x, normalizer=None, tol=1e-8, maxit=100, max_batch=1000, max_threads=1024):
+        """Per-path scale lambda with k(lambda x, lambda x) = f(k(x, x)), and
+        lambda = 0 where k(x, x) < 1 (sigpde/torch/kernel.py:180-230)."""
+        return self._normalization(x, normalizer, tol, maxit, max_batch)[0]
+
+    def _normalization(self, x, normalizer, tol, maxit, max_batch, want_iters=False):
+        normalizer = self.normalizer if normalizer is None else normalizer
+        _check_paths(x, "x")
+        N, L, d = x.shape
+        lam = torch.empty(N, device=x.device, dtype=x.dtype)
+        iters = torch.empty(N, device=x.device, dtype=torch.int32) if want_iters else None
+        if N == 0:
+            return lam, iters
+        dt = _dtype_code(x)
+        order = self.dyadic_order
+        with torch.cuda.device(x.device):
+            if _is_fused_linear(self.static_kernel):
+                x = x.contiguous()
+                scale = float(self.static_kernel.scale)
+                ws, nws = _workspace(_lib.SIGK_OP_NORMALIZE, N, N, L, L, d, order, dt, _lib.SIGK_PREC_FP64,
+                                     x.device)
+                if normalizer is log_normalizer:
+                    _lib.call("sigk_normalize", _ptr(x), N, L, d, dt, order, scale, None, None, float(tol),
+                              int(maxit), _ptr(lam), _ptr(iters), _ptr(ws), nws, _stream())
+                    return lam, iters
+                knorm = torch.empty(N, device=x.device, dtype=torch.float64)
+                _lib.call("sigk_self_norms", _ptr(x), N, L, d, dt, order, scale, _ptr(knorm), _ptr(ws), nws,
+                          _stream())
+                fnorm = torch.as_tensor(normalizer(knorm), dtype=torch.float64, device=x.device).contiguous()
+                _lib.call("sigk_normalize", _ptr(x), N, L, d, dt, order, scale, _ptr(knorm), _ptr(fnorm),
+                          float(tol), int(maxit), _ptr(lam), _ptr(iters), _ptr(ws), nws, _stream())
+                return lam, iters
+            # generic static kernel: torch builds the self-increments, in float64
+            for s0, s1 in _batches(N, max_batch):
+                inc = pairwise_inner_product(x[s0:s1], x[s0:s1], self.static_kernel, order).to(torch.float64)
+                nb, nc, _ = inc.shape
+                knorm = torch.empty(nb, device=x.device, dtype=torch.float64)
+                ws, nws = _workspace(_lib.SIGK_OP_NORMALIZE, nb, nb, nc + 1, nc + 1, 0, order, _lib.SIGK_F64,
+                                     _lib.SIGK_PREC_FP64, x.device)
+                _lib.call("sigk_pairwise_inc", _ptr(inc), nb, nc, nc, inc.stride(0), inc.stride(1), inc.stride(2),
+                          _lib.SIGK_F64, order, None, None, _ptr(knorm), _lib.SIGK_PREC_FP64, _ptr(ws), nws,
+                          _stream())
+                knorm = torch.where(torch.isnan(knorm), torch.full_like(knorm, math.inf), knorm)
+                fnorm = torch.as_tensor(normalizer(knorm), dtype=torch.float64, device=x.device).contiguous()
+                lam64 = torch.empty(nb, device=x.device, dtype=torch.float64)
+                _lib.call("sigk_normalize_inc", _ptr(inc), nb, nc, inc.stride(0), inc.stride(1), inc.stride(2),
+                          _lib.SIGK_F64, order, _ptr(knorm), _ptr(fnorm), float(tol), int(maxit), _ptr(lam64),
+                          None if iters is None else _ptr(iters[s0:s1]), _ptr(ws), nws, _stream())
+                lam[s0:s1] = lam64.to(x.dtype)
+        return lam, iters
+
+    def pairwise(self, x, y=None, normalizer=None, tol=1e-8, maxit=100, max_batch=1000, max_threads=1024):
+        """Robust pairwise kernel (sigpde/torch/kernel.py:232-291)."""
+        solver = SigPDE(self.static_kernel, self.dyadic_order, self.precision)
+        lx = self.normalization(x, normalizer, tol, maxit, max_batch, max_threads)
+        if y is None:
+            return solver.pairwise(x, None, lx, None, max_batch, max_threads)
+        ly = self.normalization(y, normalizer, tol, maxit, max_batch, max_threads)
+        return solver.pairwise(x, y, lx, ly, max_batch, max_threads)
+
+    def gram(self, x, y=None, x_scale=None, y_scale=None, normalizer=None, tol=1e-8, maxit=100, max_batch=1000,
+             max_threads=1024):
+        """Robust Gram (sigpde/torch/kernel.py:293-301): given scales skip the normalisation."""
+        xs = self.normalization(x, normalizer, tol, maxit, max_batch, max_threads) if x_scale is None else x_scale
+        if y is None:
+            ys = None
+        else:
+            ys = self.normalization(y, normalizer, tol, maxit, max_batch, max_threads) if y_scale is None else y_scale
+        solver = SigPDE(self.static_kernel, self.dyadic_order, self.precision)
+        return solver.gram(x, y, xs, ys, max_batch, max_threads)

@@ -1,0 +1,103 @@
+"""CPU-only checks: the C ABI library loads and exports every symbol that
+include/sigk.h declares, and the host-side logic of sigpde_b200.torch
+(argument checks, scale broadcasting, generic increment builders, static
+kernels) matches the reference's conventions."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+import torch
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _header_functions():
+    src = open(os.path.join(ROOT, "include", "sigk.h")).read()
+    return re.findall(r"^SIGK_API\s+[\w\s\*]+?\b(sigk_\w+)\s*\(", src, flags=re.M)
+
+
+@pytest.fixture(scope="module")
+def built_lib():
+    from sigpde_b200 import build
+    return build.build()
+
+
+def test_header_declares_the_entry_points():
+    fns = _header_functions()
+    for name in ("sigk_pairwise", "sigk_gram", "sigk_gram_sym", "sigk_normalize", "sigk_self_norms",
+                 "sigk_pairwise_inc", "sigk_gram_inc", "sigk_normalize_inc", "sigk_workspace_size",
+                 "sigk_last_error_string", "sigk_version"):
+        assert name in fns, name
+
+
+def test_library_exports_every_declared_symbol(built_lib):
+    lib = ctypes.CDLL(built_lib)
+    for name in _header_functions():
+        assert hasattr(lib, name), f"{name} declared in include/sigk.h but not exported"
+
+
+def test_binding_table_matches_header(built_lib):
+    from sigpde_b200 import _lib
+    assert set(_lib.SIGNATURES) == set(_header_functions())
+    assert _lib.version().startswith("sigk ")
+    assert _lib.last_error() == ""
+
+
+def test_library_needs_no_cuda_runtime_on_the_loader_path(built_lib):
+    # cudart is linked statically: loading never depends on LD_LIBRARY_PATH
+    deps = os.popen(f"ldd {built_lib}").read()
+    assert "libcudart" not in deps
+
+
+def test_cpu_tensors_are_rejected_before_any_device_call():
+    import sigpde_b200.torch as sig
+    k = sig.SigPDE(sig.kernels.LinearKernel(), 1)
+    x = torch.zeros((2, 5, 3))
+    with pytest.raises(ValueError, match="CUDA"):
+        k.pairwise(x)
+    with pytest.raises(ValueError, match="CUDA"):
+        k.gram(x, x)
+    with pytest.raises(ValueError, match="CUDA"):
+        sig.RobustSigPDE(sig.kernels.LinearKernel()).normalization(x)
+    with pytest.raises(ValueError):
+        sig.SigPDE(sig.kernels.LinearKernel(), 1, precision="fp16")
+
+
+def test_scale_broadcast_rules():
+    from sigpde_b200.torch.kernel import _broadcast_scale
+    like = torch.zeros(1, dtype=torch.float64)
+    assert _broadcast_scale(None, 4, like) is None
+    s = _broadcast_scale(torch.tensor([2.0]), 4, like)
+    assert s.dtype == torch.float64 and s.tolist() == [2.0] * 4
+    with pytest.raises(ValueError):
+        _broadcast_scale(torch.ones(3), 4, like)
+
+
+def test_increment_builders_match_oracle(oracle):
+    from sigpde_b200.torch import gram_inner_product, pairwise_inner_product, kernels
+    x = oracle.brownian(3, 7, 4, 1)
+    y = oracle.brownian(3, 9, 4, 2)
+    X, Y = torch.tensor(x), torch.tensor(y)
+    for order in (0, 2):
+        inc = pairwise_inner_product(X, Y, kernels.LinearKernel(), order).numpy()
+        for b in range(3):
+            np.testing.assert_allclose(inc[b], oracle.increments_linear(x[b], y[b], order), rtol=1e-12, atol=1e-15)
+        g = gram_inner_product(X, Y, kernels.RBFKernel(0.5), order).numpy()
+        want = oracle.second_difference(oracle.static_gram("rbf", x, y, 0.5), order)
+        np.testing.assert_allclose(g, want, rtol=1e-9, atol=1e-13)
+
+
+@pytest.mark.parametrize("name,param", [("LinearKernel", 0.7), ("RBFKernel", 0.9), ("L1RBFKernel", 1.3)])
+def test_static_kernels_match_oracle(oracle, name, param):
+    from sigpde_b200.torch import kernels
+    kind = {"LinearKernel": "linear", "RBFKernel": "rbf", "L1RBFKernel": "l1rbf"}[name]
+    k = getattr(kernels, name)(param)
+    x = oracle.brownian(2, 5, 3, 3)
+    y = oracle.brownian(3, 6, 3, 4)
+    g = k.gram(torch.tensor(x), torch.tensor(y)).numpy()
+    np.testing.assert_allclose(g, oracle.static_gram(kind, x, y, param), rtol=1e-10, atol=1e-13)
+    p = k.pairwise(torch.tensor(x[:2]), torch.tensor(y[:2])).numpy()
+    want = oracle.static_gram(kind, x[:2], y[:2], param)
+    np.testing.assert_allclose(p, np.stack([want[0, 0], want[1, 1]]), rtol=1e-10, atol=1e-13)
