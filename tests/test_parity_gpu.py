@@ -3,7 +3,9 @@ against the float64 oracle and the reference's golden vectors.
 
 Tolerances (stated per test):
   * precision="fp64" (float64 cells, the default): relative error <= 1e-9 per
-    entry against the float64 oracle on the same float32/float64 inputs;
+    entry against the float64 oracle on the same inputs when the output is
+    float64; float32 inputs return float32 results (as the reference does), so
+    their bound is the float32 rounding of the output, 2.5e-7 (2 ulp);
   * precision="fp32" (float32 cells): error normalised by the Cauchy-Schwarz
     bound sqrt(k(x,x) k(y,y)) <= 2e-5 (float32 cells cannot give a pointwise
     bound on near-zero entries: the cells grow to ~sqrt(k(x,x) k(y,y)));
@@ -19,6 +21,7 @@ torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
 RTOL64 = 1e-9
+RTOL_OUT32 = 2.5e-7
 CS32 = 2e-5
 LAM_RTOL = 1e-6
 
@@ -44,6 +47,10 @@ def _order(key):
 def sig():
     import sigpde_b200.torch as sig
     return sig
+
+
+def rtol_for(dt):
+    return RTOL64 if dt is torch.float64 else RTOL_OUT32
 
 
 def assert_rel(got, want, rtol=RTOL64, msg=""):
@@ -101,7 +108,7 @@ def test_golden_config1(sig, golden, oracle):
     assert_rel(got, golden["cfg1_f64_out"], RTOL64, "cfg1 f64")
     x32, y32 = golden["cfg1_f32_x"], golden["cfg1_f32_y"]
     got = host(k.pairwise(cuda(x32), cuda(y32)))
-    assert_rel(got, oracle.pairwise(x32, y32, 1), RTOL64, "cfg1 f32 inputs, fp64 cells")
+    assert_rel(got, oracle.pairwise(x32, y32, 1), RTOL_OUT32, "cfg1 f32 inputs, fp64 cells")
 
 
 def test_golden_robust(sig, golden):
@@ -112,7 +119,6 @@ def test_golden_robust(sig, golden):
         lam = host(sig.RobustSigPDE(lin, o).normalization(cuda(x, torch.float64), normalizer=nrm))
         np.testing.assert_allclose(lam, golden[key + "_out"], rtol=LAM_RTOL, atol=1e-9, err_msg=key)
     for key in _keys(golden, r"(rb_f64_N\d+_L\d+_d\d+_o\d+)_pw_out$"):
-        x, y, y2, o = (cuda(golden[key + s], torch.float64) for s in ("_x", "_y", "_y2")), None, None, None
         x, y, y2 = (cuda(golden[key + s], torch.float64) for s in ("_x", "_y", "_y2"))
         o = _order(key)
         rk = sig.RobustSigPDE(lin, o)
@@ -150,11 +156,11 @@ def test_pairwise_shapes(sig, oracle, B, Lx, Ly, d, o, dt):
     xin, yin = host(X), host(Y)
     k = sig.SigPDE(sig.kernels.LinearKernel(), o)
     got = host(k.pairwise(X, Y))
-    assert_rel(got, oracle.pairwise(xin, yin, o), RTOL64, f"pairwise {B, Lx, Ly, d, o}")
+    assert_rel(got, oracle.pairwise(xin, yin, o), rtol_for(dt), f"pairwise {B, Lx, Ly, d, o}")
     sx = rng.uniform(0.5, 2.0, B)
     sy = rng.uniform(0.5, 2.0, B)
     got = host(k.pairwise(X, Y, cuda(sx, dt), cuda(sy, dt)))
-    assert_rel(got, oracle.pairwise(xin, yin, o, host(cuda(sx, dt)), host(cuda(sy, dt))), RTOL64, "scaled")
+    assert_rel(got, oracle.pairwise(xin, yin, o, host(cuda(sx, dt)), host(cuda(sy, dt))), rtol_for(dt), "scaled")
 
 
 @pytest.mark.parametrize("Nx,Ny,L,d,o", [(3, 4, 10, 3, 1), (5, 2, 64, 8, 2), (4, 4, 140, 2, 2), (7, 7, 9, 2, 3)])
@@ -163,11 +169,12 @@ def test_gram_shapes(sig, oracle, Nx, Ny, L, d, o):
     y = oracle.brownian(Ny, L + 3, d, 4)
     X, Y = cuda(x), cuda(y)
     k = sig.SigPDE(sig.kernels.LinearKernel(), o)
-    assert_rel(host(k.gram(X, Y)), oracle.gram(host(X), host(Y), o), RTOL64, "gram")
-    assert_rel(host(k.gram(X)), oracle.gram(host(X), None, o), RTOL64, "gram sym")
+    assert_rel(host(k.gram(X, Y)), oracle.gram(host(X), host(Y), o), RTOL_OUT32, "gram")
+    assert_rel(host(k.gram(X)), oracle.gram(host(X), None, o), RTOL_OUT32, "gram sym")
     sx = cuda(np.linspace(0.5, 2.0, Nx))
-    assert_rel(host(k.gram(X, None, sx)), oracle.gram(host(X), None, o, host(sx)), RTOL64, "gram sym scaled")
-    assert_rel(host(k.gram(X, Y, sx)), oracle.gram(host(X), host(Y), o, host(sx), None), RTOL64, "gram x scaled")
+    assert_rel(host(k.gram(X, None, sx)), oracle.gram(host(X), None, o, host(sx)), RTOL_OUT32, "gram sym scaled")
+    assert_rel(host(k.gram(X, Y, sx)), oracle.gram(host(X), host(Y), o, host(sx), None), RTOL_OUT32,
+               "gram x scaled")
 
 
 def test_static_scale_and_broadcast(sig, oracle):
@@ -278,12 +285,16 @@ def test_config2_gram_sampled_and_properties(sig, oracle):
     rng = np.random.default_rng(0)
     flat = rng.choice(256 * 256, 128, replace=False)
     want = oracle.gram(host(X), host(Y), 2, pairs=flat)
-    assert_rel(G.reshape(-1)[flat], want, RTOL64, "config2 sampled")
+    assert_rel(G.reshape(-1)[flat], want, RTOL_OUT32, "config2 sampled")
     P = host(k.pairwise(X, Y))
     assert_rel(P, np.diag(G), 1e-12, "pairwise vs diag(gram)")
     S = host(k.gram(X))
     Gxx = host(k.gram(X, X))
     assert_rel(S, Gxx, 1e-12, "gram(x) vs gram(x, x)")
+    # float64 inputs give the float64 result itself
+    G64 = host(k.gram(X.double()[:16], Y.double()[:16]))
+    want = oracle.gram(host(X)[:16], host(Y)[:16], 2)
+    assert_rel(G64, want, RTOL64, "config2 rows, float64 output")
     np.testing.assert_array_equal(S, S.T)
 
 
@@ -293,7 +304,8 @@ def test_long_paths_many_bands(sig, oracle):
     y = oracle.brownian(2, 300, 32, 72)
     X, Y = cuda(x), cuda(y)
     k = sig.SigPDE(sig.kernels.LinearKernel(), 3)
-    assert_rel(host(k.pairwise(X, Y)), oracle.pairwise(host(X), host(Y), 3), 1e-8, "long")
+    assert_rel(host(k.pairwise(X, Y)), oracle.pairwise(host(X), host(Y), 3), RTOL_OUT32, "long")
+    assert_rel(host(k.pairwise(X.double(), Y.double())), oracle.pairwise(host(X), host(Y), 3), 1e-8, "long f64")
 
 
 # ----------------------------------------------------------------------------- edge cases and errors
