@@ -21,8 +21,8 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libsigk.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["sigk_api.cu"]
-HEADERS = ["wave.cuh", "sigk_kernels.cuh"]
+SOURCES = ["sigk_api.cu", "kernels_pair_f64.cu", "kernels_pair_f32.cu", "kernels_norm.cu", "kernels_stream.cu"]
+HEADERS = ["wave.cuh", "sigk_kernels.cuh", "stream.cuh", "dispatch.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",

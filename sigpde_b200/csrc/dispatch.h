@@ -1,0 +1,27 @@
+// dispatch.h -- kernel-variant getters shared by the host code and the
+// translation units that instantiate the kernels (one per file so that nvcc
+// compiles them in parallel).
+#pragma once
+
+#include <stdint.h>
+
+namespace sigk {
+
+struct PairParams;
+struct NormParams;
+struct StreamParams;
+
+using PairFn = void (*)(PairParams);
+using NormFn = void (*)(NormParams);
+using StreamFn = void (*)(StreamParams);
+using DeltaFn = void (*)(const void *, int64_t, int64_t, int64_t, void *);
+
+// f64cells: float64 cells (SIGK_PREC_FP64) vs float32; in64: float64 inputs;
+// R in {2,4,8,16} rows per lane; O = min(order, 4).
+PairFn get_pair_kernel_f64(bool in64, bool from_inc, int R, int O);
+PairFn get_pair_kernel_f32(bool in64, bool from_inc, int R, int O);
+NormFn get_norm_kernel(bool in64, bool from_inc, int R, int O);
+StreamFn get_stream_kernel(bool f64cells, bool in64, int R, int O);
+DeltaFn get_delta_kernel(bool f64cells, bool in64);
+
+} // namespace sigk

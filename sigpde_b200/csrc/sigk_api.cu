@@ -9,13 +9,15 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
 #include <unordered_map>
 
 #include "../../include/sigk.h"
-#include "sigk_kernels.cuh"
+#include "dispatch.h"
+#include "stream.cuh"
 
 namespace sigk {
 namespace {
@@ -69,24 +71,58 @@ int rows_per_coarse_lane(int R, int order)
     return rc > 0 ? rc : 1;
 }
 
+constexpr size_t kMaxStreamStageBytesPerWarp = 32 * 1024;
+
+size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+bool env_flag(const char *name)
+{
+    const char *v = getenv(name);
+    return v && v[0] && v[0] != '0';
+}
+
 struct Plan {
     int R;
     int O;
     int nbands;
     int64_t n, m;
-    size_t stage_bytes_per_warp; // 0 = no staging
-    size_t bnd_bytes;            // total boundary scratch
+    bool stream;                 // streaming kernel (one band, >= 32 column blocks)
+    size_t stage_bytes_per_warp; // shared memory per warp (0 = none)
+    size_t dx_off, dy_off;       // stream: precomputed path differences in the workspace
+    size_t bnd_off;              // multi-band: boundary rows in the workspace
     int64_t bnd_stride;          // elements per warp
+    size_t ws_bytes;             // total workspace
 };
 
-Plan make_plan(int64_t ncx, int64_t ncy, int64_t d, int order, size_t tsize, bool from_inc)
+// Kernel choice and workspace layout for one request.  sigk_workspace_size()
+// and the entry points call this with the same arguments, so the size a
+// caller allocates is the size the launch uses.
+Plan make_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, int64_t d, int order, size_t tsize,
+               bool from_inc)
 {
-    Plan pl;
+    Plan pl{};
     pl.n = ncx << order;
     pl.m = ncy << order;
     pl.O = order >= 4 ? 4 : order;
-    pl.R = pick_rows(pl.n);
-    pl.stage_bytes_per_warp = 0;
+    const int C = order >= 4 ? 8 : (1 << order);
+
+    const int Rs = pick_rows(pl.n);
+    const size_t sbytes = 2 * (size_t)rows_per_coarse_lane(Rs, order) * (size_t)d * 32 * tsize;
+    if (!from_inc && op != SIGK_OP_NORMALIZE && pl.n <= 32 * Rs && pl.m / C >= 32 &&
+        sbytes <= kMaxStreamStageBytesPerWarp && !env_flag("SIGK_NO_STREAM")) {
+        pl.stream = true;
+        pl.R = Rs;
+        pl.nbands = 1;
+        pl.stage_bytes_per_warp = sbytes;
+        const size_t dxb = align256((size_t)nx * ncx * d * tsize);
+        const size_t dyb = op == SIGK_OP_GRAM_SYM ? 0 : align256((size_t)ny * ncy * d * tsize);
+        pl.dx_off = 0;
+        pl.dy_off = op == SIGK_OP_GRAM_SYM ? 0 : dxb;
+        pl.ws_bytes = dxb + dyb;
+        return pl;
+    }
+
+    pl.R = Rs;
     if (!from_inc) {
         // shrink R (more bands) until the dx staging fits; if even R=2 does not fit, read dx from global
         int R = pl.R;
@@ -102,82 +138,22 @@ Plan make_plan(int64_t ncx, int64_t ncy, int64_t d, int order, size_t tsize, boo
         }
     }
     pl.nbands = (int)((pl.n + 32 * pl.R - 1) / (32 * pl.R));
-    pl.bnd_stride = 0;
-    pl.bnd_bytes = 0;
     if (pl.nbands > 1) {
         pl.bnd_stride = ((pl.m + 1 + 31) / 32) * 32;
-        pl.bnd_bytes = (size_t)warp_cap() * (size_t)pl.bnd_stride * tsize;
+        pl.bnd_off = 0;
+        pl.ws_bytes = (size_t)warp_cap() * (size_t)pl.bnd_stride * tsize;
     }
     return pl;
 }
 
-// ------------------------------------------------------------------ kernel tables
-using PairFn = void (*)(PairParams);
-using NormFn = void (*)(NormParams);
-
-template <typename T, typename TIN, int R, bool FI>
-PairFn pair_by_o(int O)
-{
-    switch (O) {
-    case 0: return pair_kernel<T, TIN, R, 0, FI>;
-    case 1: return pair_kernel<T, TIN, R, 1, FI>;
-    case 2: return pair_kernel<T, TIN, R, 2, FI>;
-    case 3: return pair_kernel<T, TIN, R, 3, FI>;
-    default: return pair_kernel<T, TIN, R, 4, FI>;
-    }
-}
-
-template <typename T, typename TIN, bool FI>
-PairFn pair_by_r(int R, int O)
-{
-    switch (R) {
-    case 2: return pair_by_o<T, TIN, 2, FI>(O);
-    case 4: return pair_by_o<T, TIN, 4, FI>(O);
-    case 8: return pair_by_o<T, TIN, 8, FI>(O);
-    default: return pair_by_o<T, TIN, 16, FI>(O);
-    }
-}
-
 PairFn pick_pair(int precision, int dtype, bool from_inc, int R, int O)
 {
-    const bool f64cells = (precision == SIGK_PREC_FP64);
     const bool in64 = (dtype == SIGK_F64);
-    if (f64cells) {
-        if (in64) return from_inc ? pair_by_r<double, double, true>(R, O) : pair_by_r<double, double, false>(R, O);
-        return from_inc ? pair_by_r<double, float, true>(R, O) : pair_by_r<double, float, false>(R, O);
-    }
-    if (in64) return from_inc ? pair_by_r<float, double, true>(R, O) : pair_by_r<float, double, false>(R, O);
-    return from_inc ? pair_by_r<float, float, true>(R, O) : pair_by_r<float, float, false>(R, O);
+    return precision == SIGK_PREC_FP64 ? get_pair_kernel_f64(in64, from_inc, R, O)
+                                       : get_pair_kernel_f32(in64, from_inc, R, O);
 }
 
-template <typename TIN, int R, bool FI>
-NormFn norm_by_o(int O)
-{
-    switch (O) {
-    case 0: return normalize_kernel<TIN, R, 0, FI>;
-    case 1: return normalize_kernel<TIN, R, 1, FI>;
-    case 2: return normalize_kernel<TIN, R, 2, FI>;
-    case 3: return normalize_kernel<TIN, R, 3, FI>;
-    default: return normalize_kernel<TIN, R, 4, FI>;
-    }
-}
-
-template <typename TIN, bool FI>
-NormFn norm_by_r(int R, int O)
-{
-    switch (R) {
-    case 2: return norm_by_o<TIN, 2, FI>(O);
-    case 4: return norm_by_o<TIN, 4, FI>(O);
-    case 8: return norm_by_o<TIN, 8, FI>(O);
-    default: return norm_by_o<TIN, 16, FI>(O);
-    }
-}
-
-NormFn pick_norm(int dtype, bool from_inc, int R, int O)
-{
-    if (dtype == SIGK_F64) return from_inc ? norm_by_r<double, true>(R, O) : norm_by_r<double, false>(R, O);
-    return from_inc ? norm_by_r<float, true>(R, O) : norm_by_r<float, false>(R, O);
-}
+NormFn pick_norm(int dtype, bool from_inc, int R, int O) { return get_norm_kernel(dtype == SIGK_F64, from_inc, R, O); }
 
 // ------------------------------------------------------------------ launching
 struct OccKey {
@@ -273,9 +249,9 @@ size_t tsize_of(int precision) { return precision == SIGK_PREC_FP64 ? 8 : 4; }
 
 int check_ws(const Plan &pl, void *ws, size_t ws_bytes)
 {
-    if (pl.bnd_bytes == 0) return SIGK_OK;
-    if (!ws || ws_bytes < pl.bnd_bytes)
-        return fail(SIGK_ENOMEM, "workspace of %zu bytes needed (got %zu)", pl.bnd_bytes, ws ? ws_bytes : 0);
+    if (pl.ws_bytes == 0) return SIGK_OK;
+    if (!ws || ws_bytes < pl.ws_bytes)
+        return fail(SIGK_ENOMEM, "workspace of %zu bytes needed (got %zu)", pl.ws_bytes, ws ? ws_bytes : 0);
     if (((uintptr_t)ws & 15) != 0) return fail(SIGK_EINVAL, "workspace must be 16-byte aligned");
     return SIGK_OK;
 }
@@ -295,8 +271,58 @@ int run_pairs(int op, const void *x, const void *y, int64_t nx, int64_t ny, int6
         (st = check_dev(sx, "scale_x", true)) || (st = check_dev(sy, "scale_y", true)))
         return st;
     const size_t ts = tsize_of(precision);
-    Plan pl = make_plan(lx - 1, ly - 1, d, order, ts, false);
+    const int64_t nitems = op == kOpPairwise ? nx : (op == kOpGram ? nx * ny : nx * (nx + 1) / 2);
+    Plan pl = make_plan(op, nx, ny, lx - 1, ly - 1, d, order, ts, false);
     if ((st = check_ws(pl, ws, ws_bytes))) return st;
+    const bool in64 = dtype == SIGK_F64;
+    const bool f64 = precision == SIGK_PREC_FP64;
+
+    if (pl.stream) {
+        unsigned char *wsb = reinterpret_cast<unsigned char *>(ws);
+        void *dx = wsb + pl.dx_off;
+        void *dy = wsb + pl.dy_off;
+        DeltaFn delta = get_delta_kernel(f64, in64);
+        const int nsm = sm_count();
+        auto run_delta = [&](const void *src, int64_t npaths, int64_t len, void *dst) -> int {
+            const int64_t total = npaths * (len - 1) * d;
+            int64_t blocks = (total + 255) / 256;
+            if (blocks > (int64_t)nsm * 8) blocks = (int64_t)nsm * 8;
+            delta<<<(unsigned)blocks, 256, 0, stream>>>(src, npaths, len, d, dst);
+            cudaError_t e = cudaGetLastError();
+            return e == cudaSuccess ? SIGK_OK : cuda_fail(e, "delta kernel launch");
+        };
+        if ((st = run_delta(x, nx, lx, dx))) return st;
+        if (op != kOpGramSym && (st = run_delta(y, ny, ly, dy))) return st;
+
+        StreamParams sp{};
+        sp.op = op;
+        sp.dx = dx;
+        sp.dy = op == kOpGramSym ? dx : dy;
+        sp.nx = nx;
+        sp.ny = ny;
+        sp.ncx = lx - 1;
+        sp.ncy = ly - 1;
+        sp.d = d;
+        sp.order = order;
+        sp.fscale = static_scale * std::ldexp(1.0, -2 * order);
+        sp.sx = sx;
+        sp.sy = sy;
+        sp.out = out;
+        sp.out_ld = out_ld;
+        sp.nitems = nitems;
+        StreamFn fn = get_stream_kernel(f64, in64, pl.R, pl.O);
+        const size_t smem = pl.stage_bytes_per_warp * kWarpsPerBlock;
+        int nb = 0;
+        if ((st = blocks_per_sm((const void *)fn, smem, &nb))) return st;
+        int64_t nwarps = (int64_t)nsm * nb * kWarpsPerBlock;
+        if (nwarps > nitems) nwarps = nitems;
+        sp.per_warp = (nitems + nwarps - 1) / nwarps;
+        const int64_t used = (nitems + sp.per_warp - 1) / sp.per_warp;
+        const int64_t blocks = (used + kWarpsPerBlock - 1) / kWarpsPerBlock;
+        fn<<<(unsigned)blocks, kWarpsPerBlock * 32, smem, stream>>>(sp);
+        cudaError_t e = cudaGetLastError();
+        return e == cudaSuccess ? SIGK_OK : cuda_fail(e, "stream kernel launch");
+    }
 
     PairParams p{};
     p.op = op;
@@ -313,8 +339,8 @@ int run_pairs(int op, const void *x, const void *y, int64_t nx, int64_t ny, int6
     p.sy = sy;
     p.out = out;
     p.out_ld = out_ld;
-    p.nitems = op == kOpPairwise ? nx : (op == kOpGram ? nx * ny : nx * (nx + 1) / 2);
-    p.bnd = pl.bnd_bytes ? ws : nullptr;
+    p.nitems = nitems;
+    p.bnd = pl.nbands > 1 ? ws : nullptr;
     p.bnd_stride = pl.bnd_stride;
     p.stage_smem = pl.stage_bytes_per_warp > 0;
     PairFn fn = pick_pair(precision, dtype, false, pl.R, pl.O);
@@ -335,15 +361,17 @@ const char *sigk_last_error_string(void) { return g_last_error.c_str(); }
 size_t sigk_workspace_size(int op, int64_t n_x, int64_t n_y, int64_t len_x, int64_t len_y, int64_t dim, int order,
                            int dtype, int precision)
 {
-    (void)n_x;
-    (void)n_y;
     (void)dtype;
-    if (len_x < 2 || len_y < 2 || order < 0 || order > 12 || dim < 0) return 0;
+    if (len_x < 2 || len_y < 2 || order < 0 || order > 12 || dim < 0 || n_x < 1 || n_y < 1) return 0;
     if (op == SIGK_OP_NORMALIZE) precision = SIGK_PREC_FP64;
-    if (op == SIGK_OP_GRAM_SYM || op == SIGK_OP_NORMALIZE) len_y = len_x;
+    if (op == SIGK_OP_GRAM_SYM || op == SIGK_OP_NORMALIZE) {
+        len_y = len_x;
+        n_y = n_x;
+    }
+    if (op == SIGK_OP_PAIRWISE) n_y = n_x;
     // dim == 0 selects the plan of the *_inc entry points (no dx staging)
-    Plan pl = make_plan(len_x - 1, len_y - 1, dim > 0 ? dim : 1, order, tsize_of(precision), dim == 0);
-    return pl.bnd_bytes;
+    Plan pl = make_plan(op, n_x, n_y, len_x - 1, len_y - 1, dim > 0 ? dim : 1, order, tsize_of(precision), dim == 0);
+    return pl.ws_bytes;
 }
 
 int sigk_pairwise(const void *x, const void *y, int64_t batch, int64_t len_x, int64_t len_y, int64_t dim, int dtype,
@@ -393,7 +421,7 @@ static int run_normalize(const void *x, const void *inc, int64_t n, int64_t nc, 
         (st = check_dev(fnorm, "fnorm", true)) || (st = check_dev(iters, "iters", true)))
         return st;
     if (fnorm && !knorm) return fail(SIGK_EINVAL, "fnorm given without knorm");
-    Plan pl = make_plan(nc, nc, from_inc ? 1 : d, order, 8, from_inc);
+    Plan pl = make_plan(SIGK_OP_NORMALIZE, n, n, nc, nc, from_inc ? 1 : d, order, 8, from_inc);
     if ((st = check_ws(pl, ws, ws_bytes))) return st;
     NormParams p{};
     p.x = x;
@@ -412,7 +440,7 @@ static int run_normalize(const void *x, const void *inc, int64_t n, int64_t nc, 
     p.maxit = maxit;
     p.lam = lam;
     p.iters = iters;
-    p.bnd = pl.bnd_bytes ? ws : nullptr;
+    p.bnd = pl.nbands > 1 ? ws : nullptr;
     p.bnd_stride = pl.bnd_stride;
     p.stage_smem = pl.stage_bytes_per_warp > 0;
     NormFn fn = pick_norm(dtype, from_inc, pl.R, pl.O);
@@ -434,7 +462,7 @@ int sigk_self_norms(const void *x, int64_t n, int64_t len, int64_t dim, int dtyp
     if (n < 1 || len < 2 || dim < 1) return fail(SIGK_EINVAL, "bad shape (n=%lld len=%lld dim=%lld)",
                                                  (long long)n, (long long)len, (long long)dim);
     if ((st = check_dev(x, "x", false))) return st;
-    Plan pl = make_plan(len - 1, len - 1, dim, order, 8, false);
+    Plan pl = make_plan(SIGK_OP_NORMALIZE, n, n, len - 1, len - 1, dim, order, 8, false);
     if ((st = check_ws(pl, workspace, workspace_bytes))) return st;
     NormParams p{};
     p.x = x;
@@ -448,7 +476,7 @@ int sigk_self_norms(const void *x, int64_t n, int64_t len, int64_t dim, int dtyp
     p.tol = 0;
     p.maxit = 0;
     p.lam = nullptr;
-    p.bnd = pl.bnd_bytes ? workspace : nullptr;
+    p.bnd = pl.nbands > 1 ? workspace : nullptr;
     p.bnd_stride = pl.bnd_stride;
     p.stage_smem = pl.stage_bytes_per_warp > 0;
     NormFn fn = pick_norm(dtype, false, pl.R, pl.O);
@@ -483,7 +511,7 @@ static int run_inc(int op, const void *inc, int64_t nx, int64_t ny, int64_t ncx,
     if ((st = check_dev(inc, "inc", false)) || (st = check_dev(out, "out", false)) ||
         (st = check_dev(sx, "scale_x", true)) || (st = check_dev(sy, "scale_y", true)))
         return st;
-    Plan pl = make_plan(ncx, ncy, 1, order, tsize_of(precision), true);
+    Plan pl = make_plan(op, nx, ny, ncx, ncy, 1, order, tsize_of(precision), true);
     if ((st = check_ws(pl, ws, ws_bytes))) return st;
     PairParams p{};
     p.op = op;
@@ -504,7 +532,7 @@ static int run_inc(int op, const void *inc, int64_t nx, int64_t ny, int64_t ncx,
     p.out = out;
     p.out_ld = out_ld;
     p.nitems = op == kOpPairwise ? nx : (op == kOpGram ? nx * ny : nx * (nx + 1) / 2);
-    p.bnd = pl.bnd_bytes ? ws : nullptr;
+    p.bnd = pl.nbands > 1 ? ws : nullptr;
     p.bnd_stride = pl.bnd_stride;
     p.stage_smem = 0;
     PairFn fn = pick_pair(precision, dtype, true, pl.R, pl.O);

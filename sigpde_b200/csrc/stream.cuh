@@ -23,8 +23,10 @@ namespace sigk {
 
 // dx[p][c][k] = T(x[p][c+1][k]) - T(x[p][c][k]) for all paths p.
 template <typename T, typename TIN>
-__global__ void delta_kernel(const TIN *__restrict__ x, int64_t npaths, int64_t len, int64_t d, T *__restrict__ dx)
+__global__ void delta_kernel(const void *x_, int64_t npaths, int64_t len, int64_t d, void *dx_)
 {
+    const TIN *__restrict__ x = reinterpret_cast<const TIN *>(x_);
+    T *__restrict__ dx = reinterpret_cast<T *>(dx_);
     const int64_t per_path = (len - 1) * d;
     const int64_t total = npaths * per_path;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
@@ -168,7 +170,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_kernel(StreamParam
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     const T l = left[r];
-                    const T v = fma(l + up, A[BS::rc_of(r)], -(dg * B[BS::rc_of(r)]));
+                    const T v = stencil_cell(dg, up, l, A[BS::rc_of(r)], B[BS::rc_of(r)]);
                     dg = l;
                     up = v;
                     left[r] = v;

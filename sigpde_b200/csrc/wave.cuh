@@ -34,13 +34,43 @@ __device__ __forceinline__ T ld_in(const T *p)
     return __ldg(p);
 }
 
-// A = 1 + c/2 + c^2/12, B = 1 - c^2/12
+// Stencil coefficients of one coarse cell and the cell update
+//   K11 = (K10 + K01) * A - K00 * B,   A = 1 + a,  B = 1 - b,
+//   a = c/2 + c^2/12,  b = c^2/12.
+// float64 cells hold (A, B) and update in 3 operations.  float32 cells hold
+// (a, b): rounding A = 1 + c/2 to float32 keeps only ~2^-24 / c of the
+// increment's relative precision (c shrinks like 4^-order), which made float32
+// results ~50x less accurate than the reference's float64-arithmetic /
+// float32-storage cells; the delta form
+//   K11 = (s - K00) + s * a + K00 * b,  s = K10 + K01
+// keeps c at full precision for one extra operation per cell.
 template <typename T>
 __device__ __forceinline__ void stencil_coefs(T c, T &A, T &B)
 {
     const T c2 = c * c;
     A = fma(c2, T(1.0 / 12.0), fma(c, T(0.5), T(1)));
     B = fma(c2, T(-1.0 / 12.0), T(1));
+}
+
+template <>
+__device__ __forceinline__ void stencil_coefs<float>(float c, float &a, float &b)
+{
+    const float c2 = c * c;
+    b = c2 * (1.0f / 12.0f);
+    a = fmaf(c, 0.5f, b);
+}
+
+template <typename T>
+__device__ __forceinline__ T stencil_cell(T k00, T k01, T k10, T A, T B)
+{
+    return fma(k10 + k01, A, -(k00 * B));
+}
+
+template <>
+__device__ __forceinline__ float stencil_cell<float>(float k00, float k01, float k10, float a, float b)
+{
+    const float s = k10 + k01;
+    return fmaf(s, a, fmaf(k00, b, s - k00));
 }
 
 // Compile-time shape of one lane's block.
@@ -227,7 +257,7 @@ __device__ T warp_solve(const SolveGeom &g, Src &src, T *bnd)
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
                         const T l = left[r];
-                        const T v = fma(l + up, A[BS::rc_of(r)], -(dg * B[BS::rc_of(r)]));
+                        const T v = stencil_cell(dg, up, l, A[BS::rc_of(r)], B[BS::rc_of(r)]);
                         dg = l;
                         up = v;
                         left[r] = v;
