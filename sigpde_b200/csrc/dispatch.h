@@ -14,14 +14,19 @@ struct StreamParams;
 using PairFn = void (*)(PairParams);
 using NormFn = void (*)(NormParams);
 using StreamFn = void (*)(StreamParams);
-using DeltaFn = void (*)(const void *, int64_t, int64_t, int64_t, void *);
+using DeltaFn = void (*)(const void *, int64_t, int64_t, int64_t, int64_t, double, const void *, void *);
 
 // f64cells: float64 cells (SIGK_PREC_FP64) vs float32; in64: float64 inputs;
 // R in {2,4,8,16} rows per lane; O = min(order, 4).
 PairFn get_pair_kernel_f64(bool in64, bool from_inc, int R, int O);
 PairFn get_pair_kernel_f32(bool in64, bool from_inc, int R, int O);
 NormFn get_norm_kernel(bool in64, bool from_inc, int R, int O);
-StreamFn get_stream_kernel(bool f64cells, bool in64, int R, int O);
+// D: dimension padded to a power of two in {2,...,32}; returns null unless
+// the lane's register tile (coarse rows per lane) * D <= 32.
+StreamFn get_stream_reg_kernel(bool f64cells, int R, int O, int D);
+StreamFn get_stream_reg_kernel_f64(int R, int O, int D);
+StreamFn get_stream_reg_kernel_f32(int R, int O, int D);
+StreamFn get_stream_smem_kernel(bool f64cells, int R, int O);
 DeltaFn get_delta_kernel(bool f64cells, bool in64);
 
 } // namespace sigk

@@ -87,6 +87,7 @@ struct Plan {
     int nbands;
     int64_t n, m;
     bool stream;                 // streaming kernel (one band, >= 32 column blocks)
+    int D;                       // stream: padded dimension of the register variant, 0 = shared-memory variant
     size_t stage_bytes_per_warp; // shared memory per warp (0 = none)
     size_t dx_off, dy_off;       // stream: precomputed path differences in the workspace
     size_t bnd_off;              // multi-band: boundary rows in the workspace
@@ -107,17 +108,23 @@ Plan make_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, int64_t
     const int C = order >= 4 ? 8 : (1 << order);
 
     const int Rs = pick_rows(pl.n);
-    const size_t sbytes = 2 * (size_t)rows_per_coarse_lane(Rs, order) * (size_t)d * 32 * tsize;
+    const int rc = rows_per_coarse_lane(Rs, order);
+    int Dp = 2;
+    while (Dp < d) Dp <<= 1;
+    const bool reg_ok = rc * Dp <= 32 && !env_flag("SIGK_NO_REG_DX");
+    const size_t sbytes = reg_ok ? 0 : 2 * (size_t)rc * (size_t)d * 32 * tsize;
     if (!from_inc && op != SIGK_OP_NORMALIZE && pl.n <= 32 * Rs && pl.m / C >= 32 &&
         sbytes <= kMaxStreamStageBytesPerWarp && !env_flag("SIGK_NO_STREAM")) {
         pl.stream = true;
         pl.R = Rs;
+        pl.D = reg_ok ? Dp : 0;
         pl.nbands = 1;
         pl.stage_bytes_per_warp = sbytes;
-        const size_t dxb = align256((size_t)nx * ncx * d * tsize);
-        const size_t dyb = op == SIGK_OP_GRAM_SYM ? 0 : align256((size_t)ny * ncy * d * tsize);
+        const int64_t dp = reg_ok ? Dp : d;
+        const size_t dxb = align256((size_t)nx * ncx * dp * tsize);
+        const size_t dyb = align256((size_t)ny * ncy * dp * tsize);
         pl.dx_off = 0;
-        pl.dy_off = op == SIGK_OP_GRAM_SYM ? 0 : dxb;
+        pl.dy_off = dxb;
         pl.ws_bytes = dxb + dyb;
         return pl;
     }
@@ -283,34 +290,50 @@ int run_pairs(int op, const void *x, const void *y, int64_t nx, int64_t ny, int6
         void *dy = wsb + pl.dy_off;
         DeltaFn delta = get_delta_kernel(f64, in64);
         const int nsm = sm_count();
-        auto run_delta = [&](const void *src, int64_t npaths, int64_t len, void *dst) -> int {
-            const int64_t total = npaths * (len - 1) * d;
+        const int64_t dp = pl.D ? pl.D : d;
+        auto run_delta = [&](const void *src, int64_t npaths, int64_t len, double f, const void *sc,
+                             void *dst) -> int {
+            const int64_t total = npaths * (len - 1) * dp;
             int64_t blocks = (total + 255) / 256;
             if (blocks > (int64_t)nsm * 8) blocks = (int64_t)nsm * 8;
-            delta<<<(unsigned)blocks, 256, 0, stream>>>(src, npaths, len, d, dst);
+            delta<<<(unsigned)blocks, 256, 0, stream>>>(src, npaths, len, d, dp, f, sc, dst);
             cudaError_t e = cudaGetLastError();
             return e == cudaSuccess ? SIGK_OK : cuda_fail(e, "delta kernel launch");
         };
-        if ((st = run_delta(x, nx, lx, dx))) return st;
-        if (op != kOpGramSym && (st = run_delta(y, ny, ly, dy))) return st;
+        // static scale * 4^-order and scale_x go into dX, scale_y into dY; the
+        // symmetric Gram reads one buffer for both sides, scaled by scale_x
+        const double fs = static_scale * std::ldexp(1.0, -2 * order);
+        if (op == kOpGramSym) {
+            // f goes on the row side only, so a second buffer is needed unless f == 1
+            if (fs == 1.0) {
+                if ((st = run_delta(x, nx, lx, 1.0, sx, dx))) return st;
+                dy = dx;
+            } else {
+                if ((st = run_delta(x, nx, lx, fs, sx, dx))) return st;
+                if ((st = run_delta(x, nx, lx, 1.0, sx, dy))) return st;
+            }
+        } else {
+            if ((st = run_delta(x, nx, lx, fs, sx, dx))) return st;
+            if ((st = run_delta(y, ny, ly, 1.0, sy, dy))) return st;
+        }
 
         StreamParams sp{};
         sp.op = op;
+        sp.in64 = in64;
         sp.dx = dx;
-        sp.dy = op == kOpGramSym ? dx : dy;
+        sp.dy = dy;
         sp.nx = nx;
         sp.ny = ny;
         sp.ncx = lx - 1;
         sp.ncy = ly - 1;
         sp.d = d;
+        sp.dp = dp;
         sp.order = order;
-        sp.fscale = static_scale * std::ldexp(1.0, -2 * order);
-        sp.sx = sx;
-        sp.sy = sy;
         sp.out = out;
         sp.out_ld = out_ld;
         sp.nitems = nitems;
-        StreamFn fn = get_stream_kernel(f64, in64, pl.R, pl.O);
+        StreamFn fn = pl.D ? get_stream_reg_kernel(f64, pl.R, pl.O, pl.D) : get_stream_smem_kernel(f64, pl.R, pl.O);
+        if (!fn) return fail(SIGK_EUNSUPPORTED, "no stream kernel for R=%d O=%d D=%d", pl.R, pl.O, pl.D);
         const size_t smem = pl.stage_bytes_per_warp * kWarpsPerBlock;
         int nb = 0;
         if ((st = blocks_per_sm((const void *)fn, smem, &nb))) return st;

@@ -7,55 +7,237 @@
 // that owns E pairs runs E * nsteps + 31 steps instead of E * (nsteps + 31).
 //
 // Preconditions (checked on the host): one band (refined rows <= 32 R) and
-// nsteps >= 32 column blocks per pair.  The second condition makes the double
-// buffer of staged dx rows safe: the buffer for pair k is written (by the
-// whole warp, when lane 0 starts pair k) at least one step after lane 31
-// finished pair k - 2, the last reader of that buffer.
+// nsteps >= 32 column blocks per pair.
 //
 // Increments come from path differences precomputed in T by delta_kernel
-// (float64 differences of float32 points are exact), so the inner loop does
-// no conversions: c(ci, cj) = fscale * <dX[ci], dY[cj]>.
+// (float64 differences of float32 points are exact) with all scale factors
+// folded in, so the inner loop does no conversions and no scaling:
+// c(ci, cj) = <dX[ci], dY[cj]>.
+//
+// Two variants:
+//   stream_reg_kernel  -- the lane's dx rows (RC coarse rows x D dims, D the
+//                         dimension padded to a power of two) live in
+//                         registers and are reloaded only when the lane's x
+//                         path changes (rarely, for a row-major Gram);
+//   stream_smem_kernel -- for RC * D > 32: dx rows double-buffered in shared
+//                         memory.  The buffer for pair k is written (by the
+//                         whole warp, when lane 0 starts pair k) at least one
+//                         step after lane 31 finished pair k - 2, its last
+//                         reader, because nsteps >= 32.
 #pragma once
 
 #include "sigk_kernels.cuh"
 
 namespace sigk {
 
-// dx[p][c][k] = T(x[p][c+1][k]) - T(x[p][c][k]) for all paths p.
+// dx[p][k][c] = T(x[p][c+1][k]) - T(x[p][c][k]) for all paths p, stored
+// dimension-major: the lanes of a warp read neighbouring coarse columns c of
+// one dimension k in the same instruction (lane l is one column behind lane
+// l-1), so a load touches 2 cache lines instead of 16.  Dimensions d <= k < dp
+// are written as zeros (dp = padded dimension of the register variant), so the
+// inner loop needs no bound checks.
+// Every row is multiplied by f * s[p] (s may be null): folding the static
+// scale, 4^-order and the per-path scales into the differences leaves the
+// stream kernels nothing to scale, since <f s_i dx_i, s_j dy_j> is the scaled
+// increment f * s_i * s_j * <dx_i, dy_j> of sigpde/cuda_gram_kernels.py:52,60.
 template <typename T, typename TIN>
-__global__ void delta_kernel(const void *x_, int64_t npaths, int64_t len, int64_t d, void *dx_)
+__global__ void delta_kernel(const void *x_, int64_t npaths, int64_t len, int64_t d, int64_t dp, double f,
+                             const void *s_, void *dx_)
 {
     const TIN *__restrict__ x = reinterpret_cast<const TIN *>(x_);
+    const TIN *__restrict__ sc = reinterpret_cast<const TIN *>(s_);
     T *__restrict__ dx = reinterpret_cast<T *>(dx_);
-    const int64_t per_path = (len - 1) * d;
+    const int64_t nc = len - 1;
+    const int64_t per_path = nc * dp;
     const int64_t total = npaths * per_path;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
          e += (int64_t)gridDim.x * blockDim.x) {
         const int64_t p = e / per_path;
-        const int64_t r = e - p * per_path; // c * d + k
-        const TIN *xp = x + p * len * d;
-        dx[e] = T(xp[r + d]) - T(xp[r]);
+        const int64_t r = e - p * per_path; // k * nc + c
+        const int64_t k = r / nc;
+        const int64_t c = r - k * nc;
+        if (k < d) {
+            const TIN *xp = x + p * len * d + c * d + k;
+            const T g = sc ? T(f * (double)sc[p]) : T(f);
+            dx[e] = (T(xp[d]) - T(xp[0])) * g;
+        } else {
+            dx[e] = T(0);
+        }
     }
 }
 
 struct StreamParams {
     int op;             // kOpPairwise / kOpGram / kOpGramSym
-    const void *dx;     // (nx, ncx, d) in T
-    const void *dy;     // (ny, ncy, d) in T
+    int in64;           // 1: scales and output are float64, 0: float32
+    const void *dx;     // (nx, dp, ncx) in T, scaled (see delta_kernel)
+    const void *dy;     // (ny, dp, ncy) in T, scaled
     int64_t nx, ny;
     int64_t ncx, ncy, d;
+    int64_t dp;         // padded dimension of dx / dy (d for the shared-memory variant)
     int order;
-    double fscale;
-    const void *sx;
-    const void *sy;
     void *out;
     int64_t out_ld;
     int64_t nitems;
     int64_t per_warp;   // items per warp (contiguous run)
 };
 
-template <typename T, typename TIN, int R, int O>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_kernel(StreamParams p)
+__device__ __forceinline__ void stream_decode(const StreamParams &p, int64_t item, int64_t &xi, int64_t &yj)
+{
+    if (p.op == kOpPairwise) {
+        xi = item;
+        yj = item;
+    } else if (p.op == kOpGram) {
+        xi = item / p.ny;
+        yj = item - xi * p.ny;
+    } else {
+        tri_decode(item, xi, yj);
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void stream_store(const StreamParams &p, int64_t item, int64_t xi, int64_t yj, T v)
+{
+    int64_t i0, i1 = -1;
+    if (p.op == kOpPairwise) {
+        i0 = item;
+    } else {
+        i0 = xi * p.out_ld + yj;
+        if (p.op == kOpGramSym && xi != yj) i1 = yj * p.out_ld + xi;
+    }
+    if (p.in64) {
+        double *o = reinterpret_cast<double *>(p.out);
+        o[i0] = double(v);
+        if (i1 >= 0) o[i1] = double(v);
+    } else {
+        float *o = reinterpret_cast<float *>(p.out);
+        o[i0] = float(v);
+        if (i1 >= 0) o[i1] = float(v);
+    }
+}
+
+// One R x C block of cells: left[] holds the lane's column on entry and the
+// new column on exit; top[] is the row above (from lane l-1), corner the cell
+// above-left; bot[] receives the block's bottom row.
+template <typename T, int R, int O>
+__device__ __forceinline__ void stream_block(T (&left)[R], const T (&top)[BlockShape<R, O>::C], T corner,
+                                             const T (&A)[BlockShape<R, O>::RC], const T (&B)[BlockShape<R, O>::RC],
+                                             T (&bot)[BlockShape<R, O>::C])
+{
+    using BS = BlockShape<R, O>;
+#pragma unroll
+    for (int c = 0; c < BS::C; ++c) {
+        T up = top[c];
+        T dg = (c == 0) ? corner : top[c - 1];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const T l = left[r];
+            const T v = stencil_cell(dg, up, l, A[BS::rc_of(r)], B[BS::rc_of(r)]);
+            dg = l;
+            up = v;
+            left[r] = v;
+        }
+        bot[c] = up;
+    }
+}
+
+template <typename T, int R>
+__device__ __forceinline__ T pick_row(const T (&left)[R], int rstar)
+{
+    T v = left[0];
+#pragma unroll
+    for (int r = 1; r < R; ++r)
+        if (r == rstar) v = left[r];
+    return v;
+}
+
+template <typename T, int R, int O, int D>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_reg_kernel(StreamParams p)
+{
+    using BS = BlockShape<R, O>;
+    constexpr int C = BS::C;
+    constexpr int RC = BS::RC;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int64_t gwarp = (int64_t)blockIdx.x * kWarpsPerBlock + wib;
+    const int64_t first = gwarp * p.per_warp;
+    if (first >= p.nitems) return; // warp-uniform
+    const int cnt = (int)((p.nitems - first) < p.per_warp ? (p.nitems - first) : p.per_warp);
+    const T *dX = reinterpret_cast<const T *>(p.dx);
+    const T *dY = reinterpret_cast<const T *>(p.dy);
+    const int ncx = (int)p.ncx, ncy = (int)p.ncy;
+    const int n = ncx << p.order;
+    const int nsteps = (ncy << p.order) / C;
+    const int ci0 = (lane * R) >> p.order; // first coarse row of this lane
+    const int lstar = (n - 1) / R, rstar = (n - 1) % R;
+
+    T dx[RC][D];
+    int64_t cur_x = -1;
+    T left[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) left[r] = T(1);
+    T bot[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) bot[c] = T(1);
+    T corner_next = T(1);
+    int q = 0, k = 0;
+    int64_t item = first, xi = 0, yj = 0;
+    const T *dyp = dY;
+
+    const int total = cnt * nsteps + 31;
+    for (int s = 0; s < total; ++s) {
+        T top[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) top[c] = __shfl_up_sync(kFullMask, bot[c], 1);
+        if (lane == 0) {
+#pragma unroll
+            for (int c = 0; c < C; ++c) top[c] = T(1);
+        }
+        if (s >= lane && k < cnt) {
+            if (q == 0) { // this lane starts pair `first + k`
+                item = first + k;
+                stream_decode(p, item, xi, yj);
+                dyp = dY + yj * (int64_t)D * ncy;
+                if (xi != cur_x) {
+                    cur_x = xi;
+                    const T *src = dX + xi * (int64_t)D * ncx;
+#pragma unroll
+                    for (int rc = 0; rc < RC; ++rc) {
+                        const int ci = ci0 + (RC > 1 ? rc : 0);
+#pragma unroll
+                        for (int kk = 0; kk < D; ++kk) dx[rc][kk] = (ci < ncx) ? src[kk * ncx + ci] : T(0);
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < R; ++r) left[r] = T(1);
+            }
+            const T corner = (q == 0) ? T(1) : corner_next;
+            corner_next = top[C - 1];
+            const int cj = (O <= 3) ? q : ((q * C) >> p.order); // C = 2^order when order <= 3
+            T cc[RC];
+#pragma unroll
+            for (int rc = 0; rc < RC; ++rc) cc[rc] = T(0);
+            const T *dyr = dyp + cj;
+#pragma unroll
+            for (int kk = 0; kk < D; ++kk) {
+                const T dy = dyr[kk * ncy];
+#pragma unroll
+                for (int rc = 0; rc < RC; ++rc) cc[rc] = fma(dx[rc][kk], dy, cc[rc]);
+            }
+            T A[RC], B[RC];
+#pragma unroll
+            for (int rc = 0; rc < RC; ++rc) stencil_coefs(cc[rc], A[rc], B[rc]);
+            stream_block<T, R, O>(left, top, corner, A, B, bot);
+            if (q == nsteps - 1 && lane == lstar) stream_store(p, item, xi, yj, pick_row(left, rstar));
+            if (++q == nsteps) {
+                q = 0;
+                ++k;
+            }
+        }
+    }
+}
+
+template <typename T, int R, int O>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_smem_kernel(StreamParams p)
 {
     using BS = BlockShape<R, O>;
     constexpr int C = BS::C;
@@ -66,33 +248,19 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_kernel(StreamParam
     const int64_t gwarp = (int64_t)blockIdx.x * kWarpsPerBlock + wib;
     const int64_t first = gwarp * p.per_warp;
     if (first >= p.nitems) return; // warp-uniform
-    const int64_t cnt = (p.nitems - first) < p.per_warp ? (p.nitems - first) : p.per_warp;
+    const int cnt = (int)((p.nitems - first) < p.per_warp ? (p.nitems - first) : p.per_warp);
 
-    const int64_t d = p.d;
-    const int64_t stage_elems = (int64_t)RC * d * 32;
+    const int ncx = (int)p.ncx, ncy = (int)p.ncy, d = (int)p.d;
+    const int stage_elems = RC * d * 32;
     T *buf0 = reinterpret_cast<T *>(smem_raw) + (int64_t)wib * 2 * stage_elems;
     T *buf1 = buf0 + stage_elems;
     const T *dX = reinterpret_cast<const T *>(p.dx);
     const T *dY = reinterpret_cast<const T *>(p.dy);
-    TIN *out = reinterpret_cast<TIN *>(p.out);
 
-    const int64_t n = p.ncx << p.order;
-    const int64_t nsteps = (p.ncy << p.order) / C;
-    const int64_t ci0 = ((int64_t)lane * R) >> p.order; // first coarse row of this lane
-    const int lstar = (int)((n - 1) / R);
-    const int rstar = (int)((n - 1) % R);
-
-    auto decode = [&](int64_t item, int64_t &xi, int64_t &yj) {
-        if (p.op == kOpPairwise) {
-            xi = item;
-            yj = item;
-        } else if (p.op == kOpGram) {
-            xi = item / p.ny;
-            yj = item - xi * p.ny;
-        } else {
-            tri_decode(item, xi, yj);
-        }
-    };
+    const int n = ncx << p.order;
+    const int nsteps = (ncy << p.order) / C;
+    const int ci0 = (lane * R) >> p.order;
+    const int lstar = (n - 1) / R, rstar = (n - 1) % R;
 
     T left[R];
 #pragma unroll
@@ -101,26 +269,25 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_kernel(StreamParam
 #pragma unroll
     for (int c = 0; c < C; ++c) bot[c] = T(1);
     T corner_next = T(1);
-    int64_t q = 0, k = 0;     // this lane's column block and pair offset (valid once s >= lane)
+    int q = 0, k = 0;
     int64_t item = first, xi = 0, yj = 0;
     const T *dyp = dY;
-    T fs = T(0);
     const T *dxs = buf0;
-    int64_t staged = 0;       // pairs staged so far (warp-uniform)
-    int64_t next_stage = 0;   // step at which lane 0 starts pair `staged`
+    int staged = 0;     // pairs staged so far (warp-uniform)
+    int next_stage = 0; // step at which lane 0 starts pair `staged`
 
-    const int64_t total = cnt * nsteps + 31;
-    for (int64_t s = 0; s < total; ++s) {
+    const int total = cnt * nsteps + 31;
+    for (int s = 0; s < total; ++s) {
         if (staged < cnt && s == next_stage) { // warp-uniform: lane 0 starts a new pair now
             int64_t sxi, syj;
-            decode(first + staged, sxi, syj);
+            stream_decode(p, first + staged, sxi, syj);
             T *dst = (staged & 1) ? buf1 : buf0;
-            const T *src = dX + sxi * p.ncx * d;
+            const T *src = dX + sxi * (int64_t)d * ncx;
             __syncwarp();
             for (int rc = 0; rc < RC; ++rc) {
-                const int64_t ci = ci0 + (RC > 1 ? rc : 0);
-                const bool ok = ci < p.ncx;
-                for (int64_t kk = 0; kk < d; ++kk) dst[(rc * d + kk) * 32 + lane] = ok ? src[ci * d + kk] : T(0);
+                const int ci = ci0 + (RC > 1 ? rc : 0);
+                const bool ok = ci < ncx;
+                for (int kk = 0; kk < d; ++kk) dst[(rc * d + kk) * 32 + lane] = ok ? src[kk * ncx + ci] : T(0);
             }
             __syncwarp();
             ++staged;
@@ -133,62 +300,32 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_kernel(StreamParam
 #pragma unroll
             for (int c = 0; c < C; ++c) top[c] = T(1);
         }
-        const bool active = (s >= lane) && (k < cnt);
-        if (active) {
-            if (q == 0) { // this lane starts pair `first + k`
+        if (s >= lane && k < cnt) {
+            if (q == 0) {
                 item = first + k;
-                decode(item, xi, yj);
-                dyp = dY + yj * p.ncy * d;
-                double f = p.fscale;
-                if (p.sx) f *= scale_at<TIN>(p.sx, xi);
-                if (p.sy) f *= scale_at<TIN>(p.sy, yj);
-                fs = T(f);
+                stream_decode(p, item, xi, yj);
+                dyp = dY + yj * (int64_t)d * ncy;
                 dxs = (k & 1) ? buf1 : buf0;
 #pragma unroll
                 for (int r = 0; r < R; ++r) left[r] = T(1);
             }
             const T corner = (q == 0) ? T(1) : corner_next;
             corner_next = top[C - 1];
-            // increments of this lane's coarse rows at coarse column cj
-            const int64_t cj = (q * C) >> p.order;
+            const int cj = (q * C) >> p.order;
             T cc[RC];
 #pragma unroll
             for (int rc = 0; rc < RC; ++rc) cc[rc] = T(0);
-            const T *dyr = dyp + cj * d;
-            for (int64_t kk = 0; kk < d; ++kk) {
-                const T dy = dyr[kk];
+            const T *dyr = dyp + cj;
+            for (int kk = 0; kk < d; ++kk) {
+                const T dy = dyr[kk * ncy];
 #pragma unroll
                 for (int rc = 0; rc < RC; ++rc) cc[rc] = fma(dxs[(rc * d + kk) * 32 + lane], dy, cc[rc]);
             }
             T A[RC], B[RC];
 #pragma unroll
-            for (int rc = 0; rc < RC; ++rc) stencil_coefs(cc[rc] * fs, A[rc], B[rc]);
-#pragma unroll
-            for (int c = 0; c < C; ++c) {
-                T up = top[c];
-                T dg = (c == 0) ? corner : top[c - 1];
-#pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    const T l = left[r];
-                    const T v = stencil_cell(dg, up, l, A[BS::rc_of(r)], B[BS::rc_of(r)]);
-                    dg = l;
-                    up = v;
-                    left[r] = v;
-                }
-                bot[c] = up;
-            }
-            if (q == nsteps - 1 && lane == lstar) {
-                T v = left[0];
-#pragma unroll
-                for (int r = 1; r < R; ++r)
-                    if (r == rstar) v = left[r];
-                if (p.op == kOpPairwise) {
-                    out[item] = TIN(v);
-                } else {
-                    out[xi * p.out_ld + yj] = TIN(v);
-                    if (p.op == kOpGramSym && xi != yj) out[yj * p.out_ld + xi] = TIN(v);
-                }
-            }
+            for (int rc = 0; rc < RC; ++rc) stencil_coefs(cc[rc], A[rc], B[rc]);
+            stream_block<T, R, O>(left, top, corner, A, B, bot);
+            if (q == nsteps - 1 && lane == lstar) stream_store(p, item, xi, yj, pick_row(left, rstar));
             if (++q == nsteps) {
                 q = 0;
                 ++k;

@@ -41,9 +41,13 @@ __device__ __forceinline__ T ld_in(const T *p)
 // (a, b): rounding A = 1 + c/2 to float32 keeps only ~2^-24 / c of the
 // increment's relative precision (c shrinks like 4^-order), which made float32
 // results ~50x less accurate than the reference's float64-arithmetic /
-// float32-storage cells; the delta form
-//   K11 = (s - K00) + s * a + K00 * b,  s = K10 + K01
-// keeps c at full precision for one extra operation per cell.
+// float32-storage cells.  The float32 update is
+//   K11 = K10 + ((K01 - K00) + K00 * b + s * a),  s = K10 + K01,
+// where K01 - K00 is exact (neighbouring cells are within a factor 2 of each
+// other, Sterbenz) and everything inside the parentheses is of the size of the
+// increment term, so the only rounding at the magnitude of K is the final
+// addition -- one rounding per cell, as in the reference's float32 storage.
+// It costs 5 float32 operations per cell.
 template <typename T>
 __device__ __forceinline__ void stencil_coefs(T c, T &A, T &B)
 {
@@ -70,7 +74,7 @@ template <>
 __device__ __forceinline__ float stencil_cell<float>(float k00, float k01, float k10, float a, float b)
 {
     const float s = k10 + k01;
-    return fmaf(s, a, fmaf(k00, b, s - k00));
+    return k10 + fmaf(s, a, fmaf(k00, b, k01 - k00));
 }
 
 // Compile-time shape of one lane's block.

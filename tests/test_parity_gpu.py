@@ -7,9 +7,10 @@ Tolerances (stated per test):
     float64; float32 inputs return float32 results (as the reference does), so
     their bound is the float32 rounding of the output, 2.5e-7 (2 ulp);
   * precision="fp32" (float32 cells): error normalised by the Cauchy-Schwarz
-    bound sqrt(k(x,x) k(y,y)) at most 5x that of the reference's own GPU
+    bound sqrt(k(x,x) k(y,y)) at most 4x that of the reference's own GPU
     numerics on the same inputs (float64 arithmetic, every cell stored as
-    float32; the oracle emulates it with store_f32=True), plus 1e-7.  Float32
+    float32; the oracle emulates it with store_f32=True), plus 1e-7: both
+    round each cell once at the magnitude of K.  Float32
     cells cannot give a pointwise bound on near-zero entries: the cells grow to
     ~sqrt(k(x,x) k(y,y));
   * robust lambda: relative error <= 1e-6 (absolute 1e-9 near 0).
@@ -74,8 +75,8 @@ def assert_cs(got, want, kxx, kyy, tol=CS32, msg=""):
 
 
 def fp32_tol(ref_sem, want, kxx, kyy):
-    """5x the CS-normalised error of the reference's float32 GPU numerics, + 1e-7."""
-    return 5.0 * float(cs_err(ref_sem, want, kxx, kyy).max()) + 1e-7
+    """4x the CS-normalised error of the reference's float32 GPU numerics, + 1e-7."""
+    return 4.0 * float(cs_err(ref_sem, want, kxx, kyy).max()) + 1e-7
 
 
 # ----------------------------------------------------------------------------- golden vectors
