@@ -187,6 +187,29 @@ SIGK_API int sigk_normalize_inc(const void *inc, int64_t n, int64_t nc, int64_t 
                        int order, const double *knorm, const double *fnorm, double tol, int maxit, void *lam,
                        int *iters, void *workspace, size_t workspace_bytes, sigk_stream_t stream);
 
+/*
+ * sigk_gram_noalloc -- sigk_gram for callers that cannot allocate device
+ * memory.  It has no counterpart in the reference.
+ *
+ * Same arguments and result as sigk_gram, minus the workspace: the scratch
+ * sigk_gram takes from the caller comes from an 8 MiB array that is part of
+ * this library's device image (each GPU that loads the library holds it until
+ * the process exits).  Nothing is allocated.  A Gram whose scratch
+ * (sigk_workspace_size(SIGK_OP_GRAM, ...)) exceeds 8 MiB is rejected with
+ * SIGK_EINVAL and a message naming the limit; 256 x 256 paths of length 128
+ * in 8 dimensions at order 2 with float64 cells need about 4.2 MB.
+ *
+ * The first call on a device looks up the array's device address (with that
+ * device current) and caches it; make that first call before any stream
+ * capture.  Every call shares the one array and leaves its contents behind;
+ * each call overwrites the part it reads before reading it.  Calls that
+ * overlap on the GPU (two streams, or two host threads, on one device) race on
+ * the array: serialise them.
+ */
+SIGK_API int sigk_gram_noalloc(const void *x, const void *y, int64_t n_x, int64_t n_y, int64_t len_x, int64_t len_y,
+                               int64_t dim, int dtype, int order, double static_scale, const void *scale_x,
+                               const void *scale_y, void *out, int precision, sigk_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

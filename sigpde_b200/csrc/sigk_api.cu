@@ -581,3 +581,68 @@ int sigk_gram_inc(const void *inc, int64_t n_x, int64_t n_y, int64_t nc_x, int64
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// No-allocation variant of sigk_gram.
+//
+// Some callers cannot call cudaMalloc: a host program that links only this
+// library and works inside a device-memory budget fixed up front, or a caller
+// inside a framework whose allocator it may not touch.  For them the scratch
+// that sigk_gram takes from the caller (the scaled path differences the
+// streaming kernel reads) lives in the fixed array below instead.  The array
+// is part of the library's device image, so every GPU that loads the library
+// holds these 8 MiB until the process exits.
+namespace sigk {
+namespace {
+constexpr size_t kNoAllocScratchBytes = size_t(8) << 20;
+} // namespace
+} // namespace sigk
+
+static __device__ __align__(256) unsigned char g_sigk_noalloc_scratch[sigk::kNoAllocScratchBytes];
+
+namespace sigk {
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void *g_noalloc_ptr[kMaxDevices] = {};
+
+// The device address of the scratch array on the current device.  In host
+// code the array's name is only a host-side stand-in, so the address is taken
+// once per device, with that device current, and cached.
+int noalloc_scratch(void **out)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if (dev < 0 || dev >= kMaxDevices) return fail(SIGK_EUNSUPPORTED, "device index %d >= %d", dev, kMaxDevices);
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void *ptr = nullptr;
+        e = cudaGetSymbolAddress(&ptr, g_sigk_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(scratch)");
+        g_noalloc_ptr[dev] = ptr;
+    }
+    *out = g_noalloc_ptr[dev];
+    return SIGK_OK;
+}
+} // namespace
+} // namespace sigk
+
+extern "C" int sigk_gram_noalloc(const void *x, const void *y, int64_t n_x, int64_t n_y, int64_t len_x,
+                                 int64_t len_y, int64_t dim, int dtype, int order, double static_scale,
+                                 const void *scale_x, const void *scale_y, void *out, int precision,
+                                 sigk_stream_t stream)
+{
+    const size_t need =
+        sigk_workspace_size(SIGK_OP_GRAM, n_x, n_y, len_x, len_y, dim, order, dtype, precision);
+    if (need > kNoAllocScratchBytes)
+        return fail(SIGK_EINVAL,
+                    "sigk_gram_noalloc: this Gram needs %zu bytes of scratch; the no-allocation entry point has "
+                    "%zu bytes (8 MiB); use sigk_gram with a caller workspace",
+                    need, kNoAllocScratchBytes);
+    void *scratch = nullptr;
+    int st = noalloc_scratch(&scratch);
+    if (st != SIGK_OK) return st;
+    return run_pairs(kOpGram, x, y, n_x, n_y, len_x, len_y, dim, dtype, order, static_scale, scale_x, scale_y, out,
+                     n_y, precision, scratch, kNoAllocScratchBytes, (cudaStream_t)stream);
+}
