@@ -45,7 +45,9 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu"],
+                    help="ours | reference: the float64 oracle port on the host cores | reference-gpu: the "
+                         "unmodified stojl/SigPDE Numba GPU path installed under baseline/_ref")
     ap.add_argument("--workload", default="gram256", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target length of the CPU-baseline sample")
@@ -196,7 +198,7 @@ def read_traffic(kernel_key):
         line = line.strip()
         if line.startswith(kernel_key + "="):
             try:
-                return float(line.split("=", 1)[1].split()[0])
+                return float(line.split("=", 1)[1].split("#")[0].split()[0])
             except ValueError:
                 return None
     return None
@@ -393,11 +395,86 @@ def run_ours(args, w):
         print(json.dumps(line), flush=True)
 
 
+def run_reference_gpu(args, w):
+    """The reference's own GPU path: stojl/SigPDE installed unmodified under
+    baseline/_ref, called through its public API (sigpde.torch.SigPDE.gram with
+    the default max_batch / max_threads) on the same float32 inputs.  The
+    reference synchronises the device inside every call, so each call is timed
+    on the host between two synchronisations; the L2 is flushed between calls."""
+    import numpy as np
+    import torch
+
+    ref_dir = os.path.join(ROOT, "baseline", "_ref")
+    entries, cells, _ = workload_units(w)
+    base = {"impl": "reference-gpu", "metric": "gram_entries_per_s", "unit": "entries/s"}
+    if not os.path.isdir(os.path.join(ref_dir, "sigpde")):
+        print(json.dumps(dict(base, unavailable="reference not installed under baseline/_ref")), flush=True)
+        return
+    sys.path.insert(0, ref_dir)
+    try:
+        import warnings
+        warnings.filterwarnings("ignore")
+        import sigpde.torch as refsig
+    except Exception as e:  # numba or its CUDA target missing
+        print(json.dumps(dict(base, unavailable=f"import failed: {type(e).__name__}: {e}"[:300])), flush=True)
+        return
+    dev = torch.device("cuda", 0)
+    X, Y = make_inputs(w, device=dev)
+    k = refsig.SigPDE(refsig.kernels.LinearKernel(), w["order"])
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    try:
+        out = k.gram(X, Y)
+    except Exception as e:
+        print(json.dumps(dict(base, unavailable=f"reference call failed: {type(e).__name__}: {e}"[:300])),
+              flush=True)
+        return
+    for _ in range(max(0, args.warmup - 1)):
+        k.gram(X, Y)
+    times = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        k.gram(X, Y)
+        torch.cuda.synchronize()
+        times.append((time.perf_counter() - t0) * 1e3)
+    ms = statistics.mean(times)
+    acc = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle
+        G = out.double().cpu().numpy()
+        rng = np.random.default_rng(1)
+        flat = rng.choice(entries, 64, replace=False)
+        xin, yin = X.double().cpu().numpy(), Y.double().cpu().numpy()
+        want = oracle.gram(xin, yin, w["order"], pairs=flat)
+        got = G.reshape(-1)[flat]
+        kxx = oracle.pairwise(xin[flat // w["ny"]], None, w["order"])
+        kyy = oracle.pairwise(yin[flat % w["ny"]], None, w["order"])
+        acc = {"max_rel_err": float(np.max(np.abs(got - want) / np.abs(want))),
+               "max_cs_err": float(np.max(np.abs(got - want) / np.sqrt(kxx * kyy))),
+               "sample": "64 random entries vs the float64 oracle"}
+    line = dict(base, value=entries / (ms * 1e-3), n_gpus=1, steps=args.steps, warmup=args.warmup,
+                ms_per_step=ms, p50_ms=percentile(times, 0.5), p99_ms=percentile(times, 0.99),
+                higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32 storage / f64 arithmetic",
+                data="synthetic Brownian paths (seeded PCG64), float32",
+                config={"workload": "SigPDE.gram 256x256, L=128, d=8, dyadic_order=2, LinearKernel",
+                        "global_batch": entries, "seq_len": w["L"], "parallelism": "single GPU",
+                        "l2": "flushed between timed calls (256 MB write)"},
+                cells_per_s=cells / (ms * 1e-3), accuracy=acc,
+                note="unmodified stojl/SigPDE (Numba CUDA) through sigpde.torch.SigPDE.gram, host-timed "
+                     "(the reference synchronises inside each call)")
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
         run_reference(args, w, int(os.environ.get("RANK", "0")))
+        return
+    if args.impl == "reference-gpu":
+        if int(os.environ.get("RANK", "0")) == 0:
+            run_reference_gpu(args, w)
         return
     run_ours(args, w)
 
