@@ -35,6 +35,9 @@ if ROOT not in sys.path:
 WORKLOADS = {
     # SigPDE.gram(x, y), LinearKernel, X,Y 256 Brownian paths, L=128, d=8, dyadic order 2
     "gram256": dict(nx=256, ny=256, L=128, d=8, order=2, seed_x=2001, seed_y=2002),
+    # SigPDE pairwise over 4096 (x, y) pairs, lengths uniform in [16, 512] per path, d=32,
+    # dyadic order uniform in {0, 1, 2, 3} per pair, Brownian N(0, 1/(L-1)) increments
+    "uneven4096": dict(kind="ragged", npairs=4096, lmin=16, lmax=512, d=32, orders=(0, 1, 2, 3), seed=4096),
 }
 
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
@@ -466,15 +469,192 @@ def run_reference_gpu(args, w):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------- uneven batched pairwise
+def ragged_spec(w):
+    """Seeded lengths and orders of the uneven workload."""
+    import numpy as np
+    rng = np.random.Generator(np.random.PCG64(w["seed"]))
+    lx = rng.integers(w["lmin"], w["lmax"] + 1, w["npairs"])
+    ly = rng.integers(w["lmin"], w["lmax"] + 1, w["npairs"])
+    orders = rng.choice(np.array(w["orders"]), w["npairs"])
+    return lx.tolist(), ly.tolist(), orders.tolist()
+
+
+def ragged_paths(w, lx, ly):
+    """Brownian paths of the given lengths (float64 numpy), seeded per pair."""
+    from sigpde_b200 import synthetic
+    xs = [synthetic.brownian_np(1, int(L), w["d"], w["seed"] * 100003 + 2 * b)[0] for b, L in enumerate(lx)]
+    ys = [synthetic.brownian_np(1, int(L), w["d"], w["seed"] * 100003 + 2 * b + 1)[0] for b, L in enumerate(ly)]
+    return xs, ys
+
+
+def ragged_cells(lx, ly, orders):
+    return int(sum(((a - 1) << o) * ((b - 1) << o) for a, b, o in zip(lx, ly, orders)))
+
+
+def cpu_oracle_ragged(w, xs, ys, orders, target_s, seed=7):
+    """Float64 oracle on a random sample of pairs; returns (cells/s, cores, sample)."""
+    import numpy as np
+    from oracle import oracle
+    oracle.build()
+    rng = np.random.default_rng(seed)
+    n = max(oracle.num_threads(), 8)
+    idx = []
+    t_used = 0.0
+    cells = 0
+    perm = rng.permutation(len(xs))
+    pos = 0
+    while t_used < target_s and pos < len(perm):
+        take = perm[pos:pos + n]
+        pos += n
+        t0 = time.perf_counter()
+        for b in take:  # one pair at a time (lengths differ); OpenMP inside is over one pair only
+            x = xs[b].astype(np.float32).astype(np.float64)[None]
+            y = ys[b].astype(np.float32).astype(np.float64)[None]
+            oracle.pairwise(x, y, int(orders[b]))
+        t_used += time.perf_counter() - t0
+        idx.extend(int(b) for b in take)
+        cells += sum(((len(xs[b]) - 1) << orders[b]) * ((len(ys[b]) - 1) << orders[b]) for b in take)
+    return cells / t_used, 1, f"{len(idx)} random pairs of the uneven batch ({cells:.3e} cells) in {t_used:.1f} s, 1 thread"
+
+
+def run_ours_ragged(args, w):
+    import numpy as np
+    import torch
+    import sigpde_b200.torch as sig
+    from sigpde_b200 import _lib
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    lx, ly, orders = ragged_spec(w)
+    xs, ys = ragged_paths(w, lx, ly)
+    cells = ragged_cells(lx, ly, orders)
+    X = [torch.tensor(a, dtype=torch.float32, device=dev) for a in xs]
+    Y = [torch.tensor(a, dtype=torch.float32, device=dev) for a in ys]
+    solver = sig.ragged.RaggedPairwise(lx, ly, orders, w["d"], torch.float32, dev, args.precision)
+    solver.load(X, Y)
+    solver.capture()
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    clocks = ClockSampler(0)
+    clocks.start()
+    times = timed_steps(torch, solver.solve, args.steps, args.warmup, flush, lambda: None)
+    clk = clocks.stop()
+    ms = statistics.mean(times)
+    out = solver.out.double().cpu().numpy()
+    # end to end: packed paths from pinned host memory, one graph replay, result back to pinned host memory
+    xh = solver.x_pack.cpu().pin_memory()
+    yh = solver.y_pack.cpu().pin_memory()
+    oh = torch.empty_like(solver.out, device="cpu").pin_memory()
+
+    def e2e_step():
+        solver.x_pack.copy_(xh, non_blocking=True)
+        solver.y_pack.copy_(yh, non_blocking=True)
+        oh.copy_(solver.solve(), non_blocking=True)
+
+    e2e_times = timed_steps(torch, e2e_step, args.steps, args.warmup, flush, lambda: None)
+    acc = cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle
+        rng = np.random.default_rng(1)
+        pick = rng.choice(len(xs), 32, replace=False)
+        want = np.array([oracle.pairwise(xs[b].astype(np.float32).astype(np.float64)[None],
+                                         ys[b].astype(np.float32).astype(np.float64)[None], int(orders[b]))[0]
+                         for b in pick])
+        acc = {"max_rel_err": float(np.max(np.abs(out[pick] - want) / np.abs(want))),
+               "sample": "32 random pairs vs the float64 oracle"}
+        rate, cores, sample = cpu_oracle_ragged(w, xs, ys, orders, args.cpu_seconds)
+        cpu = {"value": rate, "unit": "cells/s", "cores": cores, "kind": "port", "sample": sample}
+    line = {
+        "metric": "pde_cell_updates_per_s", "value": cells / (ms * 1e-3), "unit": "cells/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "p50_ms": percentile(times, 0.5),
+        "p99_ms": percentile(times, 0.99), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32",
+        "data": "synthetic Brownian paths (seeded PCG64), float32",
+        "config": {"workload": "pairwise 4096 uneven pairs, L~U[16,512] per path, d=32, order~U{0..3} per pair",
+                   "global_batch": w["npairs"], "seq_len": "16-512", "parallelism": "single GPU",
+                   "precision": args.precision, "l2": "flushed between timed steps (256 MB write)",
+                   "launch": "one persistent ragged launch, CUDA-graph replay"},
+        "pairs_per_s": w["npairs"] / (ms * 1e-3), "cells_per_step": cells, "accuracy": acc,
+        "e2e": {"value": cells / (statistics.mean(e2e_times) * 1e-3), "unit": "cells/s",
+                "h2d_bytes_per_step": xh.numel() * xh.element_size() + yh.numel() * yh.element_size(),
+                "d2h_bytes_per_step": oh.numel() * oh.element_size(), "ms_per_step": statistics.mean(e2e_times)},
+        "gpu_launches": args.steps, "clocks": clk, "lib": _lib.version(),
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+
+
+def run_reference_gpu_ragged(args, w):
+    """The reference's Numba path: one SigPDE.pairwise call per (len x, len y, order) bucket."""
+    import torch
+    ref_dir = os.path.join(ROOT, "baseline", "_ref")
+    base = {"impl": "reference-gpu", "metric": "pde_cell_updates_per_s", "unit": "cells/s"}
+    if not os.path.isdir(os.path.join(ref_dir, "sigpde")):
+        print(json.dumps(dict(base, unavailable="reference not installed under baseline/_ref")), flush=True)
+        return
+    sys.path.insert(0, ref_dir)
+    import warnings
+    warnings.filterwarnings("ignore")
+    import sigpde.torch as refsig
+    lx, ly, orders = ragged_spec(w)
+    xs, ys = ragged_paths(w, lx, ly)
+    cells = ragged_cells(lx, ly, orders)
+    buckets = {}
+    for b, key in enumerate(zip(lx, ly, orders)):
+        buckets.setdefault(key, []).append(b)
+    dev = torch.device("cuda", 0)
+    calls = []
+    for (a, c, o), idx in buckets.items():
+        import numpy as np
+        X = torch.tensor(np.stack([xs[b] for b in idx]), dtype=torch.float32, device=dev)
+        Y = torch.tensor(np.stack([ys[b] for b in idx]), dtype=torch.float32, device=dev)
+        calls.append((refsig.SigPDE(refsig.kernels.LinearKernel(), o), X, Y))
+    lin_calls = calls
+
+    def step():
+        for k, X, Y in lin_calls:
+            k.pairwise(X, Y)
+
+    step()  # JIT
+    times = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        step()
+        torch.cuda.synchronize()
+        times.append((time.perf_counter() - t0) * 1e3)
+    ms = statistics.mean(times)
+    print(json.dumps(dict(base, value=cells / (ms * 1e-3), ms_per_step=ms, steps=args.steps, n_gpus=1,
+                          calls_per_step=len(calls), pairs_per_s=w["npairs"] / (ms * 1e-3),
+                          config={"workload": "pairwise 4096 uneven pairs, L~U[16,512], d=32, order~U{0..3}"},
+                          note="one reference SigPDE.pairwise call per (len x, len y, order) bucket")), flush=True)
+
+
 def main():
     args = parse()
     w = WORKLOADS[args.workload]
+    ragged = w.get("kind") == "ragged"
     if args.impl == "reference":
+        if ragged:
+            if int(os.environ.get("RANK", "0")) == 0:
+                lx, ly, orders = ragged_spec(w)
+                xs, ys = ragged_paths(w, lx, ly)
+                rate, cores, sample = cpu_oracle_ragged(w, xs, ys, orders, args.cpu_seconds)
+                print(json.dumps({"impl": "reference", "metric": "pde_cell_updates_per_s", "value": rate,
+                                  "unit": "cells/s", "n_gpus": args.gpus, "higher_is_better": True,
+                                  "cpu_baseline": {"value": rate, "unit": "cells/s", "cores": cores, "kind": "port",
+                                                   "sample": sample},
+                                  "e2e": {"value": rate, "unit": "cells/s", "h2d_bytes_per_step": 0,
+                                          "d2h_bytes_per_step": 0}}), flush=True)
+            return
         run_reference(args, w, int(os.environ.get("RANK", "0")))
         return
     if args.impl == "reference-gpu":
         if int(os.environ.get("RANK", "0")) == 0:
-            run_reference_gpu(args, w)
+            (run_reference_gpu_ragged if ragged else run_reference_gpu)(args, w)
+        return
+    if ragged:
+        run_ours_ragged(args, w)
         return
     run_ours(args, w)
 

@@ -188,6 +188,42 @@ SIGK_API int sigk_normalize_inc(const void *inc, int64_t n, int64_t nc, int64_t 
                        int *iters, void *workspace, size_t workspace_bytes, sigk_stream_t stream);
 
 /*
+ * Uneven batched pairwise signature kernels: pair b compares x path b and
+ * y path b, each of its own length, at its own dyadic order, in one launch.
+ * No reference call covers this: the reference needs one SigPDE.pairwise call
+ * per (length_x, length_y, order) bucket (sigpde/torch/kernel.py:31-65).
+ *   x_pack: all x paths' points back to back, (x_points, dim) in dtype, with
+ *         x_points = sum_b x_len[b] (every path >= 2 points);
+ *   x_off[b], x_len[b] (int64, device): first point and length of x path b;
+ *         they must describe x_pack (x_off[b] = x_len[0] + ... + x_len[b-1]);
+ *   y_pack, y_off, y_len, y_points: the same for y;  order[b] (int32, device).
+ * The work plan (device arrays, built once per batch shape, see
+ * sigpde_b200/torch/ragged.py): with n_b = (min(x_len,y_len) - 1) << order and
+ * m_b = (max(x_len,y_len) - 1) << order,
+ *   pair_rows[b]  in {2, 4, 8, 16}: rows per lane;
+ *   pair_bands[b] = ceil(n_b / (32 * pair_rows[b]));
+ *   pair_bnd_off[b]: offset (cell-type elements) of the pair's
+ *         (pair_bands[b] - 1) * (m_b + 1) boundary values in a pool of bnd_elems;
+ *   item_pair[i], item_band[i] (nitems items): every band of every pair, the
+ *         bands of a pair consecutive and in increasing order, pairs in the
+ *         order they should start (longest first balances best).
+ * An item that breaks these rules (or an order outside [0, 12]) gives NaN for
+ * its pair and is not solved.  scale_x, scale_y: (npairs,) or NULL;
+ * out: (npairs,) in dtype.
+ * Workspace: sigk_ragged_workspace_size(npairs, x_points, y_points, dim,
+ * nitems, bnd_elems, precision) bytes, 256-byte aligned.
+ */
+SIGK_API size_t sigk_ragged_workspace_size(int64_t npairs, int64_t x_points, int64_t y_points, int64_t dim,
+                                           int64_t nitems, int64_t bnd_elems, int precision);
+SIGK_API int sigk_pairwise_ragged(const void *x_pack, const int64_t *x_off, const int64_t *x_len, int64_t x_points,
+                                  const void *y_pack, const int64_t *y_off, const int64_t *y_len, int64_t y_points,
+                                  const int *order, const int64_t *item_pair, const int *item_band, int64_t nitems,
+                                  const int *pair_rows, const int *pair_bands, const int64_t *pair_bnd_off,
+                                  int64_t bnd_elems, int64_t npairs, int64_t dim, int dtype, double static_scale,
+                                  const void *scale_x, const void *scale_y, void *out, int precision,
+                                  void *workspace, size_t workspace_bytes, sigk_stream_t stream);
+
+/*
  * sigk_gram_noalloc -- sigk_gram for callers that cannot allocate device
  * memory.  It has no counterpart in the reference.
  *

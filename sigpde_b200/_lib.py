@@ -56,6 +56,9 @@ SIGNATURES = {
                              _i64, _int, _vp, _sz, _vp]),
     "sigk_normalize_inc": (_int, [_vp, _i64, _i64, _i64, _i64, _i64, _int, _int, _vp, _vp, _dbl, _int, _vp, _vp, _vp,
                                   _sz, _vp]),
+    "sigk_ragged_workspace_size": (_sz, [_i64, _i64, _i64, _i64, _i64, _i64, _int]),
+    "sigk_pairwise_ragged": (_int, [_vp, _vp, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _i64,
+                                    _i64, _i64, _int, _dbl, _vp, _vp, _vp, _int, _vp, _sz, _vp]),
     "sigk_gram_noalloc": (_int, [_vp, _vp, _i64, _i64, _i64, _i64, _i64, _int, _int, _dbl, _vp, _vp, _vp, _int, _vp]),
 }
 

@@ -10,10 +10,14 @@ namespace sigk {
 struct PairParams;
 struct NormParams;
 struct StreamParams;
+struct RaggedParams;
 
 using PairFn = void (*)(PairParams);
 using NormFn = void (*)(NormParams);
 using StreamFn = void (*)(StreamParams);
+using RaggedFn = void (*)(RaggedParams);
+using RaggedDeltaFn = void (*)(const void *, const int64_t *, const int64_t *, const int *, double, const void *,
+                                int64_t, int64_t, void *);
 using DeltaFn = void (*)(const void *, int64_t, int64_t, int64_t, int64_t, double, const void *, void *);
 
 // f64cells: float64 cells (SIGK_PREC_FP64) vs float32; in64: float64 inputs;
@@ -28,5 +32,7 @@ StreamFn get_stream_reg_kernel_f64(int R, int O, int D);
 StreamFn get_stream_reg_kernel_f32(int R, int O, int D);
 StreamFn get_stream_smem_kernel(bool f64cells, int R, int O);
 DeltaFn get_delta_kernel(bool f64cells, bool in64);
+RaggedFn get_ragged_kernel(bool f64cells, bool in64);
+RaggedDeltaFn get_ragged_delta_kernel(bool f64cells, bool in64);
 
 } // namespace sigk

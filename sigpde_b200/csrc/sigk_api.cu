@@ -17,6 +17,7 @@
 
 #include "../../include/sigk.h"
 #include "dispatch.h"
+#include "ragged.cuh"
 #include "stream.cuh"
 
 namespace sigk {
@@ -645,4 +646,120 @@ extern "C" int sigk_gram_noalloc(const void *x, const void *y, int64_t n_x, int6
     if (st != SIGK_OK) return st;
     return run_pairs(kOpGram, x, y, n_x, n_y, len_x, len_y, dim, dtype, order, static_scale, scale_x, scale_y, out,
                      n_y, precision, scratch, kNoAllocScratchBytes, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
+// Uneven batched pairwise (paths of different lengths, a dyadic order per pair)
+namespace sigk {
+namespace {
+constexpr size_t kRaggedStageBytesPerWarp = 16 * 1024;
+
+struct RaggedPlan {
+    size_t counter_off, error_off, progress_off, pool_off, dx_off, dy_off, ws_bytes;
+};
+
+RaggedPlan ragged_plan(int64_t npairs, int64_t x_points, int64_t y_points, int64_t dim, int64_t nitems,
+                       int64_t bnd_elems, size_t tsize)
+{
+    RaggedPlan r{};
+    r.counter_off = 0;
+    r.error_off = 8;
+    r.progress_off = 256;
+    r.pool_off = align256(r.progress_off + (size_t)nitems * sizeof(int));
+    r.dx_off = align256(r.pool_off + (size_t)bnd_elems * tsize);
+    r.dy_off = align256(r.dx_off + (size_t)(x_points - npairs) * (size_t)dim * tsize);
+    r.ws_bytes = align256(r.dy_off + (size_t)(y_points - npairs) * (size_t)dim * tsize);
+    return r;
+}
+} // namespace
+} // namespace sigk
+
+extern "C" size_t sigk_ragged_workspace_size(int64_t npairs, int64_t x_points, int64_t y_points, int64_t dim,
+                                             int64_t nitems, int64_t bnd_elems, int precision)
+{
+    if (npairs < 1 || dim < 1 || nitems < npairs || bnd_elems < 0 || x_points < npairs || y_points < npairs) return 0;
+    return ragged_plan(npairs, x_points, y_points, dim, nitems, bnd_elems, tsize_of(precision)).ws_bytes;
+}
+
+extern "C" int sigk_pairwise_ragged(const void *x_pack, const int64_t *x_off, const int64_t *x_len, int64_t x_points,
+                                    const void *y_pack, const int64_t *y_off, const int64_t *y_len, int64_t y_points,
+                                    const int *order, const int64_t *item_pair, const int *item_band, int64_t nitems,
+                                    const int *pair_rows, const int *pair_bands, const int64_t *pair_bnd_off,
+                                    int64_t bnd_elems, int64_t npairs, int64_t dim, int dtype, double static_scale,
+                                    const void *scale_x, const void *scale_y, void *out, int precision,
+                                    void *workspace, size_t workspace_bytes, sigk_stream_t stream_)
+{
+    cudaStream_t stream = (cudaStream_t)stream_;
+    int st = check_common(dtype, precision, 0);
+    if (st) return st;
+    if (npairs < 1) return fail(SIGK_EINVAL, "npairs must be >= 1");
+    if (dim < 1) return fail(SIGK_EINVAL, "dim must be >= 1");
+    if (nitems < npairs) return fail(SIGK_EINVAL, "nitems must be >= npairs (one item per band)");
+    if (nitems > 0x7fffffffLL) return fail(SIGK_EINVAL, "too many band items");
+    if (bnd_elems < 0) return fail(SIGK_EINVAL, "bnd_elems must be >= 0");
+    if (x_points < 2 * npairs || y_points < 2 * npairs)
+        return fail(SIGK_EINVAL, "x_points / y_points must count every packed point (>= 2 per path)");
+    if ((st = check_dev(x_pack, "x_pack", false)) || (st = check_dev(x_off, "x_off", false)) ||
+        (st = check_dev(x_len, "x_len", false)) || (st = check_dev(y_pack, "y_pack", false)) ||
+        (st = check_dev(y_off, "y_off", false)) || (st = check_dev(y_len, "y_len", false)) ||
+        (st = check_dev(order, "order", false)) || (st = check_dev(item_pair, "item_pair", false)) ||
+        (st = check_dev(item_band, "item_band", false)) || (st = check_dev(pair_rows, "pair_rows", false)) ||
+        (st = check_dev(pair_bands, "pair_bands", false)) || (st = check_dev(pair_bnd_off, "pair_bnd_off", false)) ||
+        (st = check_dev(out, "out", false)) || (st = check_dev(scale_x, "scale_x", true)) ||
+        (st = check_dev(scale_y, "scale_y", true)))
+        return st;
+    const size_t ts = tsize_of(precision);
+    const bool f64 = precision == SIGK_PREC_FP64, in64 = dtype == SIGK_F64;
+    RaggedPlan pl = ragged_plan(npairs, x_points, y_points, dim, nitems, bnd_elems, ts);
+    if (!workspace || workspace_bytes < pl.ws_bytes)
+        return fail(SIGK_ENOMEM, "workspace of %zu bytes needed (got %zu)", pl.ws_bytes, workspace ? workspace_bytes : 0);
+    if (((uintptr_t)workspace & 255) != 0) return fail(SIGK_EINVAL, "workspace must be 256-byte aligned");
+    unsigned char *wsb = reinterpret_cast<unsigned char *>(workspace);
+    // work counter, error flag and per-item progress start at zero
+    cudaError_t e = cudaMemsetAsync(wsb, 0, pl.pool_off, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(counters)");
+
+    // scaled, dimension-major differences of both packs: static_scale * 4^-order * scale_x on x, scale_y on y.
+    // grid: y over paths (strided beyond 65535), x over one path's (len - 1) * dim values
+    RaggedDeltaFn delta = get_ragged_delta_kernel(f64, in64);
+    const dim3 dgrid(32, (unsigned)(npairs < 65535 ? npairs : 65535));
+    delta<<<dgrid, 256, 0, stream>>>(x_pack, x_off, x_len, order, static_scale, scale_x, npairs, dim, wsb + pl.dx_off);
+    delta<<<dgrid, 256, 0, stream>>>(y_pack, y_off, y_len, nullptr, 1.0, scale_y, npairs, dim, wsb + pl.dy_off);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "ragged delta launch");
+
+    RaggedParams p{};
+    p.dx_pack = wsb + pl.dx_off;
+    p.dy_pack = wsb + pl.dy_off;
+    p.x_off = x_off;
+    p.x_len = x_len;
+    p.y_off = y_off;
+    p.y_len = y_len;
+    p.order = order;
+    p.item_pair = item_pair;
+    p.item_band = item_band;
+    p.nitems = nitems;
+    p.pair_rows = pair_rows;
+    p.pair_bands = pair_bands;
+    p.pair_bnd_off = pair_bnd_off;
+    p.bnd_elems = bnd_elems;
+    p.npairs = npairs;
+    p.d = dim;
+    p.out = out;
+    p.counter = reinterpret_cast<unsigned long long *>(wsb + pl.counter_off);
+    p.error = reinterpret_cast<int *>(wsb + pl.error_off);
+    p.progress = reinterpret_cast<int *>(wsb + pl.progress_off);
+    p.pool = wsb + pl.pool_off;
+    p.stage_elems_per_warp = (int)(kRaggedStageBytesPerWarp / ts);
+    RaggedFn fn = get_ragged_kernel(f64, in64);
+    const size_t smem = kRaggedStageBytesPerWarp * kWarpsPerBlock;
+    int nb = 0;
+    if ((st = blocks_per_sm((const void *)fn, smem, &nb))) return st;
+    // persistent grid: never more blocks than can be resident at once (band waits rely on it)
+    int64_t blocks = (int64_t)sm_count() * nb;
+    const int64_t want = (nitems + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    if (blocks > want) blocks = want;
+    fn<<<(unsigned)blocks, kWarpsPerBlock * 32, smem, stream>>>(p);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? SIGK_OK : cuda_fail(e, "ragged kernel launch");
 }

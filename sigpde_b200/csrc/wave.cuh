@@ -175,6 +175,58 @@ struct PathIncs {
     }
 };
 
+// Source of increments from precomputed, already scaled path differences in
+// T, stored dimension-major per path (dX[k * ncx + ci], dY[k * ncy + cj]): the
+// lanes of a warp read neighbouring columns cj of one dimension k together
+// (lane l is one column behind lane l-1), so the loads coalesce.
+template <typename T, int RC>
+struct DeltaIncs {
+    const T *dX;
+    const T *dY;
+    int64_t d;
+    T *dxs;      // this warp's staging area: RC * d * 32 values, or null
+    int64_t ci0 = 0, ncx = 0, ncy = 0;
+    bool rc_per_row = false;
+
+    __device__ __forceinline__ void stage(int64_t ci0_, int64_t ncx_, int lane, bool rc_per_row_)
+    {
+        ci0 = ci0_;
+        ncx = ncx_;
+        rc_per_row = rc_per_row_;
+        if (!dxs) return;
+        __syncwarp();
+        for (int rc = 0; rc < RC; ++rc) {
+            const int64_t ci = ci0 + (rc_per_row ? rc : 0);
+            const bool ok = ci < ncx;
+            for (int64_t k = 0; k < d; ++k) dxs[(rc * d + k) * 32 + lane] = ok ? dX[k * ncx + ci] : T(0);
+        }
+        __syncwarp();
+    }
+
+    __device__ __forceinline__ void column(int64_t cj, int lane, T (&c)[RC]) const
+    {
+#pragma unroll
+        for (int rc = 0; rc < RC; ++rc) c[rc] = T(0);
+        const T *dy = dY + cj;
+        if (dxs) {
+            for (int64_t k = 0; k < d; ++k) {
+                const T v = dy[k * ncy];
+#pragma unroll
+                for (int rc = 0; rc < RC; ++rc) c[rc] = fma(dxs[(rc * d + k) * 32 + lane], v, c[rc]);
+            }
+        } else {
+            for (int64_t k = 0; k < d; ++k) {
+                const T v = dy[k * ncy];
+#pragma unroll
+                for (int rc = 0; rc < RC; ++rc) {
+                    const int64_t ci = ci0 + (rc_per_row ? rc : 0);
+                    if (ci < ncx) c[rc] = fma(dX[k * ncx + ci], v, c[rc]);
+                }
+            }
+        }
+    }
+};
+
 // Source of precomputed coarse increments (generic static kernels): strided
 // reads of inc[ci][cj] in TIN, times fscale.
 template <typename T, typename TIN, int RC>

@@ -1,0 +1,197 @@
+"""Uneven batched pairwise signature kernels (one persistent launch).
+
+The reference solves a batch with one `SigPDE.pairwise` call per shape: every
+path in a call has the same length and the whole call one dyadic order
+(sigpde/torch/kernel.py:31-65).  A batch of pairs with their own lengths and
+orders therefore costs it one call per (len x, len y, order) bucket.  Here the
+pairs go in one launch of `sigk_pairwise_ragged`: paths are packed back to
+back and each pair is cut into bands of rows; warps take bands longest pair
+first from a work counter, so a long pair runs on several warps at once as a
+pipeline while short pairs fill the rest of the GPU.  The plan (rows per lane,
+bands, boundary-buffer offsets, item order) is built here once per batch shape.
+
+    from sigpde_b200.torch import ragged
+    k = ragged.pairwise(x_paths, y_paths, orders)          # lists of (L_b, d) tensors
+
+`RaggedPairwise` keeps the packed layout, the work order and the workspace of
+one batch shape, and can capture the launch in a CUDA graph for repeated
+solves of new values with the same shapes (for example a serving loop).
+"""
+from __future__ import annotations
+
+import torch
+
+from .. import _lib
+from .kernel import _PREC, _dtype_code, _is_fused_linear, _ptr, _stream
+
+__all__ = ["pack", "pairwise", "RaggedPairwise"]
+
+
+def pack(paths, dtype=None, device=None):
+    """Pack a list of (L_i, d) paths into (sum L_i, d) plus int64 offsets and lengths."""
+    if len(paths) == 0:
+        raise ValueError("no paths")
+    d = paths[0].shape[-1]
+    dtype = paths[0].dtype if dtype is None else dtype
+    device = paths[0].device if device is None else device
+    lens = [int(p.shape[0]) for p in paths]
+    for p in paths:
+        if p.dim() != 2 or p.shape[1] != d:
+            raise ValueError("every path must be a (length, dim) tensor with the same dim")
+    packed = torch.cat([p.to(device=device, dtype=dtype) for p in paths], 0).contiguous()
+    lengths = torch.tensor(lens, dtype=torch.int64)
+    offsets = torch.zeros_like(lengths)
+    offsets[1:] = torch.cumsum(lengths, 0)[:-1]
+    return packed, offsets.to(device), lengths.to(device), lens
+
+
+STAGE_BYTES_PER_WARP = 16 * 1024  # the kernel's dx staging budget per warp
+
+
+def rows_per_lane(n, d, order, tsize):
+    """Rows per lane R for a pair with n refined rows: the smallest of 2, 4, 8,
+    16 covering the rows in one band of 32 R, shrunk while the lane's dx tile
+    (coarse rows per lane x d) does not fit the kernel's staging budget."""
+    R = 2 if n <= 64 else 4 if n <= 128 else 8 if n <= 256 else 16
+    cap = STAGE_BYTES_PER_WARP // tsize
+    while R > 2:
+        rc = 1 if order >= 4 else max(R >> order, 1)
+        if rc * d * 32 <= cap:
+            break
+        R >>= 1
+    return R
+
+
+def plan(x_lengths, y_lengths, orders, dim, tsize):
+    """Band plan of a ragged batch (see sigk_pairwise_ragged in include/sigk.h)."""
+    import numpy as np
+    lx = np.asarray(x_lengths, np.int64)
+    ly = np.asarray(y_lengths, np.int64)
+    od = np.asarray(orders, np.int64)
+    n = (np.minimum(lx, ly) - 1) << od
+    m = (np.maximum(lx, ly) - 1) << od
+    rows = np.array([rows_per_lane(int(a), dim, int(o), tsize) for a, o in zip(n, od)], np.int64)
+    bands = (n + 32 * rows - 1) // (32 * rows)
+    sizes = (bands - 1) * (m + 1)
+    bnd_off = np.zeros_like(sizes)
+    bnd_off[1:] = np.cumsum(sizes)[:-1]
+    order_of_start = np.argsort(-(n * m).astype(np.float64), kind="stable")  # longest first
+    item_pair = np.repeat(order_of_start, bands[order_of_start])
+    item_band = np.concatenate([np.arange(bands[b]) for b in order_of_start]).astype(np.int64)
+    return {"rows": rows, "bands": bands, "bnd_off": bnd_off, "bnd_elems": int(sizes.sum()),
+            "item_pair": item_pair, "item_band": item_band}
+
+
+class RaggedPairwise:
+    """Solver for one ragged batch shape: packed inputs, work order and workspace
+    are built once; `solve()` runs the launch (optionally replaying a captured
+    CUDA graph)."""
+
+    def __init__(self, x_lengths, y_lengths, orders, dim, dtype=torch.float32, device="cuda", precision="fp64",
+                 static_scale=1.0):
+        if precision not in _PREC:
+            raise ValueError(f"precision must be one of {sorted(_PREC)}")
+        x_lengths = [int(v) for v in x_lengths]
+        y_lengths = [int(v) for v in y_lengths]
+        orders = [int(v) for v in orders]
+        if not (len(x_lengths) == len(y_lengths) == len(orders)) or not x_lengths:
+            raise ValueError("x_lengths, y_lengths and orders must be non-empty and of equal length")
+        if min(x_lengths + y_lengths) < 2:
+            raise ValueError("every path needs at least 2 points")
+        if min(orders) < 0 or max(orders) > 12:
+            raise ValueError("dyadic orders must lie in [0, 12]")
+        self.device = torch.device(device)
+        self.dtype = dtype
+        self.dim = int(dim)
+        self.n = len(orders)
+        self.prec = _PREC[precision]
+        self.static_scale = float(static_scale)
+        xl = torch.tensor(x_lengths, dtype=torch.int64)
+        yl = torch.tensor(y_lengths, dtype=torch.int64)
+        xo = torch.zeros_like(xl)
+        xo[1:] = torch.cumsum(xl, 0)[:-1]
+        yo = torch.zeros_like(yl)
+        yo[1:] = torch.cumsum(yl, 0)[:-1]
+        od = torch.tensor(orders, dtype=torch.int32)
+        self.x_len, self.y_len = xl.to(self.device), yl.to(self.device)
+        self.x_off, self.y_off = xo.to(self.device), yo.to(self.device)
+        self.order = od.to(self.device)
+        pl = plan(x_lengths, y_lengths, orders, self.dim, 8 if precision == "fp64" else 4)
+        self.item_pair = torch.as_tensor(pl["item_pair"], device=self.device)
+        self.item_band = torch.as_tensor(pl["item_band"], dtype=torch.int32, device=self.device)
+        self.pair_rows = torch.as_tensor(pl["rows"], dtype=torch.int32, device=self.device)
+        self.pair_bands = torch.as_tensor(pl["bands"], dtype=torch.int32, device=self.device)
+        self.pair_bnd_off = torch.as_tensor(pl["bnd_off"], device=self.device)
+        self.bnd_elems = pl["bnd_elems"]
+        self.nitems = int(pl["item_pair"].shape[0])
+        self.x_pack = torch.zeros((int(xl.sum()), self.dim), dtype=dtype, device=self.device)
+        self.y_pack = torch.zeros((int(yl.sum()), self.dim), dtype=dtype, device=self.device)
+        self.out = torch.empty(self.n, dtype=dtype, device=self.device)
+        self.x_points = int(xl.sum())
+        self.y_points = int(yl.sum())
+        nws = _lib.lib().sigk_ragged_workspace_size(self.n, self.x_points, self.y_points, self.dim, self.nitems,
+                                                    self.bnd_elems, self.prec)
+        self.ws = torch.empty(nws, dtype=torch.uint8, device=self.device)
+        self.x_scale = None
+        self.y_scale = None
+        self.graph = None
+
+    def load(self, x_paths, y_paths, x_scale=None, y_scale=None):
+        """Copy new path values (same shapes) into the packed buffers."""
+        torch.cat([p.to(self.device, self.dtype) for p in x_paths], 0, out=self.x_pack)
+        torch.cat([p.to(self.device, self.dtype) for p in y_paths], 0, out=self.y_pack)
+        self.x_scale = None if x_scale is None else torch.as_tensor(x_scale, dtype=self.dtype, device=self.device)
+        self.y_scale = None if y_scale is None else torch.as_tensor(y_scale, dtype=self.dtype, device=self.device)
+
+    def _launch(self):
+        _lib.call("sigk_pairwise_ragged", _ptr(self.x_pack), _ptr(self.x_off), _ptr(self.x_len), self.x_points,
+                  _ptr(self.y_pack), _ptr(self.y_off), _ptr(self.y_len), self.y_points, _ptr(self.order),
+                  _ptr(self.item_pair), _ptr(self.item_band), self.nitems, _ptr(self.pair_rows),
+                  _ptr(self.pair_bands), _ptr(self.pair_bnd_off), self.bnd_elems, self.n, self.dim,
+                  _dtype_code(self.x_pack), self.static_scale, _ptr(self.x_scale), _ptr(self.y_scale),
+                  _ptr(self.out), self.prec, _ptr(self.ws), self.ws.numel(), _stream())
+
+    def capture(self):
+        """Capture the launch (counter reset + kernel) in a CUDA graph; later
+        `solve()` calls replay it.  Scales present at capture time stay bound."""
+        self._launch()  # warm-up outside the capture (loads the module, sizes the grid)
+        torch.cuda.synchronize(self.device)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self._launch()
+        self.graph = g
+        return self
+
+    def error_flag(self):
+        """1 if the last launch refused an item or a band wait ran out (synchronises)."""
+        return int(self.ws[8:12].view(torch.int32).item())
+
+    def solve(self):
+        with torch.cuda.device(self.device):
+            if self.graph is not None:
+                self.graph.replay()
+            else:
+                self._launch()
+        return self.out
+
+
+def pairwise(x_paths, y_paths, orders, static_kernel=None, x_scale=None, y_scale=None, precision="fp64"):
+    """k(x_b, y_b) for pairs with their own lengths and dyadic orders.
+
+    x_paths, y_paths: lists of (L_b, d) CUDA tensors (float32 or float64);
+    orders: list of ints.  Returns a (B,) tensor in the paths' dtype.
+    """
+    if static_kernel is not None and not _is_fused_linear(static_kernel):
+        raise NotImplementedError("ragged batches support the linear static kernel")
+    scale = 1.0 if static_kernel is None else float(static_kernel.scale)
+    if not (len(x_paths) == len(y_paths) == len(orders)):
+        raise ValueError("x_paths, y_paths and orders must have the same length")
+    dev = x_paths[0].device
+    if dev.type != "cuda":
+        raise ValueError("paths must be CUDA tensors (this package has no CPU path)")
+    dtype = x_paths[0].dtype
+    _dtype_code(x_paths[0])
+    solver = RaggedPairwise([p.shape[0] for p in x_paths], [p.shape[0] for p in y_paths], orders,
+                            x_paths[0].shape[1], dtype, dev, precision, scale)
+    solver.load(x_paths, y_paths, x_scale, y_scale)
+    return solver.solve().clone()

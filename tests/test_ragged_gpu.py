@@ -1,0 +1,124 @@
+"""Uneven batched pairwise solves (sigk_pairwise_ragged) against the float64
+oracle, pair by pair.  Tolerances as in test_parity_gpu: float64 cells, so
+the bound is 1e-9 relative for float64 outputs and 2.5e-7 (float32 output
+rounding) for float32 outputs."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+
+def _batch(oracle, specs, seed, dtype):
+    rng = np.random.default_rng(seed)
+    xs, ys = [], []
+    for i, (lx, ly, d, o) in enumerate(specs):
+        xs.append(oracle.brownian(1, lx, d, int(rng.integers(1 << 30)))[0])
+        ys.append(oracle.brownian(1, ly, d, int(rng.integers(1 << 30)))[0])
+    X = [torch.tensor(a, dtype=dtype, device="cuda") for a in xs]
+    Y = [torch.tensor(a, dtype=dtype, device="cuda") for a in ys]
+    return X, Y
+
+
+def _want(oracle, X, Y, orders, sx=None, sy=None):
+    out = []
+    for b, (x, y, o) in enumerate(zip(X, Y, orders)):
+        xin = x.double().cpu().numpy()[None]
+        yin = y.double().cpu().numpy()[None]
+        s1 = None if sx is None else np.array([float(sx[b])])
+        s2 = None if sy is None else np.array([float(sy[b])])
+        out.append(oracle.pairwise(xin, yin, o, s1, s2)[0])
+    return np.array(out)
+
+
+def _rel(got, want):
+    return float(np.max(np.abs(got - want) / np.abs(want)))
+
+
+SPECS = [
+    # (len x, len y, dim, order)
+    (16, 40, 4, 0), (40, 16, 4, 0), (33, 33, 4, 1), (70, 20, 4, 2), (9, 120, 4, 3),
+    (130, 150, 4, 2),   # two bands on the shorter side (516 rows)
+    (300, 90, 4, 1),    # swapped: 89 * 2 = 178 rows, 598 columns
+    (2, 2, 4, 0), (3, 7, 4, 5), (520, 517, 4, 0),
+]
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_ragged_matches_oracle(sig, oracle, dtype):
+    X, Y = _batch(oracle, SPECS, 1, dtype)
+    orders = [s[3] for s in SPECS]
+    got = sig.ragged.pairwise(X, Y, orders).double().cpu().numpy()
+    want = _want(oracle, X, Y, orders)
+    tol = 1e-9 if dtype is torch.float64 else 2.5e-7
+    assert _rel(got, want) <= tol
+
+
+def test_ragged_scales_and_dimension(sig, oracle):
+    specs = [(20 + 7 * i, 60 - 3 * i, 32, i % 4) for i in range(12)]
+    X, Y = _batch(oracle, specs, 2, torch.float64)
+    orders = [s[3] for s in specs]
+    sx = np.linspace(0.5, 1.5, 12)
+    sy = np.linspace(1.4, 0.6, 12)
+    got = sig.ragged.pairwise(X, Y, orders, x_scale=sx, y_scale=sy).cpu().numpy()
+    assert _rel(got, _want(oracle, X, Y, orders, sx, sy)) <= 1e-9
+
+
+def test_ragged_graph_replay_with_new_values(sig, oracle):
+    specs = [(30 + 11 * i, 25 + 5 * i, 8, (i % 3) + 1) for i in range(20)]
+    orders = [s[3] for s in specs]
+    solver = sig.ragged.RaggedPairwise([s[0] for s in specs], [s[1] for s in specs], orders, 8,
+                                       dtype=torch.float64, device="cuda")
+    X1, Y1 = _batch(oracle, specs, 3, torch.float64)
+    solver.load(X1, Y1)
+    solver.capture()
+    for seed in (4, 5):
+        X, Y = _batch(oracle, specs, seed, torch.float64)
+        solver.load(X, Y)
+        got = solver.solve().cpu().numpy()
+        assert _rel(got, _want(oracle, X, Y, orders)) <= 1e-9
+
+
+def test_ragged_long_pairs_split_into_band_pipelines(sig, oracle):
+    """Pairs of 4 to 8 bands run as pipelines of warps; mixed with short pairs."""
+    specs = [(512, 500, 8, 3), (300, 512, 8, 3), (130, 140, 8, 2)] + [(12 + i, 30 - i, 8, i % 3) for i in range(10)]
+    X, Y = _batch(oracle, specs, 7, torch.float32)
+    orders = [s[3] for s in specs]
+    solver = sig.ragged.RaggedPairwise([s[0] for s in specs], [s[1] for s in specs], orders, 8,
+                                       dtype=torch.float32, device="cuda")
+    assert int(solver.pair_bands.max()) >= 8
+    solver.load(X, Y)
+    got = solver.solve().double().cpu().numpy()
+    assert _rel(got, _want(oracle, X, Y, orders)) <= 2.5e-7
+    assert solver.error_flag() == 0
+
+
+def test_ragged_plan_is_consistent():
+    import sigpde_b200.torch.ragged as rg
+    pl = rg.plan([20, 600, 40], [500, 30, 41], [3, 1, 0], 32, 8)
+    # every pair's bands are consecutive and ordered; longest pair first
+    assert pl["item_pair"][0] == 0
+    for b in range(3):
+        idx = np.nonzero(pl["item_pair"] == b)[0]
+        assert np.all(np.diff(idx) == 1) and list(pl["item_band"][idx]) == list(range(pl["bands"][b]))
+
+
+def test_ragged_invalid_pairs_give_nan_without_faulting(sig, oracle):
+    from sigpde_b200 import _lib
+    specs = [(10, 12, 2, 1), (10, 12, 2, 1)]
+    solver = sig.ragged.RaggedPairwise([s[0] for s in specs], [s[1] for s in specs], [1, 1], 2,
+                                       dtype=torch.float64, device="cuda")
+    X, Y = _batch(oracle, specs, 6, torch.float64)
+    solver.load(X, Y)
+    solver.order[1] = 13  # outside [0, 12]: refused by the kernel, not solved
+    got = solver.solve().cpu().numpy()
+    assert np.isfinite(got[0]) and np.isnan(got[1])
+    assert solver.error_flag() == 1
+    assert _lib.lib().sigk_ragged_workspace_size(0, 0, 0, 2, 0, 0, 0) == 0
+
+
+@pytest.fixture(scope="module")
+def sig():
+    import sigpde_b200.torch as sig
+    return sig
