@@ -37,6 +37,9 @@ WORKLOADS = {
     "gram256": dict(nx=256, ny=256, L=128, d=8, order=2, seed_x=2001, seed_y=2002),
     # SigPDE pairwise over 4096 (x, y) pairs, lengths uniform in [16, 512] per path, d=32,
     # dyadic order uniform in {0, 1, 2, 3} per pair, Brownian N(0, 1/(L-1)) increments
+    # RobustSigPDE.gram(x) (normalisation + symmetric Gram), default normaliser, N=512 Brownian paths
+    # scaled by a per-path factor log-uniform in [0.5, 4], L=64, d=16, dyadic order 1
+    "robust512": dict(kind="robust", n=512, L=64, d=16, order=1, seed=512, smin=0.5, smax=4.0),
     "uneven4096": dict(kind="ragged", npairs=4096, lmin=16, lmax=512, d=32, orders=(0, 1, 2, 3), seed=4096),
 }
 
@@ -630,10 +633,148 @@ def run_reference_gpu_ragged(args, w):
                           note="one reference SigPDE.pairwise call per (len x, len y, order) bucket")), flush=True)
 
 
+# ----------------------------------------------------------------------------- robust Gram
+def robust_inputs(w):
+    from sigpde_b200 import synthetic
+    scales = synthetic.log_uniform(w["n"], w["smin"], w["smax"], w["seed"] + 1)
+    return synthetic.brownian_np(w["n"], w["L"], w["d"], w["seed"], scale=scales)
+
+
+def run_ours_robust(args, w):
+    import numpy as np
+    import torch
+    import sigpde_b200.torch as sig
+    from sigpde_b200 import _lib
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    x = robust_inputs(w)
+    X = torch.tensor(x, dtype=torch.float32, device=dev)
+    rk = sig.RobustSigPDE(sig.kernels.LinearKernel(), w["order"], precision=args.precision)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    out = rk.gram(X)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    times = timed_steps(torch, lambda: rk.gram(X), args.steps, args.warmup, flush, lambda: None)
+    clk = clocks.stop()
+    # the two phases separately: lambda root-find, then the scaled symmetric Gram
+    lam = rk.normalization(X)
+    t_norm = timed_steps(torch, lambda: rk.normalization(X), args.steps, args.warmup, flush, lambda: None)
+    k = sig.SigPDE(sig.kernels.LinearKernel(), w["order"], precision=args.precision)
+    t_gram = timed_steps(torch, lambda: k.gram(X, None, lam), args.steps, args.warmup, flush, lambda: None)
+    Xh = X.cpu().pin_memory()
+    Rh = torch.empty((w["n"], w["n"]), dtype=X.dtype).pin_memory()
+
+    def e2e_step():
+        Rh.copy_(rk.gram(Xh.to(dev, non_blocking=True)), non_blocking=True)
+
+    e2e_times = timed_steps(torch, e2e_step, args.steps, args.warmup, flush, lambda: None)
+    entries = w["n"] * w["n"]
+    ms = statistics.mean(times)
+    acc = cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle
+        xin = X.double().cpu().numpy()
+        lam_o = oracle.normalization(xin, w["order"])
+        lam_g = lam.double().cpu().numpy()
+        G = out.double().cpu().numpy()
+        rng = np.random.default_rng(1)
+        flat = rng.choice(entries, 64, replace=False)
+        want = oracle.gram(xin, xin, w["order"], lam_o, lam_o, pairs=flat)
+        got = G.reshape(-1)[flat]
+        nz = lam_o > 0
+        acc = {"lambda_max_rel_err": float(np.max(np.abs(lam_g[nz] - lam_o[nz]) / lam_o[nz])),
+               "lambda_zero_match": bool(np.all((lam_g == 0) == (lam_o == 0))),
+               "gram_max_rel_err": float(np.max(np.abs(got - want) / np.abs(want))),
+               "sample": "all 512 lambdas and 64 random Gram entries vs the float64 oracle"}
+        t0 = time.perf_counter()
+        oracle.normalization(xin, w["order"])
+        t_lam = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        sub = rng.choice(entries, 4096, replace=False)
+        oracle.gram(xin, xin, w["order"], lam_o, lam_o, pairs=sub)
+        t_g = time.perf_counter() - t0
+        cpu_ms = (t_lam + t_g * entries / 2 / 4096) * 1e3  # unique (lower-triangle) entries
+        cpu = {"value": entries / (cpu_ms * 1e-3), "unit": "entries/s", "cores": oracle.num_threads(),
+               "kind": "port", "sample": f"all 512 lambdas ({t_lam:.1f} s) + 4096 random Gram entries ({t_g:.1f} s), "
+                                         "extrapolated to the 131,328 unique entries"}
+    line = {
+        "metric": "gram_entries_per_s", "value": entries / (ms * 1e-3), "unit": "entries/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "p50_ms": percentile(times, 0.5),
+        "p99_ms": percentile(times, 0.99), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32",
+        "data": "synthetic Brownian paths (seeded PCG64), per-path scale log-uniform [0.5, 4], float32",
+        "config": {"workload": "RobustSigPDE.gram(x) N=512, L=64, d=16, dyadic_order=1, default normaliser",
+                   "global_batch": entries, "seq_len": w["L"], "parallelism": "single GPU",
+                   "precision": args.precision, "l2": "flushed between timed steps (256 MB write)"},
+        "unique_entries_per_s": w["n"] * (w["n"] + 1) / 2 / (ms * 1e-3),
+        "phases_ms": {"normalization": statistics.mean(t_norm), "scaled_symmetric_gram": statistics.mean(t_gram)},
+        "accuracy": acc,
+        "e2e": {"value": entries / (statistics.mean(e2e_times) * 1e-3), "unit": "entries/s",
+                "h2d_bytes_per_step": Xh.numel() * Xh.element_size(), "d2h_bytes_per_step": Rh.numel() * Rh.element_size(),
+                "ms_per_step": statistics.mean(e2e_times)},
+        "gpu_launches": 3 * args.steps, "clocks": clk, "lib": _lib.version(),
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+
+
+def run_reference_gpu_robust(args, w):
+    """The reference's Numba path: RobustSigPDE.gram(x) through its public API."""
+    import torch
+    ref_dir = os.path.join(ROOT, "baseline", "_ref")
+    base = {"impl": "reference-gpu", "metric": "gram_entries_per_s", "unit": "entries/s"}
+    if not os.path.isdir(os.path.join(ref_dir, "sigpde")):
+        print(json.dumps(dict(base, unavailable="reference not installed under baseline/_ref")), flush=True)
+        return
+    sys.path.insert(0, ref_dir)
+    import warnings
+    warnings.filterwarnings("ignore")
+    import sigpde.torch as refsig
+    dev = torch.device("cuda", 0)
+    X = torch.tensor(robust_inputs(w), dtype=torch.float32, device=dev)
+    rk = refsig.RobustSigPDE(refsig.kernels.LinearKernel(), w["order"])
+    out = rk.gram(X)
+    times = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rk.gram(X)
+        torch.cuda.synchronize()
+        times.append((time.perf_counter() - t0) * 1e3)
+    ms = statistics.mean(times)
+    acc = None
+    if not args.no_cpu_baseline:
+        import numpy as np
+        from oracle import oracle
+        xin = X.double().cpu().numpy()
+        lam_o = oracle.normalization(xin, w["order"])
+        lam_r = rk.normalization(X).double().cpu().numpy()
+        nz = lam_o > 0
+        acc = {"lambda_max_rel_err": float(np.max(np.abs(lam_r[nz] - lam_o[nz]) / lam_o[nz])),
+               "nonfinite_entries": int((~np.isfinite(out.double().cpu().numpy())).sum())}
+    entries = w["n"] * w["n"]
+    print(json.dumps(dict(base, value=entries / (ms * 1e-3), ms_per_step=ms, steps=args.steps, n_gpus=1,
+                          accuracy=acc, config={"workload": "RobustSigPDE.gram(x) N=512, L=64, d=16, order 1"},
+                          note="unmodified stojl/SigPDE, host-timed (it synchronises inside each call)")),
+          flush=True)
+
+
 def main():
     args = parse()
     w = WORKLOADS[args.workload]
     ragged = w.get("kind") == "ragged"
+    robust = w.get("kind") == "robust"
+    if robust:
+        if args.impl == "reference-gpu":
+            run_reference_gpu_robust(args, w)
+        elif args.impl == "ours":
+            run_ours_robust(args, w)
+        else:
+            print(json.dumps({"impl": "reference", "unavailable": "robust512 CPU arm: use the cpu_baseline of the "
+                              "default run"}), flush=True)
+        return
     if args.impl == "reference":
         if ragged:
             if int(os.environ.get("RANK", "0")) == 0:
