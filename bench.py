@@ -40,6 +40,14 @@ WORKLOADS = {
     # RobustSigPDE.gram(x) (normalisation + symmetric Gram), default normaliser, N=512 Brownian paths
     # scaled by a per-path factor log-uniform in [0.5, 4], L=64, d=16, dyadic order 1
     "robust512": dict(kind="robust", n=512, L=64, d=16, order=1, seed=512, smin=0.5, smax=4.0),
+    # Serving stream: Poisson arrivals (mean 200 req/s) of Gram requests, N log-uniform in [8, 1024],
+    # L log-uniform in [32, 1024], d in {2, 8, 32}, order in {0, 1, 2}, 30% RobustSigPDE (default
+    # normaliser), float32 Brownian paths; run as a finite trace of `requests` requests
+    "serve": dict(kind="serve", requests=120, rate=200.0, nmin=8, nmax=1024, lmin=32, lmax=1024, dims=(2, 8, 32),
+                  orders=(0, 1, 2), robust=0.3, seed=5),
+    # the same stream with N and L capped at 256 (service-sized requests)
+    "serve_light": dict(kind="serve", requests=400, rate=200.0, nmin=8, nmax=256, lmin=32, lmax=256, dims=(2, 8, 32),
+                        orders=(0, 1, 2), robust=0.3, seed=6),
     "uneven4096": dict(kind="ragged", npairs=4096, lmin=16, lmax=512, d=32, orders=(0, 1, 2, 3), seed=4096),
 }
 
@@ -58,6 +66,8 @@ def parse():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target length of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--burst", action="store_true", help="serving traces: every request arrives at t=0 "
+                    "(saturated throughput) instead of Poisson arrivals")
     return ap.parse_args()
 
 
@@ -761,11 +771,140 @@ def run_reference_gpu_robust(args, w):
           flush=True)
 
 
+# ----------------------------------------------------------------------------- serving trace
+def serve_trace(w, nreq=None):
+    """Seeded request trace: (arrival offsets in s, list of GramRequest with pinned host paths)."""
+    import numpy as np
+    import torch
+    from sigpde_b200 import synthetic
+    from sigpde_b200.serving import GramRequest
+    nreq = nreq or w["requests"]
+    rng = np.random.Generator(np.random.PCG64(w["seed"]))
+    gaps = rng.exponential(1.0 / w["rate"], nreq)
+    arrivals = np.cumsum(gaps) - gaps[0]
+    reqs = []
+    for i in range(nreq):
+        N = int(round(np.exp(rng.uniform(np.log(w["nmin"]), np.log(w["nmax"])))))
+        L = int(round(np.exp(rng.uniform(np.log(w["lmin"]), np.log(w["lmax"])))))
+        d = int(rng.choice(w["dims"]))
+        o = int(rng.choice(w["orders"]))
+        kind = "robust" if rng.random() < w["robust"] else "gram"
+        x = synthetic.brownian_np(N, L, d, int(rng.integers(1 << 31)))
+        reqs.append(GramRequest(x=torch.tensor(x, dtype=torch.float32).pin_memory(), order=o, kind=kind, rid=i))
+    return arrivals, reqs
+
+
+def _req_cells(r):
+    N, L, _ = r.x.shape
+    n = (L - 1) << r.order
+    return N * N * n * n
+
+
+def run_serve(args, w):
+    import numpy as np
+    import torch
+    from sigpde_b200 import _lib
+    from sigpde_b200.serving import GramServer, serve_sequential
+    torch.cuda.set_device(0)
+    arrivals, reqs = serve_trace(w)
+    if args.burst:
+        arrivals = np.zeros_like(arrivals)
+    cells = sum(_req_cells(r) for r in reqs)
+    entries = sum(r.x.shape[0] ** 2 for r in reqs)
+    # warm up the kernel variants once (first-use costs are not part of serving)
+    _, warm = serve_trace(w, 8)
+    serve_sequential(warm, args.precision)
+
+    def summarize(handles, t_first, t_last):
+        lat = [h.latency * 1e3 for h in handles]
+        span = t_last - t_first
+        return {"requests_per_s": len(handles) / span, "entries_per_s": entries / span, "cells_per_s": cells / span,
+                "p50_ms": percentile(lat, 0.5), "p99_ms": percentile(lat, 0.99), "makespan_s": span,
+                "errors": sum(h.error is not None for h in handles)}
+
+    # continuous-batching server, Poisson arrivals
+    clocks = ClockSampler(0)
+    clocks.start()
+    with GramServer(max_inflight=8, precision=args.precision) as srv:
+        t0 = time.perf_counter()
+        handles = []
+        for i, r in enumerate(reqs):
+            target = t0 + arrivals[i]
+            while time.perf_counter() < target:
+                time.sleep(max(0.0, min(1e-3, target - time.perf_counter())))
+            r.arrival = target
+            handles.append(srv.submit(r))
+        for h in handles:
+            h.wait(timeout=600)
+        peak = srv.peak_inflight
+    clk = clocks.stop()
+    served = summarize(handles, t0, max(h.t_done for h in handles))
+    served["peak_inflight"] = peak
+    # per-request plain launches, same arrivals
+    for r in reqs:
+        r.arrival = 0.0
+    t1 = time.perf_counter()
+    seq = serve_sequential(reqs, args.precision, arrivals=arrivals)
+    plain = summarize(seq, t1, max(h.t_done for h in seq))
+    # identical results alone and in the mix
+    same = all(np.array_equal(a.result.numpy(), b.result.numpy()) for a, b in zip(handles, seq))
+    # float64 spot checks on ~1% of the outputs (entries sampled across requests)
+    spot = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle
+        rng = np.random.default_rng(0)
+        errs = []
+        budget = max(8, entries // 100)
+        picks = rng.choice(len(reqs), min(len(reqs), 12), replace=False)
+        for k in picks:
+            r, h = reqs[k], handles[k]
+            N = r.x.shape[0]
+            x = r.x.double().numpy()
+            if r.kind == "robust":
+                lam = oracle.normalization(x, r.order)
+                npick = 2
+            else:
+                lam = None
+                npick = 4
+            for _ in range(npick):
+                i, j = int(rng.integers(N)), int(rng.integers(N))
+                if r.x.shape[1] * (1 << r.order) > 1200 and r.x.shape[0] > 256:
+                    continue  # keep the CPU check bounded
+                want = oracle.gram(x, x, r.order, lam, lam, pairs=[i * N + j])[0]
+                got = float(h.result[i, j])
+                errs.append(abs(got - want) / abs(want))
+        spot = {"checked_entries": len(errs), "max_rel_err": float(max(errs)) if errs else None,
+                "target_entries_1pct": int(budget),
+                "note": "entries sampled from 12 random requests (robust: lambda from the oracle too)"}
+    line = {
+        "metric": "served_requests_per_s", "value": served["requests_per_s"], "unit": "requests/s", "n_gpus": 1,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32",
+        "data": "synthetic Brownian paths (seeded PCG64), float32, pinned host memory",
+        "config": {"workload": f"serving trace: {len(reqs)} Gram requests, Poisson {w['rate']}/s, "
+                               f"N~logU[{w['nmin']},{w['nmax']}], L~logU[{w['lmin']},{w['lmax']}], d in {{2,8,32}}, "
+                               "order in {0,1,2}, 30% robust" + (" (burst: all at t=0)" if args.burst else ""),
+                   "parallelism": "single GPU, 8 in-flight streams, HBM-footprint admission"},
+        "served": served, "per_request_plain_launches": plain,
+        "throughput_ratio_vs_plain": served["requests_per_s"] / plain["requests_per_s"],
+        "results_identical_alone_and_in_mix": same, "fp64_spot_check": spot,
+        "trace_cells": cells, "trace_entries": entries, "clocks": clk, "lib": _lib.version(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     w = WORKLOADS[args.workload]
     ragged = w.get("kind") == "ragged"
     robust = w.get("kind") == "robust"
+    if w.get("kind") == "serve":
+        if args.impl == "ours":
+            run_serve(args, w)
+        else:
+            print(json.dumps({"impl": args.impl, "unavailable": "serving trace: the reference has no server; "
+                              "the per-request plain-launch arm is inside the default run"}), flush=True)
+        return
     if robust:
         if args.impl == "reference-gpu":
             run_reference_gpu_robust(args, w)

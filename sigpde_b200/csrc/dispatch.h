@@ -24,7 +24,8 @@ using DeltaFn = void (*)(const void *, int64_t, int64_t, int64_t, int64_t, doubl
 // R in {2,4,8,16} rows per lane; O = min(order, 4).
 PairFn get_pair_kernel_f64(bool in64, bool from_inc, int R, int O);
 PairFn get_pair_kernel_f32(bool in64, bool from_inc, int R, int O);
-NormFn get_norm_kernel(bool in64, bool from_inc, int R, int O);
+// mode: kNormDelta, kNormGiven or kNormTile (sigk_kernels.cuh)
+NormFn get_norm_kernel(bool in64, int mode, int R, int O);
 // D: dimension padded to a power of two in {2,...,32}; returns null unless
 // the lane's register tile (coarse rows per lane) * D <= 32.
 StreamFn get_stream_reg_kernel(bool f64cells, int R, int O, int D);

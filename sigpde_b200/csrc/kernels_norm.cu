@@ -4,32 +4,40 @@
 
 namespace sigk {
 namespace {
-template <typename TIN, int R, bool FI>
+template <typename TIN, int R, int M>
 NormFn by_o(int O)
 {
     switch (O) {
-    case 0: return normalize_kernel<TIN, R, 0, FI>;
-    case 1: return normalize_kernel<TIN, R, 1, FI>;
-    case 2: return normalize_kernel<TIN, R, 2, FI>;
-    case 3: return normalize_kernel<TIN, R, 3, FI>;
-    default: return normalize_kernel<TIN, R, 4, FI>;
+    case 0: return normalize_kernel<TIN, R, 0, M>;
+    case 1: return normalize_kernel<TIN, R, 1, M>;
+    case 2: return normalize_kernel<TIN, R, 2, M>;
+    case 3: return normalize_kernel<TIN, R, 3, M>;
+    default: return normalize_kernel<TIN, R, 4, M>;
     }
 }
-template <typename TIN, bool FI>
+template <typename TIN, int M>
 NormFn by_r(int R, int O)
 {
     switch (R) {
-    case 2: return by_o<TIN, 2, FI>(O);
-    case 4: return by_o<TIN, 4, FI>(O);
-    case 8: return by_o<TIN, 8, FI>(O);
-    default: return by_o<TIN, 16, FI>(O);
+    case 2: return by_o<TIN, 2, M>(O);
+    case 4: return by_o<TIN, 4, M>(O);
+    case 8: return by_o<TIN, 8, M>(O);
+    default: return by_o<TIN, 16, M>(O);
+    }
+}
+template <typename TIN>
+NormFn by_mode(int mode, int R, int O)
+{
+    switch (mode) {
+    case kNormGiven: return by_r<TIN, kNormGiven>(R, O);
+    case kNormTile: return by_r<TIN, kNormTile>(R, O);
+    default: return by_r<TIN, kNormDelta>(R, O);
     }
 }
 } // namespace
 
-NormFn get_norm_kernel(bool in64, bool from_inc, int R, int O)
+NormFn get_norm_kernel(bool in64, int mode, int R, int O)
 {
-    if (in64) return from_inc ? by_r<double, true>(R, O) : by_r<double, false>(R, O);
-    return from_inc ? by_r<float, true>(R, O) : by_r<float, false>(R, O);
+    return in64 ? by_mode<double>(mode, R, O) : by_mode<float>(mode, R, O);
 }
 } // namespace sigk

@@ -161,7 +161,6 @@ PairFn pick_pair(int precision, int dtype, bool from_inc, int R, int O)
                                        : get_pair_kernel_f32(in64, from_inc, R, O);
 }
 
-NormFn pick_norm(int dtype, bool from_inc, int R, int O) { return get_norm_kernel(dtype == SIGK_F64, from_inc, R, O); }
 
 // ------------------------------------------------------------------ launching
 struct OccKey {
@@ -194,7 +193,14 @@ int blocks_per_sm(const void *fn, size_t smem, int *out)
         }
     }
     if (smem > 48 * 1024) {
-        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        // Opt the kernel in to the device maximum (not to this request's size): the
+        // attribute is per function, and a later, smaller request must not lower it
+        // below the size of an earlier one that is still cached above.
+        int optin = 0;
+        e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
+        if (smem > (size_t)optin) return fail(SIGK_ELAUNCH, "kernel needs %zu bytes of shared memory (max %d)", smem, optin);
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
         if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
     }
     int nb = 0;
@@ -371,6 +377,43 @@ int run_pairs(int op, const void *x, const void *y, int64_t nx, int64_t ny, int6
     return launch(fn, p, p.nitems, pl.stage_bytes_per_warp * kWarpsPerBlock, stream);
 }
 
+// Normalisation plan: the increment source (a shared-memory tile of the
+// path's coarse increments when it fits, else precomputed differences, or the
+// caller's increments), the variant, shared memory and workspace layout
+// (boundary rows for multi-band paths, then the float64 differences).
+constexpr size_t kNormTileBytesPerWarp = 48 * 1024;
+
+struct NormPlan {
+    int mode, R, O, nbands;
+    int64_t tile_pitch, bnd_stride;
+    size_t smem_per_warp, bnd_bytes, dx_off, ws_bytes;
+};
+
+NormPlan norm_plan(int64_t n, int64_t nc, int64_t d, int order, bool from_inc)
+{
+    NormPlan q{};
+    const int64_t tile_pitch = nc | 1; // odd pitch: neighbouring lanes' rows fall in different banks
+    const size_t tile = (size_t)nc * (size_t)tile_pitch * sizeof(double);
+    if (from_inc)
+        q.mode = kNormGiven;
+    else if (tile <= kNormTileBytesPerWarp && !env_flag("SIGK_NO_NORM_TILE"))
+        q.mode = kNormTile;
+    else
+        q.mode = kNormDelta;
+    // only the difference mode stages rows of dx (and may shrink R to fit them)
+    Plan pl = make_plan(SIGK_OP_NORMALIZE, n, n, nc, nc, d, order, 8, q.mode != kNormDelta);
+    q.R = pl.R;
+    q.O = pl.O;
+    q.nbands = pl.nbands;
+    q.bnd_stride = pl.bnd_stride;
+    q.bnd_bytes = align256(pl.ws_bytes);
+    q.tile_pitch = tile_pitch;
+    q.smem_per_warp = q.mode == kNormTile ? tile : q.mode == kNormDelta ? pl.stage_bytes_per_warp : 0;
+    q.dx_off = q.bnd_bytes;
+    q.ws_bytes = from_inc ? q.bnd_bytes : q.dx_off + align256((size_t)n * (size_t)d * (size_t)nc * sizeof(double));
+    return q;
+}
+
 } // namespace
 } // namespace sigk
 
@@ -393,6 +436,7 @@ size_t sigk_workspace_size(int op, int64_t n_x, int64_t n_y, int64_t len_x, int6
         n_y = n_x;
     }
     if (op == SIGK_OP_PAIRWISE) n_y = n_x;
+    if (op == SIGK_OP_NORMALIZE) return norm_plan(n_x, len_x - 1, dim > 0 ? dim : 1, order, dim == 0).ws_bytes;
     // dim == 0 selects the plan of the *_inc entry points (no dx staging)
     Plan pl = make_plan(op, n_x, n_y, len_x - 1, len_y - 1, dim > 0 ? dim : 1, order, tsize_of(precision), dim == 0);
     return pl.ws_bytes;
@@ -422,10 +466,12 @@ int sigk_gram_sym(const void *x, int64_t n, int64_t len, int64_t dim, int dtype,
                      precision, workspace, workspace_bytes, (cudaStream_t)stream);
 }
 
-static int run_normalize(const void *x, const void *inc, int64_t n, int64_t nc, int64_t d, int64_t s0, int64_t s1,
-                         int64_t s2, int dtype, int order, double static_scale, double *knorm, const double *fnorm,
-                         double tol, int maxit, void *lam, int *iters, void *ws, size_t ws_bytes,
-                         cudaStream_t stream)
+// Shared body of sigk_normalize, sigk_normalize_inc and sigk_self_norms
+// (maxit = 0, no lambda output).
+static int normalize_impl(const void *x, const void *inc, int64_t n, int64_t nc, int64_t d, int64_t s0, int64_t s1,
+                          int64_t s2, int dtype, int order, double static_scale, double *knorm, const double *fnorm,
+                          double tol, int maxit, void *lam, bool need_lam, int *iters, void *ws, size_t ws_bytes,
+                          cudaStream_t stream)
 {
     int st = check_common(dtype, SIGK_PREC_FP64, order);
     if (st) return st;
@@ -441,14 +487,32 @@ static int run_normalize(const void *x, const void *inc, int64_t n, int64_t nc, 
         if (d < 1) return fail(SIGK_EINVAL, "dim must be >= 1");
         if ((st = check_dev(x, "x", false))) return st;
     }
-    if ((st = check_dev(lam, "lam", false)) || (st = check_dev(knorm, "knorm", true)) ||
+    if ((st = check_dev(lam, "lam", !need_lam)) || (st = check_dev(knorm, "knorm", true)) ||
         (st = check_dev(fnorm, "fnorm", true)) || (st = check_dev(iters, "iters", true)))
         return st;
     if (fnorm && !knorm) return fail(SIGK_EINVAL, "fnorm given without knorm");
-    Plan pl = make_plan(SIGK_OP_NORMALIZE, n, n, nc, nc, from_inc ? 1 : d, order, 8, from_inc);
-    if ((st = check_ws(pl, ws, ws_bytes))) return st;
+    NormPlan q = norm_plan(n, nc, d, order, from_inc);
+    if (q.ws_bytes) {
+        if (!ws || ws_bytes < q.ws_bytes)
+            return fail(SIGK_ENOMEM, "workspace of %zu bytes needed (got %zu)", q.ws_bytes, ws ? ws_bytes : 0);
+        if (((uintptr_t)ws & 255) != 0) return fail(SIGK_EINVAL, "workspace must be 256-byte aligned");
+    }
+    unsigned char *wsb = reinterpret_cast<unsigned char *>(ws);
+    double *dx = nullptr;
+    if (!from_inc) { // unscaled float64 differences, dimension-major (the kernel applies the scale)
+        dx = reinterpret_cast<double *>(wsb + q.dx_off);
+        DeltaFn delta = get_delta_kernel(true, dtype == SIGK_F64);
+        const int64_t total = n * nc * d;
+        int64_t blocks = (total + 255) / 256;
+        if (blocks > (int64_t)sm_count() * 8) blocks = (int64_t)sm_count() * 8;
+        delta<<<(unsigned)blocks, 256, 0, stream>>>(x, n, nc + 1, d, d, 1.0, nullptr, dx);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(e, "delta kernel launch");
+    }
     NormParams p{};
     p.x = x;
+    p.dx = dx;
+    p.tile_pitch = q.tile_pitch;
     p.n = n;
     p.nc = nc;
     p.d = d;
@@ -464,47 +528,32 @@ static int run_normalize(const void *x, const void *inc, int64_t n, int64_t nc, 
     p.maxit = maxit;
     p.lam = lam;
     p.iters = iters;
-    p.bnd = pl.nbands > 1 ? ws : nullptr;
-    p.bnd_stride = pl.bnd_stride;
-    p.stage_smem = pl.stage_bytes_per_warp > 0;
-    NormFn fn = pick_norm(dtype, from_inc, pl.R, pl.O);
-    return launch(fn, p, n, pl.stage_bytes_per_warp * kWarpsPerBlock, stream);
+    p.bnd = q.nbands > 1 ? ws : nullptr;
+    p.bnd_stride = q.bnd_stride;
+    p.stage_smem = q.smem_per_warp > 0;
+    NormFn fn = get_norm_kernel(dtype == SIGK_F64, q.mode, q.R, q.O);
+    return launch(fn, p, n, q.smem_per_warp * kWarpsPerBlock, stream);
+}
+
+static int run_normalize(const void *x, const void *inc, int64_t n, int64_t nc, int64_t d, int64_t s0, int64_t s1,
+                         int64_t s2, int dtype, int order, double static_scale, double *knorm, const double *fnorm,
+                         double tol, int maxit, void *lam, int *iters, void *ws, size_t ws_bytes,
+                         cudaStream_t stream)
+{
+    return normalize_impl(x, inc, n, nc, d, s0, s1, s2, dtype, order, static_scale, knorm, fnorm, tol, maxit, lam,
+                          true, iters, ws, ws_bytes, stream);
 }
 
 int sigk_self_norms(const void *x, int64_t n, int64_t len, int64_t dim, int dtype, int order, double static_scale,
                     double *knorm, void *workspace, size_t workspace_bytes, sigk_stream_t stream)
 {
     // k(x,x) with float64 cells, written as float64; NaN -> +inf is applied by
-    // the normalisation kernel with maxit = 0 (no bracket iterations).
+    // the normalisation kernel, which with maxit = 0 runs no bracket iterations.
     int st = check_dev(knorm, "knorm", false);
     if (st) return st;
-    if (!x) return fail(SIGK_EINVAL, "x is NULL");
-    // lam output is required by the kernel; reuse knorm's storage would alias,
-    // so run the pair kernel directly with float64 output instead.
-    st = check_common(dtype, SIGK_PREC_FP64, order);
-    if (st) return st;
-    if (n < 1 || len < 2 || dim < 1) return fail(SIGK_EINVAL, "bad shape (n=%lld len=%lld dim=%lld)",
-                                                 (long long)n, (long long)len, (long long)dim);
-    if ((st = check_dev(x, "x", false))) return st;
-    Plan pl = make_plan(SIGK_OP_NORMALIZE, n, n, len - 1, len - 1, dim, order, 8, false);
-    if ((st = check_ws(pl, workspace, workspace_bytes))) return st;
-    NormParams p{};
-    p.x = x;
-    p.n = n;
-    p.nc = len - 1;
-    p.d = dim;
-    p.order = order;
-    p.fscale = static_scale * std::ldexp(1.0, -2 * order);
-    p.knorm = knorm;
-    p.fnorm = nullptr;
-    p.tol = 0;
-    p.maxit = 0;
-    p.lam = nullptr;
-    p.bnd = pl.nbands > 1 ? workspace : nullptr;
-    p.bnd_stride = pl.bnd_stride;
-    p.stage_smem = pl.stage_bytes_per_warp > 0;
-    NormFn fn = pick_norm(dtype, false, pl.R, pl.O);
-    return launch(fn, p, n, pl.stage_bytes_per_warp * kWarpsPerBlock, (cudaStream_t)stream);
+    if (len < 2) return fail(SIGK_EINVAL, "path length must be >= 2");
+    return normalize_impl(x, nullptr, n, len - 1, dim, 0, 0, 0, dtype, order, static_scale, knorm, nullptr, 0.0, 0,
+                          nullptr, false, nullptr, workspace, workspace_bytes, (cudaStream_t)stream);
 }
 
 int sigk_normalize(const void *x, int64_t n, int64_t len, int64_t dim, int dtype, int order, double static_scale,

@@ -118,8 +118,12 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) pair_kernel(PairParams p)
     }
 }
 
+enum : int { kNormDelta = 0, kNormGiven = 1, kNormTile = 2 };
+
 struct NormParams {
     const void *x;
+    const double *dx;   // delta / tile modes: path differences (n, d, nc), dimension-major, unscaled
+    int64_t tile_pitch; // tile mode: row pitch (elements) of the shared-memory increment tile
     int64_t n;
     int64_t nc;
     int64_t d;
@@ -142,7 +146,7 @@ struct NormParams {
 // the argument order of sigpde/torch/kernel.py:186-193: g(l) = k(l x) - f(k),
 // g(0) = 1 - f(k), g(1) = k - f(k).  All bracket state is float64 and
 // warp-uniform; the PDE solve returns the same value in every lane.
-template <typename TIN, int R, int O, bool FROM_INC>
+template <typename TIN, int R, int O, int MODE>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) normalize_kernel(NormParams p)
 {
     using T = double;
@@ -157,25 +161,45 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) normalize_kernel(NormPara
     TIN *lam_out = reinterpret_cast<TIN *>(p.lam);
 
     for (int64_t b = gwarp; b < p.n; b += nwarps) {
-        PathIncs<T, TIN, BS::RC> psrc;
+        DeltaIncs<T, BS::RC> dsrc;
         GivenIncs<T, TIN, BS::RC> gsrc;
-        if constexpr (FROM_INC) {
+        TileIncs<T, BS::RC> tsrc;
+        if constexpr (MODE == kNormGiven) {
             gsrc.inc = reinterpret_cast<const TIN *>(p.inc) + b * p.is0;
             gsrc.si = p.is1;
             gsrc.sj = p.is2;
+        } else if constexpr (MODE == kNormDelta) {
+            dsrc.dX = p.dx + b * p.d * p.nc;
+            dsrc.dY = dsrc.dX;
+            dsrc.d = p.d;
+            dsrc.ncy = p.nc;
+            dsrc.dxs = p.stage_smem ? reinterpret_cast<T *>(smem_raw) + (int64_t)wib * BS::RC * p.d * 32 : nullptr;
         } else {
-            psrc.X = reinterpret_cast<const TIN *>(p.x) + b * (p.nc + 1) * p.d;
-            psrc.Y = psrc.X;
-            psrc.d = p.d;
-            psrc.dxs = p.stage_smem ? reinterpret_cast<T *>(smem_raw) + (int64_t)wib * BS::RC * p.d * 32 : nullptr;
+            // build this path's coarse increment tile once: tile[cj][ci] = <dx_ci, dx_cj>
+            T *tile = reinterpret_cast<T *>(smem_raw) + (int64_t)wib * p.nc * p.tile_pitch;
+            const double *dxb = p.dx + b * p.d * p.nc;
+            __syncwarp(); // the previous path's solves are done with the tile
+            for (int64_t e = lane; e < p.nc * p.nc; e += 32) {
+                const int64_t cj = e / p.nc;
+                const int64_t ci = e - cj * p.nc;
+                T acc = T(0);
+                for (int64_t k = 0; k < p.d; ++k) acc = fma(dxb[k * p.nc + ci], dxb[k * p.nc + cj], acc);
+                tile[cj * p.tile_pitch + ci] = acc;
+            }
+            __syncwarp();
+            tsrc.tile = tile;
+            tsrc.pitch = p.tile_pitch;
         }
         auto solve = [&](double scale) -> double {
-            if constexpr (FROM_INC) {
+            if constexpr (MODE == kNormGiven) {
                 gsrc.fscale = p.fscale * scale;
                 return warp_solve<T, R, O>(g, gsrc, bnd);
+            } else if constexpr (MODE == kNormDelta) {
+                dsrc.fscale = p.fscale * scale;
+                return warp_solve<T, R, O>(g, dsrc, bnd);
             } else {
-                psrc.fscale = p.fscale * scale;
-                return warp_solve<T, R, O>(g, psrc, bnd);
+                tsrc.fscale = p.fscale * scale;
+                return warp_solve<T, R, O>(g, tsrc, bnd);
             }
         };
 

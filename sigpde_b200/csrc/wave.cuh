@@ -187,6 +187,7 @@ struct DeltaIncs {
     T *dxs;      // this warp's staging area: RC * d * 32 values, or null
     int64_t ci0 = 0, ncx = 0, ncy = 0;
     bool rc_per_row = false;
+    T fscale = T(1); // extra factor on every increment (the robust kernel's t^2)
 
     __device__ __forceinline__ void stage(int64_t ci0_, int64_t ncx_, int lane, bool rc_per_row_)
     {
@@ -223,6 +224,38 @@ struct DeltaIncs {
                     if (ci < ncx) c[rc] = fma(dX[k * ncx + ci], v, c[rc]);
                 }
             }
+        }
+#pragma unroll
+        for (int rc = 0; rc < RC; ++rc) c[rc] *= fscale;
+    }
+};
+
+// Source of increments from a coarse increment tile held in shared memory,
+// tile[cj * pitch + ci], times fscale.  Used when the same pair is solved many
+// times (the robust root-find re-solves a path's self-kernel every iteration
+// with a new scale): the tile is built once per path.
+template <typename T, int RC>
+struct TileIncs {
+    const T *tile;
+    int64_t pitch;
+    T fscale;
+    int64_t ci0 = 0, ncx = 0;
+    bool rc_per_row = false;
+
+    __device__ __forceinline__ void stage(int64_t ci0_, int64_t ncx_, int, bool rc_per_row_)
+    {
+        ci0 = ci0_;
+        ncx = ncx_;
+        rc_per_row = rc_per_row_;
+    }
+
+    __device__ __forceinline__ void column(int64_t cj, int, T (&c)[RC]) const
+    {
+        const T *col = tile + cj * pitch;
+#pragma unroll
+        for (int rc = 0; rc < RC; ++rc) {
+            const int64_t ci = ci0 + (rc_per_row ? rc : 0);
+            c[rc] = (ci < ncx) ? col[ci] * fscale : T(0);
         }
     }
 };

@@ -1,0 +1,347 @@
+"""Request server for signature-kernel Gram solves with continuous batching.
+
+Requests (a Gram k(x_i, y_j), a symmetric Gram k(x_i, x_j), or a robust Gram
+with per-path normalisation) arrive at any time.  A scheduler thread admits
+them in arrival order as soon as two resources allow it:
+
+* a slot: one of `max_inflight` CUDA streams is free;
+* device memory: the request's footprint (paths, result, kernel workspace,
+  robust scratch), estimated before admission, fits in the HBM budget next to
+  the footprints of the requests already on the device.
+
+Among the requests waiting, the cheapest (fewest PDE cells) is admitted
+first; a request that has waited longer than `max_wait_s` goes first
+regardless, so nothing starves.  An admitted request is enqueued on its own
+stream: host-to-device copy of its paths (pinned staging), the solve with the
+kernel variant that fits its shape, and the device-to-host copy of the
+result.  A large Gram is solved in row blocks of about `chunk_cells` cells,
+one launch each: a persistent kernel holds every SM until it ends, so
+chunking lets requests admitted meanwhile get SMs between chunks instead of
+waiting for the whole large request.  Requests admitted while others are
+running execute concurrently on the device, and copies overlap compute.  Completion
+is detected with CUDA events; the result, the timestamps (arrival, admission,
+completion) and any error are delivered on the request's handle.
+
+Every solve is deterministic and a request's kernels only read its own
+buffers, so a request's result does not depend on what else is in flight.
+
+`serve_sequential` runs the same requests one at a time (copy in, solve, copy
+out, synchronise) -- the per-request plain-launch baseline.
+"""
+from __future__ import annotations
+
+import collections
+import dataclasses
+import queue
+import threading
+import time
+from typing import Optional
+
+import torch
+
+from . import _lib
+from .torch import kernel as _k
+from .torch import static_kernels as _sk
+
+__all__ = ["GramRequest", "RequestHandle", "GramServer", "serve_sequential", "footprint_bytes", "request_cells"]
+
+
+@dataclasses.dataclass
+class GramRequest:
+    """One request.  x (and y) are (N, L, d) float32/float64 tensors, on the
+    host (pinned or pageable) or on the device.  kind: "gram" (k(x_i, y_j),
+    or the symmetric Gram when y is None) or "robust" (RobustSigPDE.gram with
+    the default normaliser)."""
+
+    x: torch.Tensor
+    y: Optional[torch.Tensor] = None
+    order: int = 0
+    kind: str = "gram"
+    rid: int = -1
+    arrival: float = 0.0  # seconds on the server's clock (time.perf_counter)
+
+
+class RequestHandle:
+    """Result of one request: `wait()` returns the (Nx, Ny) host tensor or raises."""
+
+    def __init__(self, req: GramRequest):
+        self.req = req
+        self._done = threading.Event()
+        self.cost = 0
+        self.result: Optional[torch.Tensor] = None
+        self.error: Optional[BaseException] = None
+        self.t_admit = None
+        self.t_done = None
+
+    def _finish(self, result=None, error=None):
+        self.result = result
+        self.error = error
+        self.t_done = time.perf_counter()
+        self._done.set()
+
+    def done(self) -> bool:
+        return self._done.is_set()
+
+    def wait(self, timeout=None):
+        if not self._done.wait(timeout):
+            raise TimeoutError(f"request {self.req.rid} not finished")
+        if self.error is not None:
+            raise self.error
+        return self.result
+
+    @property
+    def latency(self) -> Optional[float]:
+        return None if self.t_done is None else self.t_done - self.req.arrival
+
+
+def footprint_bytes(req: GramRequest, precision: str = "fp64") -> int:
+    """Device bytes a request holds while in flight (paths, result, workspace, robust scratch)."""
+    x = req.x
+    y = x if req.y is None else req.y
+    nx, lx, d = x.shape
+    ny, ly = y.shape[0], y.shape[1]
+    es = x.element_size()
+    prec = _k._PREC[precision]
+    dt = _k._dtype_code(x)
+    sym = req.y is None
+    op = _lib.SIGK_OP_GRAM_SYM if sym else _lib.SIGK_OP_GRAM
+    ws = _lib.lib().sigk_workspace_size(op, nx, ny, lx, ly, d, req.order, dt, prec)
+    total = x.numel() * es + (0 if sym else y.numel() * es) + nx * ny * es + ws
+    if req.kind == "robust":
+        nws = _lib.lib().sigk_workspace_size(_lib.SIGK_OP_NORMALIZE, nx, nx, lx, lx, d, req.order, dt, prec)
+        total += nws + (nx + ny) * (8 + es)
+    return int(total)
+
+
+class _Inflight:
+    __slots__ = ("handle", "stream", "event", "bytes", "out_host", "keep")
+
+    def __init__(self, handle, stream, event, nbytes, out_host, keep):
+        self.handle = handle
+        self.stream = stream
+        self.event = event
+        self.bytes = nbytes
+        self.out_host = out_host
+        self.keep = keep
+
+
+def request_cells(req: GramRequest) -> int:
+    """Refined PDE cells of a request (its cost, for ordering and chunking)."""
+    x = req.x
+    y = x if req.y is None else req.y
+    n = (x.shape[1] - 1) << req.order
+    m = (y.shape[1] - 1) << req.order
+    return int(x.shape[0]) * int(y.shape[0]) * n * m
+
+
+def _solve_on_stream(req: GramRequest, precision: str, device, stream, chunk_cells: int = 0):
+    """Enqueue copy-in, solve and copy-out of one request on `stream`.
+    Returns (pinned host result, tensors to keep alive until the event).
+    chunk_cells > 0 splits a large (non-symmetric or robust) Gram into row
+    blocks of about that many cells, one launch each."""
+    with torch.cuda.stream(stream):
+        x = req.x.to(device, non_blocking=True)
+        y = None if req.y is None else req.y.to(device, non_blocking=True)
+        lin = _sk.LinearKernel()
+        if req.kind not in ("gram", "robust"):
+            raise ValueError(f"unknown request kind {req.kind!r}")
+        k = _k.SigPDE(lin, req.order, precision=precision)
+        sx = sy = None
+        if req.kind == "robust":
+            rk = _k.RobustSigPDE(lin, req.order, precision=precision)
+            sx = rk.normalization(x)
+            sy = sx if y is None else rk.normalization(y)
+        cells = request_cells(req)
+        rows = x.shape[0]
+        if chunk_cells > 0 and cells > chunk_cells and rows > 1:
+            step = max(1, int(rows * chunk_cells // cells))
+            if y is None:
+                # symmetric: per row block, the diagonal block with the symmetric kernel and the
+                # block to its left with x_i on the rows -- the orientation the symmetric kernel
+                # uses for i >= j -- mirrored, so every entry is the unchunked entry bit for bit
+                out = torch.empty((rows, rows), dtype=x.dtype, device=device)
+                for i0 in range(0, rows, step):
+                    i1 = min(rows, i0 + step)
+                    s_blk = None if sx is None else sx[i0:i1]
+                    out[i0:i1, i0:i1] = k.gram(x[i0:i1], None, s_blk)
+                    if i0 > 0:
+                        left = k.gram(x[i0:i1], x[:i0], s_blk, None if sx is None else sx[:i0])
+                        out[i0:i1, :i0] = left
+                        out[:i0, i0:i1] = left.t()
+            else:
+                out = torch.empty((rows, y.shape[0]), dtype=x.dtype, device=device)
+                for i0 in range(0, rows, step):
+                    i1 = min(rows, i0 + step)
+                    out[i0:i1] = k.gram(x[i0:i1], y, None if sx is None else sx[i0:i1], sy)
+        else:
+            out = k.gram(x, y, sx, sy if y is not None else None)
+        host = torch.empty(out.shape, dtype=out.dtype, pin_memory=True)
+        host.copy_(out, non_blocking=True)
+    return host, (x, y, out, sx, sy)
+
+
+class GramServer:
+    """Continuous-batching server (see the module docstring).
+
+    hbm_budget_bytes: device memory the in-flight requests may hold together
+    (default: 80% of the free memory at start).  A request larger than the
+    whole budget fails at admission with MemoryError instead of waiting
+    forever.
+    """
+
+    def __init__(self, device="cuda", max_inflight: int = 8, hbm_budget_bytes: Optional[int] = None,
+                 precision: str = "fp64", poll_interval_s: float = 50e-6, chunk_cells: int = 2 * 10 ** 12,
+                 max_wait_s: float = 2.0):
+        self.device = torch.device(device)
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        self.precision = precision
+        self.max_inflight = int(max_inflight)
+        if hbm_budget_bytes is None:
+            free, _ = torch.cuda.mem_get_info(self.device)
+            hbm_budget_bytes = int(0.8 * free)
+        self.budget = int(hbm_budget_bytes)
+        self.poll = poll_interval_s
+        self.chunk_cells = int(chunk_cells)
+        self.max_wait_s = float(max_wait_s)
+        self._q: "queue.Queue[RequestHandle]" = queue.Queue()
+        self._pending: collections.deque = collections.deque()
+        self._inflight: list = []
+        self._streams = [torch.cuda.Stream(self.device) for _ in range(self.max_inflight)]
+        self._free_streams = list(self._streams)
+        self._used = 0
+        self._stop = threading.Event()
+        self._ids = 0
+        self._lock = threading.Lock()
+        self.peak_inflight = 0
+        self.peak_bytes = 0
+        self._thread = threading.Thread(target=self._run, name="sigk-server", daemon=True)
+        self._thread.start()
+
+    # ------------------------------------------------------------------ client side
+    def submit(self, req: GramRequest) -> RequestHandle:
+        with self._lock:
+            if req.rid < 0:
+                req.rid = self._ids
+            self._ids += 1
+        if not req.arrival:
+            req.arrival = time.perf_counter()
+        h = RequestHandle(req)
+        try:
+            h.cost = request_cells(req)
+        except Exception:
+            h.cost = 0
+        self._q.put(h)
+        return h
+
+    def close(self, wait: bool = True):
+        self._stop.set()
+        if wait:
+            self._thread.join()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ------------------------------------------------------------------ scheduler
+    def _next(self):
+        """The waiting request to admit next: one that waited too long, else the cheapest."""
+        now = time.perf_counter()
+        old = [h for h in self._pending if now - h.req.arrival > self.max_wait_s]
+        pool = old if old else self._pending
+        return min(pool, key=lambda h: (h.req.arrival if old else h.cost))
+
+    def _admit(self):
+        while self._pending and self._free_streams:
+            h = self._next()
+            try:
+                need = footprint_bytes(h.req, self.precision)
+            except Exception as e:  # malformed request: fail it, keep serving
+                self._pending.remove(h)
+                h._finish(error=e)
+                continue
+            if need > self.budget:
+                self._pending.remove(h)
+                h._finish(error=MemoryError(f"request {h.req.rid} needs {need} bytes, budget is {self.budget}"))
+                continue
+            if self._used + need > self.budget:
+                return  # wait for memory to free up
+            self._pending.remove(h)
+            stream = self._free_streams.pop()
+            h.t_admit = time.perf_counter()
+            try:
+                with torch.cuda.device(self.device):
+                    out_host, keep = _solve_on_stream(h.req, self.precision, self.device, stream,
+                                                      self.chunk_cells)
+                    ev = torch.cuda.Event()
+                    ev.record(stream)
+            except Exception as e:
+                self._free_streams.append(stream)
+                h._finish(error=e)
+                continue
+            self._used += need
+            self._inflight.append(_Inflight(h, stream, ev, need, out_host, keep))
+            self.peak_inflight = max(self.peak_inflight, len(self._inflight))
+            self.peak_bytes = max(self.peak_bytes, self._used)
+
+    def _reap(self):
+        still = []
+        for f in self._inflight:
+            if f.event.query():
+                self._used -= f.bytes
+                self._free_streams.append(f.stream)
+                f.keep = None
+                f.handle._finish(result=f.out_host)
+            else:
+                still.append(f)
+        self._inflight = still
+
+    def _run(self):
+        torch.cuda.set_device(self.device)
+        while True:
+            while True:
+                try:
+                    self._pending.append(self._q.get_nowait())
+                except queue.Empty:
+                    break
+            self._reap()
+            self._admit()
+            if self._stop.is_set() and not self._pending and not self._inflight and self._q.empty():
+                return
+            if not self._inflight and not self._pending:
+                try:
+                    self._pending.append(self._q.get(timeout=0.01))
+                except queue.Empty:
+                    pass
+            else:
+                time.sleep(self.poll)
+
+
+def serve_sequential(requests, precision: str = "fp64", device="cuda", arrivals=None):
+    """The per-request plain-launch baseline: each request alone (copy in,
+    solve, copy out, synchronise), in arrival order, starting no earlier than
+    its arrival.  Returns a list of RequestHandle."""
+    device = torch.device(device)
+    stream = torch.cuda.Stream(device)
+    handles = []
+    t0 = time.perf_counter()
+    for i, req in enumerate(requests):
+        if arrivals is not None:
+            target = t0 + arrivals[i]
+            while time.perf_counter() < target:
+                time.sleep(max(0.0, min(1e-3, target - time.perf_counter())))
+            req.arrival = target
+        elif not req.arrival:
+            req.arrival = time.perf_counter()
+        h = RequestHandle(req)
+        h.t_admit = time.perf_counter()
+        try:
+            host, _ = _solve_on_stream(req, precision, device, stream)
+            stream.synchronize()
+            h._finish(result=host)
+        except Exception as e:
+            h._finish(error=e)
+        handles.append(h)
+    return handles

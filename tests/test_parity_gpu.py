@@ -295,6 +295,35 @@ def test_robust_normalization_config3_shape(sig, oracle):
     np.testing.assert_allclose(lam, oracle.normalization(host(X), 1, nrm), rtol=LAM_RTOL, atol=1e-9)
 
 
+@pytest.mark.parametrize("L,d,order", [(70, 3, 3), (130, 2, 1), (12, 40, 2)])
+def test_robust_normalization_increment_sources(sig, oracle, L, d, order, monkeypatch):
+    """The shared-memory increment tile (paths of up to 77 cells) and the
+    precomputed-difference source (longer paths, or SIGK_NO_NORM_TILE=1), with
+    one and several bands of rows, against the oracle and against each other."""
+    rng = np.random.default_rng(L + d)
+    scales = np.exp(rng.uniform(np.log(0.5), np.log(4.0), 10))
+    x = oracle.brownian(10, L, d, 61 + L, scale=scales)
+    X = cuda(x, torch.float64)
+    rk = sig.RobustSigPDE(sig.kernels.LinearKernel(), order)
+    lam = host(rk.normalization(X))
+    want = oracle.normalization(x, order)
+    np.testing.assert_allclose(lam, want, rtol=LAM_RTOL, atol=1e-9)
+    assert (want > 0).sum() >= 3
+    monkeypatch.setenv("SIGK_NO_NORM_TILE", "1")
+    lam_delta = host(rk.normalization(X))
+    np.testing.assert_allclose(lam_delta, lam, rtol=1e-12, atol=1e-14)
+
+
+def test_robust_normalization_alternating_shared_memory_sizes(sig, oracle):
+    """One kernel instance launched with large, then smaller, then large
+    shared-memory tiles (the per-function opt-in must cover all of them)."""
+    rk = sig.RobustSigPDE(sig.kernels.LinearKernel(), 2)
+    for L in (52, 30, 52, 40, 60):
+        x = oracle.brownian(4, L, 32, 70 + L, scale=np.array([0.6, 1.5, 2.5, 3.5]))
+        lam = host(rk.normalization(cuda(x, torch.float64)))
+        np.testing.assert_allclose(lam, oracle.normalization(x, 2), rtol=LAM_RTOL, atol=1e-9)
+
+
 def test_robust_gram_and_pairwise(sig, oracle):
     rng = np.random.default_rng(4)
     scales = np.exp(rng.uniform(np.log(0.5), np.log(4.0), 6))

@@ -1,0 +1,122 @@
+"""The request server (sigpde_b200.serving): continuous batching with
+HBM-footprint admission.
+
+* each request's result in a concurrent mix equals the same request solved
+  alone through the API (the solves are deterministic and only read their own
+  buffers, so the tolerance is 0: bitwise equal);
+* requests overlap on the device (more than one in flight at once);
+* the in-flight footprint never exceeds the HBM budget; a request larger than
+  the whole budget fails alone with MemoryError;
+* a malformed request fails alone, the others complete;
+* float64 spot checks against the oracle (float32 outputs: 2.5e-7 relative).
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests(oracle, n, seed, dtype=torch.float32):
+    from sigpde_b200.serving import GramRequest
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(n):
+        N = int(rng.integers(3, 40))
+        L = int(rng.integers(8, 80))
+        d = int(rng.choice([2, 8, 32]))
+        o = int(rng.integers(0, 3))
+        kind = "robust" if rng.random() < 0.3 else "gram"
+        sc = np.exp(rng.uniform(np.log(0.5), np.log(4.0), N)) if kind == "robust" else None
+        x = torch.tensor(oracle.brownian(N, L, d, int(rng.integers(1 << 30)), scale=sc), dtype=dtype).pin_memory()
+        y = None
+        if kind == "gram" and rng.random() < 0.5:
+            y = torch.tensor(oracle.brownian(int(rng.integers(2, 30)), L + int(rng.integers(0, 20)), d,
+                                             int(rng.integers(1 << 30))), dtype=dtype).pin_memory()
+        reqs.append(GramRequest(x=x, y=y, order=o, kind=kind))
+    return reqs
+
+
+def _alone(req):
+    import sigpde_b200.torch as sig
+    x = req.x.cuda()
+    y = None if req.y is None else req.y.cuda()
+    if req.kind == "robust":
+        return sig.RobustSigPDE(sig.kernels.LinearKernel(), req.order).gram(x, y).cpu()
+    return sig.SigPDE(sig.kernels.LinearKernel(), req.order).gram(x, y).cpu()
+
+
+def test_results_in_the_mix_equal_results_alone(oracle):
+    from sigpde_b200.serving import GramServer
+    reqs = _requests(oracle, 24, 1)
+    with GramServer(max_inflight=6) as srv:
+        handles = [srv.submit(r) for r in reqs]
+        results = [h.wait(timeout=120) for h in handles]
+        peak = srv.peak_inflight
+    assert peak > 1, "requests should overlap on the device"
+    for r, got in zip(reqs, results):
+        np.testing.assert_array_equal(got.numpy(), _alone(r).numpy())
+    # float64 spot checks on a few entries
+    rng = np.random.default_rng(0)
+    for r, got in list(zip(reqs, results))[:6]:
+        x = r.x.double().numpy()
+        y = None if r.y is None else r.y.double().numpy()
+        i = int(rng.integers(got.shape[0]))
+        j = int(rng.integers(got.shape[1]))
+        if r.kind == "robust":
+            want = oracle.robust_gram(x, y, r.order)[i, j]
+        else:
+            yy = x if y is None else y
+            want = oracle.gram(x, yy, r.order, pairs=[i * yy.shape[0] + j])[0]
+        assert abs(float(got[i, j]) - want) <= 2.5e-7 * abs(want) + 1e-300
+
+
+def test_admission_respects_the_hbm_budget(oracle):
+    from sigpde_b200.serving import GramServer, footprint_bytes
+    reqs = _requests(oracle, 12, 2)
+    sizes = [footprint_bytes(r) for r in reqs]
+    budget = 2 * max(sizes)
+    big = _requests(oracle, 1, 3)[0]
+    big_size = footprint_bytes(big)
+    small_budget = max(budget, 1)
+    with GramServer(max_inflight=8, hbm_budget_bytes=small_budget) as srv:
+        handles = [srv.submit(r) for r in reqs]
+        for h in handles:
+            h.wait(timeout=120)
+        assert srv.peak_bytes <= small_budget
+    if big_size > small_budget:
+        with GramServer(max_inflight=2, hbm_budget_bytes=small_budget) as srv:
+            h = srv.submit(big)
+            with pytest.raises(MemoryError):
+                h.wait(timeout=60)
+
+
+def test_a_bad_request_fails_alone(oracle):
+    from sigpde_b200.serving import GramRequest, GramServer
+    reqs = _requests(oracle, 6, 4)
+    bad = GramRequest(x=torch.zeros((4, 1, 3)), order=1)  # one point per path: rejected by the API
+    with GramServer(max_inflight=4) as srv:
+        handles = [srv.submit(r) for r in reqs[:3]] + [srv.submit(bad)] + [srv.submit(r) for r in reqs[3:]]
+        with pytest.raises(ValueError):
+            handles[3].wait(timeout=60)
+        for h, r in zip(handles[:3] + handles[4:], reqs):
+            np.testing.assert_array_equal(h.wait(timeout=120).numpy(), _alone(r).numpy())
+
+
+def test_chunked_large_requests_match(oracle):
+    """Row-block chunking of large Grams (forced with a tiny chunk size) gives the same result."""
+    from sigpde_b200.serving import GramServer
+    reqs = _requests(oracle, 8, 6)
+    with GramServer(max_inflight=3, chunk_cells=10 ** 5) as srv:
+        handles = [srv.submit(r) for r in reqs]
+        for h, r in zip(handles, reqs):
+            np.testing.assert_array_equal(h.wait(timeout=120).numpy(), _alone(r).numpy())
+
+
+def test_sequential_baseline_gives_the_same_results(oracle):
+    from sigpde_b200.serving import serve_sequential
+    reqs = _requests(oracle, 5, 5)
+    handles = serve_sequential(reqs)
+    for h, r in zip(handles, reqs):
+        np.testing.assert_array_equal(h.wait().numpy(), _alone(r).numpy())
