@@ -63,7 +63,7 @@ def parse():
                     help="ours | reference: the float64 oracle port on the host cores | reference-gpu: the "
                          "unmodified stojl/SigPDE Numba GPU path installed under baseline/_ref")
     ap.add_argument("--workload", default="gram256", choices=sorted(WORKLOADS))
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "tc32", "tc64"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target length of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--burst", action="store_true", help="serving traces: every request arrives at t=0 "
@@ -174,6 +174,14 @@ def device_peak_tflops(torch, dtype, n=4096, reps=5):
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
+LAUNCHES = {"last": None}  # libsigk kernels enqueued by the last timed region
+
+
+def _launch_count():
+    mod = sys.modules.get("sigpde_b200._lib")
+    return mod.launch_count() if mod is not None else None
+
+
 def timed_steps(torch, step, K, W, flush_buf, barrier):
     for _ in range(W):
         step()
@@ -182,6 +190,7 @@ def timed_steps(torch, step, K, W, flush_buf, barrier):
     torch.cuda.synchronize()
     stream = torch.cuda.current_stream()
     evs = []
+    c0 = _launch_count()
     for _ in range(K):
         flush_buf.zero_()  # L2 flush between timed steps (outside the events)
         s = torch.cuda.Event(enable_timing=True)
@@ -190,6 +199,8 @@ def timed_steps(torch, step, K, W, flush_buf, barrier):
         step()
         e.record(stream)
         evs.append((s, e))
+    c1 = _launch_count()
+    LAUNCHES["last"] = None if c0 is None else c1 - c0
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
@@ -317,6 +328,7 @@ def run_ours(args, w):
     clocks = ClockSampler(local)
     clocks.start()
     times = timed_steps(torch, lambda: k.gram(X, Y), args.steps, args.warmup, flush, barrier)
+    launches = LAUNCHES["last"]
     clk = clocks.stop()
     total_ms = sum(times)
     if world > 1:
@@ -346,7 +358,7 @@ def run_ours(args, w):
     line = None
     if rank == 0:
         ms = statistics.mean(times)
-        fp64 = args.precision == "fp64"
+        fp64 = args.precision in ("fp64", "tc64")  # float64 cells
         peak = device_peak_tflops(torch, torch.float64 if fp64 else torch.float32)
         achieved = flops / (ms * 1e-3) / 1e12
         traffic = read_traffic(f"gram256_{args.precision}")
@@ -366,6 +378,19 @@ def run_ours(args, w):
             acc = {"max_rel_err": float(np.max(np.abs(got - want) / np.abs(want))),
                    "max_cs_err": float(np.max(np.abs(got - want) / np.sqrt(kxx * kyy))),
                    "sample": "64 random entries vs the float64 oracle"}
+            # the other precision modes on the same inputs and sample: time and error
+            modes = {}
+            for prec in ("fp64", "fp32", "tc32", "tc64"):
+                if prec == args.precision:
+                    continue
+                km = sig.SigPDE(sig.kernels.LinearKernel(), w["order"], precision=prec)
+                tm = timed_steps(torch, lambda: km.gram(X, Y), args.steps, args.warmup, flush, lambda: None)
+                gm = km.gram(X, Y).double().cpu().numpy().reshape(-1)[flat]
+                modes[prec] = {"ms_per_step": statistics.mean(tm),
+                               "entries_per_s": entries / (statistics.mean(tm) * 1e-3),
+                               "max_rel_err": float(np.max(np.abs(gm - want) / np.abs(want))),
+                               "max_cs_err": float(np.max(np.abs(gm - want) / np.sqrt(kxx * kyy)))}
+            acc["other_precision_modes"] = modes
             rate, cores, sample = cpu_oracle_rate(w, args.cpu_seconds)
             cpu = {"value": rate, "unit": "entries/s", "cores": cores, "kind": "port",
                    "sample": f"{sample}; float64 C restatement of the reference solver (OpenMP)"}
@@ -398,7 +423,7 @@ def run_ours(args, w):
             "e2e": {"value": e2e_value, "unit": "entries/s", "h2d_bytes_per_step": X.numel() * X.element_size()
                     + Y.numel() * Y.element_size(), "d2h_bytes_per_step": Rh.numel() * Rh.element_size(),
                     "ms_per_step": statistics.mean(e2e_times)},
-            "gpu_launches": args.steps,
+            "gpu_launches": launches,
             "clocks": clk,
             "lib": _lib.version(),
         }
@@ -550,6 +575,7 @@ def run_ours_ragged(args, w):
     clocks = ClockSampler(0)
     clocks.start()
     times = timed_steps(torch, solver.solve, args.steps, args.warmup, flush, lambda: None)
+    launches = solver.graph_kernels * args.steps  # graph replays: the captured kernels, once per step
     clk = clocks.stop()
     ms = statistics.mean(times)
     out = solver.out.double().cpu().numpy()
@@ -580,7 +606,7 @@ def run_ours_ragged(args, w):
         "metric": "pde_cell_updates_per_s", "value": cells / (ms * 1e-3), "unit": "cells/s", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "p50_ms": percentile(times, 0.5),
         "p99_ms": percentile(times, 0.99), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if args.precision == "fp64" else "f32",
+        "dtype": "f64" if args.precision in ("fp64", "tc64") else "f32",
         "data": "synthetic Brownian paths (seeded PCG64), float32",
         "config": {"workload": "pairwise 4096 uneven pairs, L~U[16,512] per path, d=32, order~U{0..3} per pair",
                    "global_batch": w["npairs"], "seq_len": "16-512", "parallelism": "single GPU",
@@ -590,7 +616,7 @@ def run_ours_ragged(args, w):
         "e2e": {"value": cells / (statistics.mean(e2e_times) * 1e-3), "unit": "cells/s",
                 "h2d_bytes_per_step": xh.numel() * xh.element_size() + yh.numel() * yh.element_size(),
                 "d2h_bytes_per_step": oh.numel() * oh.element_size(), "ms_per_step": statistics.mean(e2e_times)},
-        "gpu_launches": args.steps, "clocks": clk, "lib": _lib.version(),
+        "gpu_launches": launches, "clocks": clk, "lib": _lib.version(),
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu
@@ -666,6 +692,7 @@ def run_ours_robust(args, w):
     clocks = ClockSampler(0)
     clocks.start()
     times = timed_steps(torch, lambda: rk.gram(X), args.steps, args.warmup, flush, lambda: None)
+    launches = LAUNCHES["last"]
     clk = clocks.stop()
     # the two phases separately: lambda root-find, then the scaled symmetric Gram
     lam = rk.normalization(X)
@@ -712,7 +739,7 @@ def run_ours_robust(args, w):
         "metric": "gram_entries_per_s", "value": entries / (ms * 1e-3), "unit": "entries/s", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "p50_ms": percentile(times, 0.5),
         "p99_ms": percentile(times, 0.99), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if args.precision == "fp64" else "f32",
+        "dtype": "f64" if args.precision in ("fp64", "tc64") else "f32",
         "data": "synthetic Brownian paths (seeded PCG64), per-path scale log-uniform [0.5, 4], float32",
         "config": {"workload": "RobustSigPDE.gram(x) N=512, L=64, d=16, dyadic_order=1, default normaliser",
                    "global_batch": entries, "seq_len": w["L"], "parallelism": "single GPU",
@@ -723,7 +750,7 @@ def run_ours_robust(args, w):
         "e2e": {"value": entries / (statistics.mean(e2e_times) * 1e-3), "unit": "entries/s",
                 "h2d_bytes_per_step": Xh.numel() * Xh.element_size(), "d2h_bytes_per_step": Rh.numel() * Rh.element_size(),
                 "ms_per_step": statistics.mean(e2e_times)},
-        "gpu_launches": 3 * args.steps, "clocks": clk, "lib": _lib.version(),
+        "gpu_launches": launches, "clocks": clk, "lib": _lib.version(),
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu
@@ -879,7 +906,7 @@ def run_serve(args, w):
     line = {
         "metric": "served_requests_per_s", "value": served["requests_per_s"], "unit": "requests/s", "n_gpus": 1,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if args.precision == "fp64" else "f32",
+        "dtype": "f64" if args.precision in ("fp64", "tc64") else "f32",
         "data": "synthetic Brownian paths (seeded PCG64), float32, pinned host memory",
         "config": {"workload": f"serving trace: {len(reqs)} Gram requests, Poisson {w['rate']}/s, "
                                f"N~logU[{w['nmin']},{w['nmax']}], L~logU[{w['lmin']},{w['lmax']}], d in {{2,8,32}}, "

@@ -26,8 +26,21 @@
  *   SIGK_PREC_FP64  increments <dx_i,dy_j> and PDE cells in float64 (default;
  *                   no worse than the reference's GPU path, which does float64
  *                   arithmetic with float32 storage, and far better).
- *   SIGK_PREC_FP32  increments and cells in float32 (fastest; its error grows
- *                   with |K| along the grid and is reported by the tests).
+ *   SIGK_PREC_FP32  increments and cells in float32 (its error grows with |K|
+ *                   along the grid and is reported by the tests).
+ *   SIGK_PREC_TC32  linear-kernel increments of all pairs from one tensor-core
+ *   SIGK_PREC_TC64  GEMM in split TF32 (hi*hi + hi*lo + lo*hi, float32
+ *                   accumulate; ~1e-6 relative per increment), stored as a
+ *                   float32 matrix in the workspace and read by the wavefront;
+ *                   cells in float32 (TC32) or float64 (TC64).  Applies to
+ *                   sigk_pairwise / sigk_gram / sigk_gram_sym when each pair
+ *                   fits one band of rows ((len - 1) * 2^order <= 512) and
+ *                   dim <= 32; other shapes, and the *_inc, ragged and
+ *                   normalisation entry points, form increments on the CUDA
+ *                   cores with the same cell precision.  The workspace holds
+ *                   the increment matrix: up to 6 GiB per call (the x paths
+ *                   are processed in chunks beyond that; SIGK_TC_CHUNK_MB
+ *                   sets the chunk size).
  */
 #ifndef SIGK_H_
 #define SIGK_H_
@@ -58,7 +71,7 @@ typedef enum {
 
 typedef enum { SIGK_F32 = 0, SIGK_F64 = 1 } sigk_dtype;
 
-typedef enum { SIGK_PREC_FP64 = 0, SIGK_PREC_FP32 = 1 } sigk_precision;
+typedef enum { SIGK_PREC_FP64 = 0, SIGK_PREC_FP32 = 1, SIGK_PREC_TC32 = 2, SIGK_PREC_TC64 = 3 } sigk_precision;
 
 typedef enum {
     SIGK_OP_PAIRWISE = 0,     /* out[b]    = k(x_b, y_b)                                */
@@ -72,6 +85,10 @@ SIGK_API const char *sigk_version(void);
 
 /* Description of the last error on this host thread ("" if none). */
 SIGK_API const char *sigk_last_error_string(void);
+
+/* Number of kernels this library has enqueued since it was loaded (all
+ * threads, all devices); a caller can difference it around a region. */
+SIGK_API uint64_t sigk_launch_count(void);
 
 /*
  * Bytes of caller-provided scratch an entry point needs for the given shape.

@@ -26,6 +26,8 @@ SIGK_F32 = 0
 SIGK_F64 = 1
 SIGK_PREC_FP64 = 0
 SIGK_PREC_FP32 = 1
+SIGK_PREC_TC32 = 2
+SIGK_PREC_TC64 = 3
 SIGK_OP_PAIRWISE = 0
 SIGK_OP_GRAM = 1
 SIGK_OP_GRAM_SYM = 2
@@ -41,6 +43,7 @@ _sz = ctypes.c_size_t
 SIGNATURES = {
     "sigk_version": (ctypes.c_char_p, []),
     "sigk_last_error_string": (ctypes.c_char_p, []),
+    "sigk_launch_count": (ctypes.c_uint64, []),
     "sigk_workspace_size": (_sz, [_int, _i64, _i64, _i64, _i64, _i64, _int, _int, _int]),
     "sigk_pairwise": (_int, [_vp, _vp, _i64, _i64, _i64, _i64, _int, _int, _dbl, _vp, _vp, _vp, _int, _vp, _sz,
                              _vp]),
@@ -107,3 +110,8 @@ def call(name: str, *args) -> None:
 
 def version() -> str:
     return lib().sigk_version().decode()
+
+
+def launch_count() -> int:
+    """Kernels enqueued by libsigk.so since it was loaded (all threads)."""
+    return int(lib().sigk_launch_count())

@@ -11,6 +11,12 @@ struct PairParams;
 struct NormParams;
 struct StreamParams;
 struct RaggedParams;
+struct StreamIncParams;
+struct TcImageParams;
+struct TcGemmParams;
+}
+struct CUtensorMap_st; // cuda.h
+namespace sigk {
 
 using PairFn = void (*)(PairParams);
 using NormFn = void (*)(NormParams);
@@ -18,6 +24,9 @@ using StreamFn = void (*)(StreamParams);
 using RaggedFn = void (*)(RaggedParams);
 using RaggedDeltaFn = void (*)(const void *, const int64_t *, const int64_t *, const int *, double, const void *,
                                 int64_t, int64_t, void *);
+using StreamIncFn = void (*)(StreamIncParams);
+using TcImageFn = void (*)(TcImageParams);
+using TcGemmFn = void (*)(TcGemmParams, CUtensorMap_st);
 using DeltaFn = void (*)(const void *, int64_t, int64_t, int64_t, int64_t, double, const void *, void *);
 
 // f64cells: float64 cells (SIGK_PREC_FP64) vs float32; in64: float64 inputs;
@@ -35,5 +44,11 @@ StreamFn get_stream_smem_kernel(bool f64cells, int R, int O);
 DeltaFn get_delta_kernel(bool f64cells, bool in64);
 RaggedFn get_ragged_kernel(bool f64cells, bool in64);
 RaggedDeltaFn get_ragged_delta_kernel(bool f64cells, bool in64);
+// Tensor-core increments (tc.cuh): operand images, the TF32x3 GEMM (N tile
+// kTcBN) and the streaming wavefront that reads its output.
+constexpr int kTcBN = 256;
+TcImageFn get_tc_image_kernel(bool in64);
+TcGemmFn get_tc_gemm_kernel();
+StreamIncFn get_stream_inc_kernel(bool f64cells, int R, int O);
 
 } // namespace sigk

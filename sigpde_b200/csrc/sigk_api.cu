@@ -4,6 +4,7 @@
 // shape (rows per lane R, dyadic order O, cell precision T, input dtype TIN),
 // sizes a persistent grid to the device's resident capacity and enqueues the
 // launch on the caller's stream.  Nothing here allocates device memory.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -11,6 +12,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <unordered_map>
@@ -19,6 +21,7 @@
 #include "dispatch.h"
 #include "ragged.cuh"
 #include "stream.cuh"
+#include "tc.cuh"
 
 namespace sigk {
 namespace {
@@ -75,6 +78,10 @@ int rows_per_coarse_lane(int R, int order)
 constexpr size_t kMaxStreamStageBytesPerWarp = 32 * 1024;
 
 size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+// Kernels enqueued by this library since load (sigk_launch_count).
+std::atomic<uint64_t> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 bool env_flag(const char *name)
 {
@@ -157,7 +164,7 @@ Plan make_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, int64_t
 PairFn pick_pair(int precision, int dtype, bool from_inc, int R, int O)
 {
     const bool in64 = (dtype == SIGK_F64);
-    return precision == SIGK_PREC_FP64 ? get_pair_kernel_f64(in64, from_inc, R, O)
+    return (precision == SIGK_PREC_FP64 || precision == SIGK_PREC_TC64) ? get_pair_kernel_f64(in64, from_inc, R, O)
                                        : get_pair_kernel_f32(in64, from_inc, R, O);
 }
 
@@ -227,6 +234,7 @@ int launch(void (*fn)(P), P params, int64_t nitems, size_t smem, cudaStream_t st
     const int64_t blocks = want < cap ? want : cap;
     if (blocks <= 0) return SIGK_OK;
     fn<<<(unsigned)blocks, kWarpsPerBlock * 32, smem, stream>>>(params);
+    count_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
     return SIGK_OK;
@@ -246,8 +254,9 @@ bool is_device_ptr(const void *p)
 int check_common(int dtype, int precision, int order)
 {
     if (dtype != SIGK_F32 && dtype != SIGK_F64) return fail(SIGK_EINVAL, "dtype must be SIGK_F32 or SIGK_F64");
-    if (precision != SIGK_PREC_FP64 && precision != SIGK_PREC_FP32)
-        return fail(SIGK_EINVAL, "precision must be SIGK_PREC_FP64 or SIGK_PREC_FP32");
+    if (precision != SIGK_PREC_FP64 && precision != SIGK_PREC_FP32 && precision != SIGK_PREC_TC32 &&
+        precision != SIGK_PREC_TC64)
+        return fail(SIGK_EINVAL, "precision must be SIGK_PREC_FP64, _FP32, _TC32 or _TC64");
     if (order < 0 || order > 12) return fail(SIGK_EINVAL, "dyadic order %d outside [0, 12]", order);
     return SIGK_OK;
 }
@@ -259,7 +268,15 @@ int check_dev(const void *p, const char *name, bool nullable)
     return SIGK_OK;
 }
 
-size_t tsize_of(int precision) { return precision == SIGK_PREC_FP64 ? 8 : 4; }
+// Cell precision of a mode: the tensor-core modes differ from FP64 / FP32 only
+// in how the increments of linear-kernel pairs are formed.
+int cell_prec(int precision)
+{
+    return (precision == SIGK_PREC_FP64 || precision == SIGK_PREC_TC64) ? SIGK_PREC_FP64 : SIGK_PREC_FP32;
+}
+bool is_tc(int precision) { return precision == SIGK_PREC_TC32 || precision == SIGK_PREC_TC64; }
+
+size_t tsize_of(int precision) { return cell_prec(precision) == SIGK_PREC_FP64 ? 8 : 4; }
 
 int check_ws(const Plan &pl, void *ws, size_t ws_bytes)
 {
@@ -267,6 +284,271 @@ int check_ws(const Plan &pl, void *ws, size_t ws_bytes)
     if (!ws || ws_bytes < pl.ws_bytes)
         return fail(SIGK_ENOMEM, "workspace of %zu bytes needed (got %zu)", pl.ws_bytes, ws ? ws_bytes : 0);
     if (((uintptr_t)ws & 15) != 0) return fail(SIGK_EINVAL, "workspace must be 16-byte aligned");
+    return SIGK_OK;
+}
+
+
+// ------------------------------------------------------------------ tensor-core increments
+// Plan of a linear-kernel request in a TC mode: the increments of every pair
+// come from one TF32x3 tensor-core GEMM (tc.cuh) into an fp32 matrix in the
+// workspace, which a streaming wavefront then reads.  Eligible: one band of
+// rows per pair (the streaming kernel's shapes) and dim <= 32 (the operand
+// tiles of both stages fit shared memory).  The x paths are cut into chunks
+// so that the matrix stays under kTcChunkBytes (SIGK_TC_CHUNK_MB overrides).
+constexpr size_t kTcChunkBytes = size_t(6) << 30;
+
+struct TcPlan {
+    bool ok;
+    int R, O;
+    int kp;
+    int64_t rows_x, rows_y;   // matrix rows per x path (ncx rounded up to 4) and per y path
+    int64_t chunk, nchunks;   // x paths per chunk
+    int64_t a_tiles, b_tiles; // operand tiles per image
+    size_t a_bytes, b_bytes;  // bytes of one (hi or lo) image
+    size_t err_off, a_off, b_off, ct_off, ws_bytes;
+};
+
+size_t tc_chunk_cap()
+{
+    const char *v = getenv("SIGK_TC_CHUNK_MB");
+    if (v && v[0]) {
+        long long mb = atoll(v);
+        if (mb > 0) return (size_t)mb << 20;
+    }
+    return kTcChunkBytes;
+}
+
+TcPlan make_tc_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, int64_t d, int order)
+{
+    TcPlan t{};
+    const int64_t n = ncx << order, m = ncy << order;
+    const int C = order >= 4 ? 8 : (1 << order);
+    const int Rs = pick_rows(n);
+    if (d > 32 || n > 32 * Rs || m / C < 32 || env_flag("SIGK_NO_TC")) return t;
+    t.ok = true;
+    t.R = Rs;
+    t.O = order >= 4 ? 4 : order;
+    t.kp = (int)((d + 7) / 8 * 8);
+    t.rows_x = (ncx + 3) / 4 * 4;
+    t.rows_y = ncy;
+    const int64_t width = op == kOpPairwise ? ncy : (op == kOpGram ? ny : nx) * ncy; // matrix rows per x path
+    const size_t per_x = (size_t)t.rows_x * (size_t)width * sizeof(float);
+    int64_t chunk = (int64_t)(tc_chunk_cap() / per_x);
+    if (chunk < 1) chunk = 1;
+    if (chunk > nx) chunk = nx;
+    t.chunk = chunk;
+    t.nchunks = (nx + chunk - 1) / chunk;
+    t.a_tiles = (chunk * t.rows_x + kTcM - 1) / kTcM;
+    const int64_t b_rows = op == kOpPairwise ? chunk * ncy : (op == kOpGram ? ny : nx) * ncy;
+    t.b_tiles = (b_rows + kTcBN - 1) / kTcBN;
+    t.a_bytes = align256((size_t)t.a_tiles * kTcM * t.kp * sizeof(float));
+    t.b_bytes = align256((size_t)t.b_tiles * kTcBN * t.kp * sizeof(float));
+    t.err_off = 0;
+    t.a_off = 256;
+    t.b_off = t.a_off + 2 * t.a_bytes;
+    t.ct_off = t.b_off + 2 * t.b_bytes;
+    t.ws_bytes = t.ct_off + align256((size_t)chunk * per_x);
+    return t;
+}
+
+int tc_image(bool in64, const void *x, int64_t npaths, int64_t len, int64_t d, int64_t rows_per_path, int64_t tile_rows,
+             int64_t ntiles, int kp, double f, const void *s, float *hi, float *lo, cudaStream_t stream)
+{
+    TcImageParams ip{};
+    ip.x = x;
+    ip.npaths = npaths;
+    ip.len = len;
+    ip.d = d;
+    ip.rows_per_path = rows_per_path;
+    ip.tile_rows = tile_rows;
+    ip.ntiles = ntiles;
+    ip.kp = kp;
+    ip.f = f;
+    ip.s = s;
+    ip.hi = hi;
+    ip.lo = lo;
+    const int64_t total = ntiles * tile_rows * kp;
+    int64_t blocks = (total + 255) / 256;
+    if (blocks > (int64_t)sm_count() * 8) blocks = (int64_t)sm_count() * 8;
+    get_tc_image_kernel(in64)<<<(unsigned)blocks, 256, 0, stream>>>(ip);
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? SIGK_OK : cuda_fail(e, "operand image kernel launch");
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against libcuda).
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+int encode_out_map(CUtensorMap *map, float *out, int64_t ld, int64_t n_rows)
+{
+    static std::mutex mu;
+    static EncodeTiledFn encode = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (!encode) {
+            void *fn = nullptr;
+            cudaDriverEntryPointQueryResult q{};
+            cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+            if (e != cudaSuccess || !fn || q != cudaDriverEntryPointSuccess)
+                return fail(SIGK_ELAUNCH, "cuTensorMapEncodeTiled is not available from the driver");
+            encode = reinterpret_cast<EncodeTiledFn>(fn);
+        }
+    }
+    // the increment matrix: n_rows rows of ld floats; boxes of 128 floats x 32 rows
+    const cuuint64_t dims[2] = {(cuuint64_t)ld, (cuuint64_t)n_rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(float)};
+    const cuuint32_t box[2] = {(cuuint32_t)kTcM, (cuuint32_t)kTcStageCols};
+    const cuuint32_t estr[2] = {1, 1};
+    CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, out, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(SIGK_ELAUNCH, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return SIGK_OK;
+}
+
+int tc_gemm(const TcGemmParams &gp, cudaStream_t stream)
+{
+    TcGemmFn fn = get_tc_gemm_kernel();
+    const size_t smem = tc_gemm_smem(kTcBN, gp.kp);
+    static std::mutex mu;
+    static bool attr_set[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (dev < 0 || dev >= 64) return fail(SIGK_EINVAL, "device index %d out of range", dev);
+        if (!attr_set[dev]) {
+            int optin = 0;
+            e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
+            if ((size_t)optin < smem) return fail(SIGK_ELAUNCH, "GEMM needs %zu bytes of shared memory", smem);
+            e = cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+            attr_set[dev] = true;
+        }
+    }
+    CUtensorMap map;
+    memset(&map, 0, sizeof(map));
+    if (gp.mode != kTcDiag) {
+        if ((gp.ld & 3) != 0 || ((uintptr_t)gp.out & 15) != 0)
+            return fail(SIGK_EINVAL, "increment matrix rows must be 16-byte aligned");
+        int st = encode_out_map(&map, gp.out, gp.ld, gp.n_rows);
+        if (st) return st;
+    }
+    int64_t grid = gp.mtiles * gp.ntiles;
+    if (grid > sm_count()) grid = sm_count();
+    fn<<<(unsigned)grid, kTcThreads, smem, stream>>>(gp, map);
+    count_launch();
+    e = cudaGetLastError();
+    return e == cudaSuccess ? SIGK_OK : cuda_fail(e, "tensor-core GEMM launch");
+}
+
+int run_pairs_tc(const TcPlan &t, int op, const void *x, const void *y, int64_t nx, int64_t ny, int64_t lx, int64_t ly,
+                 int64_t d, int dtype, int order, double static_scale, const void *sx, const void *sy, void *out,
+                 int64_t out_ld, int precision, void *ws, cudaStream_t stream)
+{
+    int st;
+    const bool in64 = dtype == SIGK_F64;
+    const size_t es = in64 ? 8 : 4;
+    const int64_t ncx = lx - 1, ncy = ly - 1;
+    unsigned char *wsb = reinterpret_cast<unsigned char *>(ws);
+    unsigned *err = reinterpret_cast<unsigned *>(wsb + t.err_off);
+    float *a_hi = reinterpret_cast<float *>(wsb + t.a_off), *a_lo = reinterpret_cast<float *>(wsb + t.a_off + t.a_bytes);
+    float *b_hi = reinterpret_cast<float *>(wsb + t.b_off), *b_lo = reinterpret_cast<float *>(wsb + t.b_off + t.b_bytes);
+    float *ct = reinterpret_cast<float *>(wsb + t.ct_off);
+    cudaError_t e = cudaMemsetAsync(err, 0, sizeof(unsigned), stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+    const double fs = static_scale * std::ldexp(1.0, -2 * order); // x side: static scale * 4^-order * scale_x
+    const char *xb = reinterpret_cast<const char *>(x);
+    const char *yb = reinterpret_cast<const char *>(y);
+    const char *sxb = reinterpret_cast<const char *>(sx);
+    const char *syb = reinterpret_cast<const char *>(sy);
+    if (op != kOpPairwise) { // the y side image is shared by all chunks
+        const bool sym = op == kOpGramSym;
+        if ((st = tc_image(in64, sym ? x : y, sym ? nx : ny, ly, d, ncy, kTcBN, t.b_tiles, t.kp, 1.0, sym ? sx : sy,
+                           b_hi, b_lo, stream)))
+            return st;
+    }
+    const bool f64 = cell_prec(precision) == SIGK_PREC_FP64;
+    StreamIncFn fn = get_stream_inc_kernel(f64, t.R, t.O);
+    int nb = 0;
+    if ((st = blocks_per_sm((const void *)fn, 0, &nb))) return st;
+    const int64_t warps = (int64_t)sm_count() * nb * kWarpsPerBlock;
+
+    for (int64_t c = 0; c < t.nchunks; ++c) {
+        const int64_t i0 = c * t.chunk, i1 = (i0 + t.chunk < nx) ? i0 + t.chunk : nx, nxc = i1 - i0;
+        const int64_t a_tiles = (nxc * t.rows_x + kTcM - 1) / kTcM;
+        if ((st = tc_image(in64, xb + i0 * lx * d * es, nxc, lx, d, t.rows_x, kTcM, a_tiles, t.kp, fs,
+                           sx ? sxb + i0 * es : nullptr, a_hi, a_lo, stream)))
+            return st;
+        int64_t ny_rows;
+        if (op == kOpPairwise) {
+            ny_rows = nxc * ncy;
+            if ((st = tc_image(in64, yb + i0 * ly * d * es, nxc, ly, d, ncy, kTcBN, (ny_rows + kTcBN - 1) / kTcBN,
+                               t.kp, 1.0, sy ? syb + i0 * es : nullptr, b_hi, b_lo, stream)))
+                return st;
+        } else {
+            ny_rows = (op == kOpGram ? ny : i1) * ncy;
+        }
+        TcGemmParams gp{};
+        gp.a_hi = a_hi;
+        gp.a_lo = a_lo;
+        gp.b_hi = b_hi;
+        gp.b_lo = b_lo;
+        gp.mtiles = a_tiles;
+        gp.ntiles = (ny_rows + kTcBN - 1) / kTcBN;
+        gp.kp = t.kp;
+        gp.mode = op == kOpPairwise ? kTcDiag : (op == kOpGramSym ? kTcLower : kTcAll);
+        gp.m_rows = nxc * t.rows_x;
+        gp.n_rows = ny_rows;
+        gp.rows_x = t.rows_x;
+        gp.rows_y = ncy;
+        gp.npaths_x = nxc;
+        gp.npaths_y = op == kOpPairwise ? nxc : (op == kOpGram ? ny : i1);
+        gp.x0 = op == kOpGramSym ? i0 : 0;
+        gp.out = ct;
+        gp.ld = nxc * t.rows_x;
+        gp.err = err;
+        if ((st = tc_gemm(gp, stream))) return st;
+
+        StreamIncParams sp{};
+        sp.op = op;
+        sp.in64 = in64;
+        sp.inc = ct;
+        sp.ld = gp.ld;
+        sp.rows_x = t.rows_x;
+        sp.x0 = i0;
+        sp.nx = nx;
+        sp.ny = ny;
+        sp.ncx = ncx;
+        sp.ncy = ncy;
+        sp.order = order;
+        sp.out = out;
+        sp.out_ld = out_ld;
+        sp.err = err;
+        if (op == kOpPairwise) {
+            sp.item0 = i0;
+            sp.nitems = nxc;
+        } else if (op == kOpGram) {
+            sp.item0 = i0 * ny;
+            sp.nitems = nxc * ny;
+        } else {
+            sp.item0 = i0 * (i0 + 1) / 2;
+            sp.nitems = i1 * (i1 + 1) / 2 - sp.item0;
+        }
+        int64_t nw = warps < sp.nitems ? warps : sp.nitems;
+        sp.per_warp = (sp.nitems + nw - 1) / nw;
+        const int64_t used = (sp.nitems + sp.per_warp - 1) / sp.per_warp;
+        const int64_t blocks = (used + kWarpsPerBlock - 1) / kWarpsPerBlock;
+        fn<<<(unsigned)blocks, kWarpsPerBlock * 32, 0, stream>>>(sp);
+        count_launch();
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(e, "stream increment kernel launch");
+    }
     return SIGK_OK;
 }
 
@@ -284,6 +566,17 @@ int run_pairs(int op, const void *x, const void *y, int64_t nx, int64_t ny, int6
     if ((st = check_dev(x, "x", false)) || (st = check_dev(y, "y", false)) || (st = check_dev(out, "out", false)) ||
         (st = check_dev(sx, "scale_x", true)) || (st = check_dev(sy, "scale_y", true)))
         return st;
+    if (is_tc(precision)) {
+        TcPlan t = make_tc_plan(op, nx, ny, lx - 1, ly - 1, d, order);
+        if (t.ok) {
+            if (!ws || ws_bytes < t.ws_bytes)
+                return fail(SIGK_ENOMEM, "workspace of %zu bytes needed (got %zu)", t.ws_bytes, ws ? ws_bytes : 0);
+            if (((uintptr_t)ws & 255) != 0) return fail(SIGK_EINVAL, "workspace must be 256-byte aligned");
+            return run_pairs_tc(t, op, x, y, nx, ny, lx, ly, d, dtype, order, static_scale, sx, sy, out, out_ld,
+                                precision, ws, stream);
+        }
+        precision = cell_prec(precision); // shapes outside the TC plan: CUDA-core increments, same cells
+    }
     const size_t ts = tsize_of(precision);
     const int64_t nitems = op == kOpPairwise ? nx : (op == kOpGram ? nx * ny : nx * (nx + 1) / 2);
     Plan pl = make_plan(op, nx, ny, lx - 1, ly - 1, d, order, ts, false);
@@ -304,6 +597,7 @@ int run_pairs(int op, const void *x, const void *y, int64_t nx, int64_t ny, int6
             int64_t blocks = (total + 255) / 256;
             if (blocks > (int64_t)nsm * 8) blocks = (int64_t)nsm * 8;
             delta<<<(unsigned)blocks, 256, 0, stream>>>(src, npaths, len, d, dp, f, sc, dst);
+            count_launch();
             cudaError_t e = cudaGetLastError();
             return e == cudaSuccess ? SIGK_OK : cuda_fail(e, "delta kernel launch");
         };
@@ -350,6 +644,7 @@ int run_pairs(int op, const void *x, const void *y, int64_t nx, int64_t ny, int6
         const int64_t used = (nitems + sp.per_warp - 1) / sp.per_warp;
         const int64_t blocks = (used + kWarpsPerBlock - 1) / kWarpsPerBlock;
         fn<<<(unsigned)blocks, kWarpsPerBlock * 32, smem, stream>>>(sp);
+        count_launch();
         cudaError_t e = cudaGetLastError();
         return e == cudaSuccess ? SIGK_OK : cuda_fail(e, "stream kernel launch");
     }
@@ -425,6 +720,8 @@ const char *sigk_version(void) { return "sigk 0.1.0 sm_100a"; }
 
 const char *sigk_last_error_string(void) { return g_last_error.c_str(); }
 
+uint64_t sigk_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
 size_t sigk_workspace_size(int op, int64_t n_x, int64_t n_y, int64_t len_x, int64_t len_y, int64_t dim, int order,
                            int dtype, int precision)
 {
@@ -437,6 +734,10 @@ size_t sigk_workspace_size(int op, int64_t n_x, int64_t n_y, int64_t len_x, int6
     }
     if (op == SIGK_OP_PAIRWISE) n_y = n_x;
     if (op == SIGK_OP_NORMALIZE) return norm_plan(n_x, len_x - 1, dim > 0 ? dim : 1, order, dim == 0).ws_bytes;
+    if (is_tc(precision) && dim > 0) {
+        TcPlan t = make_tc_plan(op, n_x, n_y, len_x - 1, len_y - 1, dim, order);
+        if (t.ok) return t.ws_bytes;
+    }
     // dim == 0 selects the plan of the *_inc entry points (no dx staging)
     Plan pl = make_plan(op, n_x, n_y, len_x - 1, len_y - 1, dim > 0 ? dim : 1, order, tsize_of(precision), dim == 0);
     return pl.ws_bytes;
@@ -506,6 +807,7 @@ static int normalize_impl(const void *x, const void *inc, int64_t n, int64_t nc,
         int64_t blocks = (total + 255) / 256;
         if (blocks > (int64_t)sm_count() * 8) blocks = (int64_t)sm_count() * 8;
         delta<<<(unsigned)blocks, 256, 0, stream>>>(x, n, nc + 1, d, d, 1.0, nullptr, dx);
+        count_launch();
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_fail(e, "delta kernel launch");
     }
@@ -758,7 +1060,7 @@ extern "C" int sigk_pairwise_ragged(const void *x_pack, const int64_t *x_off, co
         (st = check_dev(scale_y, "scale_y", true)))
         return st;
     const size_t ts = tsize_of(precision);
-    const bool f64 = precision == SIGK_PREC_FP64, in64 = dtype == SIGK_F64;
+    const bool f64 = cell_prec(precision) == SIGK_PREC_FP64, in64 = dtype == SIGK_F64;
     RaggedPlan pl = ragged_plan(npairs, x_points, y_points, dim, nitems, bnd_elems, ts);
     if (!workspace || workspace_bytes < pl.ws_bytes)
         return fail(SIGK_ENOMEM, "workspace of %zu bytes needed (got %zu)", pl.ws_bytes, workspace ? workspace_bytes : 0);
@@ -773,7 +1075,9 @@ extern "C" int sigk_pairwise_ragged(const void *x_pack, const int64_t *x_off, co
     RaggedDeltaFn delta = get_ragged_delta_kernel(f64, in64);
     const dim3 dgrid(32, (unsigned)(npairs < 65535 ? npairs : 65535));
     delta<<<dgrid, 256, 0, stream>>>(x_pack, x_off, x_len, order, static_scale, scale_x, npairs, dim, wsb + pl.dx_off);
+    count_launch();
     delta<<<dgrid, 256, 0, stream>>>(y_pack, y_off, y_len, nullptr, 1.0, scale_y, npairs, dim, wsb + pl.dy_off);
+    count_launch();
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "ragged delta launch");
 
@@ -809,6 +1113,7 @@ extern "C" int sigk_pairwise_ragged(const void *x_pack, const int64_t *x_off, co
     const int64_t want = (nitems + kWarpsPerBlock - 1) / kWarpsPerBlock;
     if (blocks > want) blocks = want;
     fn<<<(unsigned)blocks, kWarpsPerBlock * 32, smem, stream>>>(p);
+    count_launch();
     e = cudaGetLastError();
     return e == cudaSuccess ? SIGK_OK : cuda_fail(e, "ragged kernel launch");
 }

@@ -1,0 +1,598 @@
+// Tensor-core increments: the coarse increment matrix <dx_ci, dy_cj> of every
+// pair, computed as one dense contraction over the path dimension on the
+// 5th-generation tensor cores, then consumed by a streaming wavefront.
+//
+// The reference builds the increments with a static-kernel Gram and a 4-term
+// second difference (sigpde/torch/kernel.py:13-21, static_kernels.py:3-11);
+// for the linear kernel that is C = A * B^T with A the scaled differences of
+// the x paths (one row per coarse cell) and B those of the y paths.
+//
+// Precision: split TF32.  Each difference v (exact in float64) is written as
+// hi + lo with hi = tf32(v), lo = tf32(v - hi); the MMA sums hi*hi' + hi*lo' +
+// lo*hi' in float32 (the lo*lo' term is below float32 resolution).  That keeps
+// ~21 bits of each product instead of TF32's 11 (the "3xTF32" scheme).
+//
+// Kernels
+//   tc_image_kernel     float64 differences -> hi/lo operand images laid out
+//                       exactly as the MMA reads them from shared memory, so
+//                       a whole operand tile is one contiguous bulk copy;
+//   tc_gemm_kernel      persistent, one CTA per SM, warp-specialised: a
+//                       producer lane stages each tile's operands with
+//                       cp.async.bulk (TMA engine, completion on an mbarrier)
+//                       and issues tcgen05.mma into one of two TMEM
+//                       accumulators while 8 epilogue warps drain the other
+//                       (tcgen05.ld -> shared memory -> 2-D TMA tensor store,
+//                       cp.async.bulk.tensor, to HBM);
+//   stream_inc_kernel   the streaming wavefront of stream.cuh reading its
+//                       increments from that matrix (vector loads of the
+//                       lane's coarse rows) instead of forming dot products.
+#pragma once
+
+#include <cuda.h> // CUtensorMap
+
+#include "stream.cuh"
+
+namespace sigk {
+
+constexpr int kTcM = 128;          // MMA M (rows of A per tile)
+constexpr long kTcSpinLimit = 1L << 24;
+
+enum : int { kTcAll = 0, kTcLower = 1, kTcDiag = 2 };
+
+// ------------------------------------------------------------------ TF32 split
+// Round a float to the nearest TF32 value (10 explicit mantissa bits), ties to
+// even, by integer arithmetic on the bit pattern.  Inputs here are finite and
+// far from overflow (scaled path differences).
+__device__ __forceinline__ float tf32_rne(float v)
+{
+    unsigned u = __float_as_uint(v);
+    u += 0x0FFFu + ((u >> 13) & 1u);
+    u &= 0xFFFFE000u;
+    return __uint_as_float(u);
+}
+
+struct TcImageParams {
+    const void *x;      // (npaths, len, d) in TIN
+    int64_t npaths, len, d;
+    int64_t rows_per_path; // rows of a path in the image (>= len - 1; extra rows are zero)
+    int64_t tile_rows;     // rows per operand tile (128 for A, BN for B)
+    int64_t ntiles;
+    int kp;                // K padded to a multiple of 8
+    double f;              // scale f * s[p]
+    const void *s;         // per-path scale in TIN or null
+    float *hi, *lo;
+};
+
+// Image layout: element (row m, k) of tile t = m / tile_rows, r = m % tile_rows
+// sits at float offset ((t * kp/4 + k/4) * tile_rows + r) * 4 + k%4: for each
+// 16-byte chunk of K, the tile's rows are contiguous.  This is the canonical
+// K-major, no-swizzle operand layout of tcgen05.mma (8-row core matrices of
+// 16-byte rows; 128 bytes between row groups, tile_rows*16 bytes between K
+// chunks).
+template <typename TIN>
+__global__ void tc_image_kernel(TcImageParams p)
+{
+    const TIN *__restrict__ x = reinterpret_cast<const TIN *>(p.x);
+    const TIN *__restrict__ sc = reinterpret_cast<const TIN *>(p.s);
+    const int64_t nkc = p.kp / 4;
+    const int64_t total = p.ntiles * p.tile_rows * p.kp;
+    const int64_t nc = p.len - 1;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k4 = e & 3;
+        const int64_t r = (e >> 2) % p.tile_rows;
+        const int64_t rest = (e >> 2) / p.tile_rows;
+        const int64_t kc = rest % nkc;
+        const int64_t t = rest / nkc;
+        const int64_t m = t * p.tile_rows + r;
+        const int64_t k = kc * 4 + k4;
+        const int64_t path = m / p.rows_per_path;
+        const int64_t c = m - path * p.rows_per_path;
+        float hi = 0.f, lo = 0.f;
+        if (path < p.npaths && c < nc && k < p.d) {
+            const TIN *xp = x + (path * p.len + c) * p.d + k;
+            const double g = sc ? p.f * (double)sc[path] : p.f;
+            const double v = ((double)xp[p.d] - (double)xp[0]) * g;
+            hi = tf32_rne((float)v);
+            lo = tf32_rne((float)(v - (double)hi));
+        }
+        p.hi[e] = hi;
+        p.lo[e] = lo;
+    }
+}
+
+// ------------------------------------------------------------------ PTX wrappers
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(bar),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity)
+{
+    uint32_t done;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(done)
+                 : "r"(bar), "r"(parity)
+                 : "memory");
+    return done != 0;
+}
+
+// Bounded wait on an mbarrier phase; false when the limit ran out.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+{
+    for (long i = 0; i < kTcSpinLimit; ++i) {
+        if (mbar_test(bar, parity)) return true;
+        if (i > 64) __nanosleep(64);
+    }
+    return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Shared-memory matrix descriptor (tcgen05): start address, leading (K
+// direction) and stride (M/N direction) byte offsets in 16-byte units, the
+// sm_100 descriptor version (bit 46) and layout type 0 = no swizzle.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo)
+{
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor for kind::tf32: float32 accumulator (bits 4-5 = 1),
+// A and B TF32 (bits 7-9 and 10-12 = 2), both K-major, N >> 3 at bit 17,
+// M >> 4 at bit 24.
+__host__ __device__ constexpr uint32_t tf32_idesc(int M, int N)
+{
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+                 "l"(a), "l"(b), "r"(idesc), "r"(acc)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+// 32 consecutive TMEM columns of this warp's 32 lanes: v[j] = column col + j of lane (row) lane.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32])
+{
+    uint32_t r[32];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                 "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+                 "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                   "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+                   "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+                   "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
+                   "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                 : "r"(taddr)
+                 : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+// ------------------------------------------------------------------ GEMM
+struct TcGemmParams {
+    const float *a_hi, *a_lo; // A image: mtiles tiles of 128 rows
+    const float *b_hi, *b_lo; // B image: ntiles tiles of BN rows
+    int64_t mtiles, ntiles;
+    int kp;
+    int mode;                 // kTcAll / kTcLower (symmetric Gram) / kTcDiag (pairwise)
+    int64_t m_rows, n_rows;   // rows of A / B that are stored (the rest is tile padding)
+    int64_t rows_x, rows_y;   // rows per x path (A) and per y path (B)
+    int64_t npaths_x, npaths_y;
+    int64_t x0;               // kTcLower: global index of the first x path of A (chunked symmetric Gram)
+    float *out;
+    int64_t ld;               // kTcAll/kTcLower: out[n * ld + m]; kTcDiag: out[n * rows_x + m % rows_x]
+    unsigned *err;
+};
+
+template <int BN>
+__device__ __forceinline__ bool tc_tile_needed(const TcGemmParams &p, int64_t mt, int64_t nt)
+{
+    if (p.mode == kTcAll) return true;
+    int64_t i_lo = (mt * kTcM) / p.rows_x;
+    int64_t i_hi = (mt * kTcM + kTcM - 1) / p.rows_x;
+    if (i_hi >= p.npaths_x) i_hi = p.npaths_x - 1;
+    int64_t j_lo = (nt * BN) / p.rows_y;
+    int64_t j_hi = (nt * BN + BN - 1) / p.rows_y;
+    if (j_hi >= p.npaths_y) j_hi = p.npaths_y - 1;
+    if (p.mode == kTcLower) return j_lo <= i_hi + p.x0;
+    return j_lo <= i_hi && i_lo <= j_hi;
+}
+
+template <int BN>
+__device__ __forceinline__ int64_t tc_next_tile(const TcGemmParams &p, int64_t t)
+{
+    const int64_t total = p.mtiles * p.ntiles;
+    for (; t < total; t += gridDim.x)
+        if (tc_tile_needed<BN>(p, t / p.ntiles, t % p.ntiles)) return t;
+    return total;
+}
+
+__device__ __forceinline__ void named_bar(int id, int nthreads)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar)
+{
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(bar) : "memory");
+}
+
+// 2-D tiled TMA store of a shared-memory box (x = innermost coordinate).
+__device__ __forceinline__ void tma_store_2d(const void *map, uint32_t src, int x, int y)
+{
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];" ::"l"(map), "r"(src),
+                 "r"(x), "r"(y)
+                 : "memory");
+}
+
+// Warp roles of tc_gemm_kernel: warps 0-7 drain the accumulators (two per
+// TMEM lane quarter, one per half of the N columns); warp 8 owns the TMEM
+// allocation and its lane 0 stages operands and issues the MMAs.
+constexpr int kTcEpiWarps = 8;
+constexpr int kTcThreads = (kTcEpiWarps + 1) * 32;
+constexpr int kTcStageCols = 32; // columns per TMA store box (box = 128 rows x 32 columns)
+
+// Shared-memory layout of tc_gemm_kernel<BN> (byte offsets).
+struct TcSmem {
+    uint32_t staging;  // 2 halves x 2 buffers x (32 columns x 128 rows) floats
+    uint32_t operands; // a_hi, a_lo (128 x kp), b_hi, b_lo (BN x kp)
+    uint32_t bars;     // full, mma_done[2], acc_empty[2]
+    uint32_t misc;     // TMEM address, abort flag, per-warp ok flags
+    uint32_t total;
+};
+
+__host__ __device__ __forceinline__ TcSmem tc_smem_layout(int bn, int kp)
+{
+    TcSmem s{};
+    s.staging = 0;
+    s.operands = 2 * 2 * kTcStageCols * kTcM * 4;
+    s.bars = s.operands + (2 * kTcM + 2 * bn) * kp * 4;
+    s.misc = s.bars + 5 * 8;
+    s.total = s.misc + 16 + 4 * kTcEpiWarps;
+    return s;
+}
+
+template <int BN>
+__global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(TcGemmParams p, const __grid_constant__ CUtensorMap out_map)
+{
+    static_assert(BN % 64 == 0 && BN >= 64 && BN <= 256, "N of a kind::tf32 MMA with M = 128, in 64-column halves");
+    constexpr uint32_t kCols = 2 * BN; // two accumulators
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const TcSmem L = tc_smem_layout(BN, p.kp);
+    const uint32_t a_bytes = (uint32_t)kTcM * p.kp * 4;
+    const uint32_t b_bytes = (uint32_t)BN * p.kp * 4;
+    const uint32_t sbase = smem_u32(smem);
+    const uint32_t s_ahi = sbase + L.operands, s_alo = s_ahi + a_bytes;
+    const uint32_t s_bhi = s_alo + a_bytes, s_blo = s_bhi + b_bytes;
+    const uint32_t bar_full = sbase + L.bars, bar_mma0 = bar_full + 8, bar_empty0 = bar_full + 24;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + L.misc);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(smem + L.misc + 4);
+    volatile int *ok_flags = reinterpret_cast<volatile int *>(smem + L.misc + 16);
+
+    if (warp == kTcEpiWarps) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(kCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        mbar_init(bar_full, 1);
+        mbar_init(bar_mma0, 1);
+        mbar_init(bar_mma0 + 8, 1);
+        mbar_init(bar_empty0, kTcEpiWarps);
+        mbar_init(bar_empty0 + 8, kTcEpiWarps);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == kTcEpiWarps) {
+        // ---------------------------------------------------------- producer / MMA issuer
+        if (lane == 0) {
+            const uint32_t idesc = tf32_idesc(kTcM, BN);
+            int it = 0;
+            for (int64_t tile = tc_next_tile<BN>(p, blockIdx.x); tile < p.mtiles * p.ntiles;
+                 tile = tc_next_tile<BN>(p, tile + gridDim.x), ++it) {
+                if (*abort_flag) break;
+                const int b = it & 1;
+                bool ok = true;
+                if (it >= 2) ok = mbar_wait(bar_empty0 + 8 * b, ((it - 2) >> 1) & 1); // accumulator b drained
+                if (ok && it >= 1) ok = mbar_wait(bar_mma0 + 8 * ((it - 1) & 1), ((it - 1) >> 1) & 1); // operands free
+                if (!ok) {
+                    atomicOr(p.err, 2u);
+                    *abort_flag = 1;
+                    break;
+                }
+                const int64_t mt = tile / p.ntiles, nt = tile % p.ntiles;
+                mbar_expect_tx(bar_full, 2 * a_bytes + 2 * b_bytes);
+                bulk_g2s(s_ahi, p.a_hi + mt * (int64_t)kTcM * p.kp, a_bytes, bar_full);
+                bulk_g2s(s_alo, p.a_lo + mt * (int64_t)kTcM * p.kp, a_bytes, bar_full);
+                bulk_g2s(s_bhi, p.b_hi + nt * (int64_t)BN * p.kp, b_bytes, bar_full);
+                bulk_g2s(s_blo, p.b_lo + nt * (int64_t)BN * p.kp, b_bytes, bar_full);
+                if (!mbar_wait(bar_full, it & 1)) {
+                    atomicOr(p.err, 1u);
+                    *abort_flag = 1;
+                    mbar_wait(bar_full, it & 1); // a second bounded chance for copies in flight to land
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d = tmem + (uint32_t)(b * BN);
+                // K step ks covers K chunks 2ks and 2ks+1 (8 TF32 values); small terms first
+                for (int ks = 0; ks < p.kp / 8; ++ks) {
+                    const uint32_t ao = (uint32_t)ks * 2 * kTcM * 16, bo = (uint32_t)ks * 2 * BN * 16;
+                    const uint64_t ahi = smem_desc(s_ahi + ao, kTcM * 16, 128);
+                    const uint64_t alo = smem_desc(s_alo + ao, kTcM * 16, 128);
+                    const uint64_t bhi = smem_desc(s_bhi + bo, BN * 16, 128);
+                    const uint64_t blo = smem_desc(s_blo + bo, BN * 16, 128);
+                    mma_tf32(d, alo, bhi, idesc, ks > 0 ? 1u : 0u);
+                    mma_tf32(d, ahi, blo, idesc, 1u);
+                    mma_tf32(d, ahi, bhi, idesc, 1u);
+                }
+                mma_commit(bar_mma0 + 8 * b);
+            }
+            if (it >= 1) mbar_wait(bar_mma0 + 8 * ((it - 1) & 1), ((it - 1) >> 1) & 1); // last MMAs done
+        }
+        __syncwarp();
+    } else {
+        // ---------------------------------------------------------- epilogue: TMEM -> HBM
+        const int quarter = warp & 3, half = warp >> 2;
+        const bool leader = quarter == 0 && lane == 0; // issues this half's TMA stores
+        float *staging = reinterpret_cast<float *>(smem + L.staging);
+        int ctr = 0; // chunks stored by this half (selects the staging buffer)
+        int it = 0;
+        for (int64_t tile = tc_next_tile<BN>(p, blockIdx.x); tile < p.mtiles * p.ntiles;
+             tile = tc_next_tile<BN>(p, tile + gridDim.x), ++it) {
+            const int b = it & 1;
+            bool ok = !*abort_flag && mbar_wait(bar_mma0 + 8 * b, (it >> 1) & 1);
+            if (!ok) {
+                atomicOr(p.err, 2u);
+                *abort_flag = 1;
+            }
+            // the four warps of a half agree before any named barrier of the tile
+            if (lane == 0) ok_flags[warp] = ok ? 1 : 0;
+            named_bar(1 + half, 128);
+            ok = ok_flags[4 * half] && ok_flags[4 * half + 1] && ok_flags[4 * half + 2] && ok_flags[4 * half + 3];
+            named_bar(1 + half, 128);
+            if (!ok) break;
+            tc_fence_after();
+            const int64_t mt = tile / p.ntiles, nt = tile % p.ntiles;
+            const int64_t m = mt * kTcM + quarter * 32 + lane;
+            for (int c = 0; c < BN / 64; ++c, ++ctr) {
+                const int col = half * (BN / 2) + c * 32;
+                float v[32];
+                tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * BN + col), v);
+                const int64_t n0 = nt * BN + col;
+                if (p.mode != kTcDiag) {
+                    float *buf = staging + (size_t)(half * 2 + (ctr & 1)) * (kTcStageCols * kTcM);
+                    if (leader) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+                    named_bar(1 + half, 128); // buf is no longer read by an earlier store
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) buf[j * kTcM + quarter * 32 + lane] = v[j];
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    named_bar(1 + half, 128); // buf complete
+                    if (leader) {
+                        tma_store_2d(&out_map, smem_u32(buf), (int)(mt * kTcM), (int)n0);
+                        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+                    }
+                } else {
+                    const bool mok = m < p.m_rows;
+                    const int64_t px = mok ? m / p.rows_x : 0;
+                    const int64_t cx = m - px * p.rows_x;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const int64_t n = n0 + j;
+                        if (mok && n < p.n_rows && n / p.rows_y == px) p.out[n * p.rows_x + cx] = v[j];
+                    }
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(bar_empty0 + 8 * b);
+        }
+        if (leader) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    }
+    __syncthreads();
+    if (warp == kTcEpiWarps) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
+    }
+}
+
+// Dynamic shared memory of tc_gemm_kernel<BN>; at least 200 KB so that one
+// CTA holds an SM (and all of its TMEM columns).
+__host__ __forceinline__ size_t tc_gemm_smem(int bn, int kp)
+{
+    const size_t s = tc_smem_layout(bn, kp).total;
+    return s < 200 * 1024 ? 200 * 1024 : s;
+}
+
+// ------------------------------------------------------------------ wavefront
+struct StreamIncParams {
+    int op;           // kOpPairwise / kOpGram / kOpGramSym
+    int in64;         // output dtype
+    const float *inc; // increment matrix (see tc_gemm_kernel)
+    int64_t ld;       // Gram ops: floats between rows cj of the matrix
+    int64_t rows_x;   // rows per x path in the matrix (ncx rounded up to 4)
+    int64_t x0;       // first x path of this chunk (Gram ops)
+    int64_t nx, ny;
+    int64_t ncx, ncy;
+    int order;
+    void *out;
+    int64_t out_ld;
+    int64_t item0;    // first item of this chunk
+    int64_t nitems;   // items in this chunk
+    int64_t per_warp;
+    const unsigned *err; // non-zero: the GEMM gave up a wait; results are NaN
+};
+
+// The lane's RC coarse rows at coarse column cj of the pair's block: RC
+// consecutive floats (vector loads, 16-byte aligned because rows_x, ld and
+// the lane's first row are multiples of 4 when RC >= 4).
+template <typename T, int RC>
+__device__ __forceinline__ void load_incs(const float *row, int ci0, int ncx, T (&c)[RC])
+{
+    if constexpr (RC == 1) {
+        c[0] = ci0 < ncx ? T(row[ci0]) : T(0);
+    } else if constexpr (RC == 2) {
+        float2 v = ci0 < ncx ? *reinterpret_cast<const float2 *>(row + ci0) : make_float2(0.f, 0.f);
+        c[0] = T(v.x);
+        c[1] = T(v.y);
+    } else {
+#pragma unroll
+        for (int q = 0; q < RC / 4; ++q) {
+            float4 v = (ci0 + 4 * q < ncx) ? *reinterpret_cast<const float4 *>(row + ci0 + 4 * q)
+                                           : make_float4(0.f, 0.f, 0.f, 0.f);
+            c[4 * q + 0] = T(v.x);
+            c[4 * q + 1] = T(v.y);
+            c[4 * q + 2] = T(v.z);
+            c[4 * q + 3] = T(v.w);
+        }
+    }
+}
+
+template <typename T, int R, int O>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_inc_kernel(StreamIncParams p)
+{
+    using BS = BlockShape<R, O>;
+    constexpr int C = BS::C;
+    constexpr int RC = BS::RC;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int64_t gwarp = (int64_t)blockIdx.x * kWarpsPerBlock + wib;
+    const int64_t first = gwarp * p.per_warp;
+    if (first >= p.nitems) return; // warp-uniform
+    const int cnt = (int)((p.nitems - first) < p.per_warp ? (p.nitems - first) : p.per_warp);
+    const int ncx = (int)p.ncx, ncy = (int)p.ncy;
+    const int n = ncx << p.order;
+    const int nsteps = (ncy << p.order) / C;
+    const int ci0 = (lane * R) >> p.order;
+    const int lstar = (n - 1) / R, rstar = (n - 1) % R;
+    const int64_t row_ld = p.op == kOpPairwise ? p.rows_x : p.ld;
+    StreamParams sp{}; // for stream_decode / stream_store
+    sp.op = p.op;
+    sp.in64 = p.in64;
+    sp.ny = p.ny;
+    sp.out = p.out;
+    sp.out_ld = p.out_ld;
+    if (*p.err) { // the increments are incomplete: report NaN rather than wrong numbers
+        for (int k2 = lane; k2 < cnt; k2 += 32) {
+            int64_t xi, yj;
+            const int64_t item = p.item0 + first + k2;
+            stream_decode(sp, item, xi, yj);
+            stream_store(sp, item, xi, yj, T(NAN));
+        }
+        return;
+    }
+
+    T left[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) left[r] = T(1);
+    T bot[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) bot[c] = T(1);
+    T corner_next = T(1);
+    int q = 0, k = 0;
+    int64_t item = 0, xi = 0, yj = 0;
+    const float *base = p.inc;
+    // The lane's increments for its next active step are loaded one step
+    // ahead (software pipelining across the memory latency).
+    float pre[RC];
+    bool have_pre = false;
+    auto pair_base = [&](int64_t it) -> const float * {
+        int64_t a, b2;
+        stream_decode(sp, it, a, b2);
+        return p.op == kOpPairwise ? p.inc + (it - p.item0) * (int64_t)ncy * p.rows_x
+                                   : p.inc + b2 * (int64_t)ncy * p.ld + (a - p.x0) * p.rows_x;
+    };
+
+    const int total = cnt * nsteps + 31;
+    for (int s = 0; s < total; ++s) {
+        T top[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) top[c] = __shfl_up_sync(kFullMask, bot[c], 1);
+        if (lane == 0) {
+#pragma unroll
+            for (int c = 0; c < C; ++c) top[c] = T(1);
+        }
+        if (s >= lane && k < cnt) {
+            if (q == 0) {
+                item = p.item0 + first + k;
+                stream_decode(sp, item, xi, yj);
+                base = pair_base(item);
+#pragma unroll
+                for (int r = 0; r < R; ++r) left[r] = T(1);
+            }
+            const T corner = (q == 0) ? T(1) : corner_next;
+            corner_next = top[C - 1];
+            float cur[RC];
+            if (have_pre) {
+#pragma unroll
+                for (int rc = 0; rc < RC; ++rc) cur[rc] = pre[rc];
+            } else {
+                const int cj = (O <= 3) ? q : ((q * C) >> p.order);
+                load_incs<float, RC>(base + (int64_t)cj * row_ld, ci0, ncx, cur);
+            }
+            { // prefetch the next step's increments
+                int q2 = q + 1, k2 = k;
+                if (q2 == nsteps) {
+                    q2 = 0;
+                    ++k2;
+                }
+                have_pre = k2 < cnt;
+                if (have_pre) {
+                    const float *b2 = (q2 == 0) ? pair_base(p.item0 + first + k2) : base;
+                    const int cj2 = (O <= 3) ? q2 : ((q2 * C) >> p.order);
+                    load_incs<float, RC>(b2 + (int64_t)cj2 * row_ld, ci0, ncx, pre);
+                }
+            }
+            T A[RC], B[RC];
+#pragma unroll
+            for (int rc = 0; rc < RC; ++rc) stencil_coefs(T(cur[rc]), A[rc], B[rc]);
+            stream_block<T, R, O>(left, top, corner, A, B, bot);
+            if (q == nsteps - 1 && lane == lstar) stream_store(sp, item, xi, yj, pick_row(left, rstar));
+            if (++q == nsteps) {
+                q = 0;
+                ++k;
+            }
+        }
+    }
+}
+
+} // namespace sigk

@@ -9,8 +9,11 @@ Differences from the reference that a caller can observe:
   * PDE cells are float64 by default (`precision="fp64"`), also for float32
     inputs, and the robust normalisation always runs in float64, including
     k(x,x) and f(k(x,x)); the reference rounds every cell to the input dtype
-    and overflows k(x,x) to inf in float32 (SURVEY: 17.6% of the robust
-    benchmark paths).  `precision="fp32"` gives float32 cells;
+    and overflows k(x,x) to inf in float32 (17.6% of the paths of the robust
+    benchmark, N=512 L=64 d=16, scales log-uniform in [0.5, 4]).
+    `precision="fp32"` gives float32 cells; "tc32" / "tc64" form the
+    linear-kernel increments with one split-TF32 tensor-core GEMM and solve
+    float32 / float64 cells (sigk.h describes where they apply);
   * `max_batch` / `max_threads` are accepted and only bound the memory of the
     generic-increment path (non-linear static kernels); the linear kernel runs
     any batch in one launch.
@@ -24,7 +27,8 @@ import torch
 from .. import _lib
 from . import static_kernels
 
-_PREC = {"fp64": _lib.SIGK_PREC_FP64, "fp32": _lib.SIGK_PREC_FP32}
+_PREC = {"fp64": _lib.SIGK_PREC_FP64, "fp32": _lib.SIGK_PREC_FP32, "tc32": _lib.SIGK_PREC_TC32,
+         "tc64": _lib.SIGK_PREC_TC64}
 
 
 def _dtype_code(t: torch.Tensor) -> int:

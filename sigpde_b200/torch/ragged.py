@@ -157,8 +157,10 @@ class RaggedPairwise:
         self._launch()  # warm-up outside the capture (loads the module, sizes the grid)
         torch.cuda.synchronize(self.device)
         g = torch.cuda.CUDAGraph()
+        c0 = _lib.launch_count()
         with torch.cuda.graph(g):
             self._launch()
+        self.graph_kernels = _lib.launch_count() - c0  # kernels each replay runs
         self.graph = g
         return self
 
