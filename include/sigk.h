@@ -241,6 +241,55 @@ SIGK_API int sigk_pairwise_ragged(const void *x_pack, const int64_t *x_off, cons
                                   void *workspace, size_t workspace_bytes, sigk_stream_t stream);
 
 /*
+ * Tensor-core increments for an uneven batch (precision SIGK_PREC_TC32 or
+ * SIGK_PREC_TC64, dim <= 32).  Pair b's coarse increments
+ * <d row_ci, d col_cj> (row path = the shorter of its two paths, as the
+ * wavefront puts it on the rows; rows_b = its coarse cells, cols_b the other
+ * path's) come from one grouped split-TF32 tcgen05 GEMM into a float32 block
+ * of cols_b columns of ld_b = round_up(rows_b, 4) floats, which the wavefront
+ * then reads.  The plan (device arrays except the counts, built once per batch
+ * shape, see sigpde_b200/torch/ragged.py):
+ *   a_row0[b]: first row of pair b's row path in the A operand image (a
+ *     multiple of 8, the pair taking round_up(rows_b, 8) rows); a_rows: image
+ *     rows, at least the last pair's end + 128;
+ *   b_row0[b], b_rows: the same for the column paths (end + 256);
+ *   inc_off[b]: offset (floats, a multiple of 4) of pair b's block in a matrix
+ *     of inc_elems floats;
+ *   tiles (ntiles x 6 int64): one 128 x 256 GEMM tile each,
+ *     {a_row, b_row, m_valid, n_valid, out_off, ld}: a_row = a_row0[b] + 128 i,
+ *     b_row = b_row0[b] + 256 j, m_valid = min(128, rows_b - 128 i),
+ *     n_valid = min(256, cols_b - 256 j), out_off = inc_off[b] + 256 j ld_b +
+ *     128 i, ld = ld_b, for every tile (i, j) of every pair.
+ * A tile entry outside these buffers is skipped and the affected pairs give
+ * NaN (with the error flag of the ragged launch set).  The remaining
+ * arguments are those of sigk_pairwise_ragged.  Workspace:
+ * sigk_ragged_tc_workspace_size(npairs, dim, nitems, bnd_elems, precision,
+ * &plan) bytes, 256-byte aligned.
+ */
+typedef struct {
+    const int64_t *a_row0;
+    const int64_t *b_row0;
+    int64_t a_rows;
+    int64_t b_rows;
+    const int64_t *inc_off;
+    int64_t inc_elems;
+    const int64_t *tiles;
+    int64_t ntiles;
+} sigk_ragged_tc_plan;
+
+SIGK_API size_t sigk_ragged_tc_workspace_size(int64_t npairs, int64_t dim, int64_t nitems, int64_t bnd_elems,
+                                              int precision, const sigk_ragged_tc_plan *plan);
+SIGK_API int sigk_pairwise_ragged_tc(const void *x_pack, const int64_t *x_off, const int64_t *x_len,
+                                     int64_t x_points, const void *y_pack, const int64_t *y_off,
+                                     const int64_t *y_len, int64_t y_points, const int *order,
+                                     const int64_t *item_pair, const int *item_band, int64_t nitems,
+                                     const int *pair_rows, const int *pair_bands, const int64_t *pair_bnd_off,
+                                     int64_t bnd_elems, int64_t npairs, int64_t dim, int dtype, double static_scale,
+                                     const void *scale_x, const void *scale_y, void *out, int precision,
+                                     const sigk_ragged_tc_plan *plan, void *workspace, size_t workspace_bytes,
+                                     sigk_stream_t stream);
+
+/*
  * sigk_gram_noalloc -- sigk_gram for callers that cannot allocate device
  * memory.  It has no counterpart in the reference.
  *

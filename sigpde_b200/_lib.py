@@ -40,6 +40,15 @@ _int = ctypes.c_int
 _dbl = ctypes.c_double
 _sz = ctypes.c_size_t
 
+class RaggedTcPlan(ctypes.Structure):
+    """sigk_ragged_tc_plan (include/sigk.h)."""
+    _fields_ = [("a_row0", ctypes.c_void_p), ("b_row0", ctypes.c_void_p), ("a_rows", ctypes.c_int64),
+                ("b_rows", ctypes.c_int64), ("inc_off", ctypes.c_void_p), ("inc_elems", ctypes.c_int64),
+                ("tiles", ctypes.c_void_p), ("ntiles", ctypes.c_int64)]
+
+
+_plan_p = ctypes.POINTER(RaggedTcPlan)
+
 SIGNATURES = {
     "sigk_version": (ctypes.c_char_p, []),
     "sigk_last_error_string": (ctypes.c_char_p, []),
@@ -62,6 +71,9 @@ SIGNATURES = {
     "sigk_ragged_workspace_size": (_sz, [_i64, _i64, _i64, _i64, _i64, _i64, _int]),
     "sigk_pairwise_ragged": (_int, [_vp, _vp, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _i64,
                                     _i64, _i64, _int, _dbl, _vp, _vp, _vp, _int, _vp, _sz, _vp]),
+    "sigk_ragged_tc_workspace_size": (_sz, [_i64, _i64, _i64, _i64, _int, _plan_p]),
+    "sigk_pairwise_ragged_tc": (_int, [_vp, _vp, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _vp,
+                                       _i64, _i64, _i64, _int, _dbl, _vp, _vp, _vp, _int, _plan_p, _vp, _sz, _vp]),
     "sigk_gram_noalloc": (_int, [_vp, _vp, _i64, _i64, _i64, _i64, _i64, _int, _int, _dbl, _vp, _vp, _vp, _int, _vp]),
 }
 

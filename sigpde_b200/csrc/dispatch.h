@@ -14,6 +14,7 @@ struct RaggedParams;
 struct StreamIncParams;
 struct TcImageParams;
 struct TcGemmParams;
+struct TcRaggedImageParams;
 }
 struct CUtensorMap_st; // cuda.h
 namespace sigk {
@@ -26,6 +27,7 @@ using RaggedDeltaFn = void (*)(const void *, const int64_t *, const int64_t *, c
                                 int64_t, int64_t, void *);
 using StreamIncFn = void (*)(StreamIncParams);
 using TcImageFn = void (*)(TcImageParams);
+using TcRaggedImageFn = void (*)(TcRaggedImageParams);
 using TcGemmFn = void (*)(TcGemmParams, CUtensorMap_st);
 using DeltaFn = void (*)(const void *, int64_t, int64_t, int64_t, int64_t, double, const void *, void *);
 
@@ -42,13 +44,15 @@ StreamFn get_stream_reg_kernel_f64(int R, int O, int D);
 StreamFn get_stream_reg_kernel_f32(int R, int O, int D);
 StreamFn get_stream_smem_kernel(bool f64cells, int R, int O);
 DeltaFn get_delta_kernel(bool f64cells, bool in64);
-RaggedFn get_ragged_kernel(bool f64cells, bool in64);
+// mat: increments from a precomputed matrix (tensor-core modes) instead of differences
+RaggedFn get_ragged_kernel(bool f64cells, bool in64, bool mat);
 RaggedDeltaFn get_ragged_delta_kernel(bool f64cells, bool in64);
 // Tensor-core increments (tc.cuh): operand images, the TF32x3 GEMM (N tile
 // kTcBN) and the streaming wavefront that reads its output.
 constexpr int kTcBN = 256;
 TcImageFn get_tc_image_kernel(bool in64);
 TcGemmFn get_tc_gemm_kernel();
+TcRaggedImageFn get_tc_ragged_image_kernel(bool in64);
 StreamIncFn get_stream_inc_kernel(bool f64cells, int R, int O);
 
 } // namespace sigk

@@ -36,4 +36,9 @@ TcImageFn get_tc_image_kernel(bool in64) { return in64 ? tc_image_kernel<double>
 
 TcGemmFn get_tc_gemm_kernel() { return tc_gemm_kernel<kTcBN>; }
 
+TcRaggedImageFn get_tc_ragged_image_kernel(bool in64)
+{
+    return in64 ? tc_ragged_image_kernel<double> : tc_ragged_image_kernel<float>;
+}
+
 } // namespace sigk

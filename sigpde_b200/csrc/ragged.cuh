@@ -79,6 +79,46 @@ struct RaggedParams {
     int *error;                 // set to 1 if a wait ran out or an item was invalid
     void *pool;                 // boundary rows
     int stage_elems_per_warp;   // dx staging capacity (elements of T) per warp
+    // precomputed increments (tensor-core modes): pair b's block starts at inc + inc_off[b], column-major
+    // over its coarse cells (row path on the rows) with round_up(rows, 4) floats per column
+    const float *inc;
+    const int64_t *inc_off;
+    int64_t inc_elems;
+    const unsigned *tc_err;     // non-zero: the GEMM skipped a tile, the matrix is incomplete
+};
+
+// Increments read from a precomputed float matrix: c[rc] = m[cj * ld + ci0 + rc].
+template <typename T, int RC>
+struct MatIncs {
+    const float *base;
+    int64_t ld;
+    int ci0 = 0, ncx = 0;
+    __device__ __forceinline__ void stage(int64_t ci0_, int64_t ncx_, int, bool)
+    {
+        ci0 = (int)ci0_;
+        ncx = (int)ncx_;
+    }
+    __device__ __forceinline__ void column(int64_t cj, int, T (&c)[RC]) const
+    {
+        const float *row = base + cj * ld;
+        if constexpr (RC == 1) {
+            c[0] = ci0 < ncx ? T(row[ci0]) : T(0);
+        } else if constexpr (RC == 2) {
+            const float2 v = ci0 < ncx ? *reinterpret_cast<const float2 *>(row + ci0) : make_float2(0.f, 0.f);
+            c[0] = T(v.x);
+            c[1] = T(v.y);
+        } else {
+#pragma unroll
+            for (int q = 0; q < RC / 4; ++q) {
+                const float4 v = (ci0 + 4 * q < ncx) ? *reinterpret_cast<const float4 *>(row + ci0 + 4 * q)
+                                                     : make_float4(0.f, 0.f, 0.f, 0.f);
+                c[4 * q + 0] = T(v.x);
+                c[4 * q + 1] = T(v.y);
+                c[4 * q + 2] = T(v.z);
+                c[4 * q + 3] = T(v.w);
+            }
+        }
+    }
 };
 
 constexpr long long kProgressPollLimit = 1ll << 26; // ~4 s with 64 ns sleeps
@@ -205,38 +245,52 @@ __device__ T band_solve(const SolveGeom &g, Src &src, int band, bool last, const
     return result;
 }
 
-template <typename T, int R, int O>
-__device__ T ragged_band(const T *dX, const T *dY, int64_t ncx, int64_t ncy, int64_t d, int order, T *stage,
-                         int stage_cap, int band, bool last, const T *top_buf, const int *top_prog, T *bot_buf,
-                         int *bot_prog, int *error)
+// The increments of one band: from the scaled differences (DeltaIncs, MAT =
+// false) or from the pair's precomputed block (MatIncs, MAT = true).
+struct BandSource {
+    const void *dX, *dY;  // differences (T), !MAT
+    int64_t d;
+    const float *mat;     // increment block, MAT
+    int64_t ld;
+};
+
+template <typename T, int R, int O, bool MAT>
+__device__ T ragged_band(const BandSource &bs, int64_t ncx, int64_t ncy, int order, T *stage, int stage_cap, int band,
+                         bool last, const T *top_buf, const int *top_prog, T *bot_buf, int *bot_prog, int *error)
 {
     using BS = BlockShape<R, O>;
-    DeltaIncs<T, BS::RC> src;
-    src.dX = dX;
-    src.dY = dY;
-    src.d = d;
-    src.ncy = ncy;
-    src.dxs = ((int64_t)BS::RC * d * 32 <= stage_cap) ? stage : nullptr;
     const SolveGeom g = make_geom<R, O>(ncx, ncy, order);
-    return band_solve<T, R, O>(g, src, band, last, top_buf, top_prog, bot_buf, bot_prog, error);
-}
-
-template <typename T, int R>
-__device__ T ragged_band_by_o(const T *dX, const T *dY, int64_t ncx, int64_t ncy, int64_t d, int order, T *stage,
-                              int stage_cap, int band, bool last, const T *tb, const int *tp, T *bb, int *bp,
-                              int *error)
-{
-    switch (order) {
-    case 0: return ragged_band<T, R, 0>(dX, dY, ncx, ncy, d, order, stage, stage_cap, band, last, tb, tp, bb, bp, error);
-    case 1: return ragged_band<T, R, 1>(dX, dY, ncx, ncy, d, order, stage, stage_cap, band, last, tb, tp, bb, bp, error);
-    case 2: return ragged_band<T, R, 2>(dX, dY, ncx, ncy, d, order, stage, stage_cap, band, last, tb, tp, bb, bp, error);
-    case 3: return ragged_band<T, R, 3>(dX, dY, ncx, ncy, d, order, stage, stage_cap, band, last, tb, tp, bb, bp, error);
-    default:
-        return ragged_band<T, R, 4>(dX, dY, ncx, ncy, d, order, stage, stage_cap, band, last, tb, tp, bb, bp, error);
+    if constexpr (MAT) {
+        MatIncs<T, BS::RC> src;
+        src.base = bs.mat;
+        src.ld = bs.ld;
+        return band_solve<T, R, O>(g, src, band, last, top_buf, top_prog, bot_buf, bot_prog, error);
+    } else {
+        DeltaIncs<T, BS::RC> src;
+        src.dX = reinterpret_cast<const T *>(bs.dX);
+        src.dY = reinterpret_cast<const T *>(bs.dY);
+        src.d = bs.d;
+        src.ncy = ncy;
+        src.dxs = ((int64_t)BS::RC * bs.d * 32 <= stage_cap) ? stage : nullptr;
+        return band_solve<T, R, O>(g, src, band, last, top_buf, top_prog, bot_buf, bot_prog, error);
     }
 }
 
-template <typename T, typename TIN>
+template <typename T, int R, bool MAT>
+__device__ T ragged_band_by_o(const BandSource &bs, int64_t ncx, int64_t ncy, int order, T *stage, int stage_cap,
+                              int band, bool last, const T *tb, const int *tp, T *bb, int *bp, int *error)
+{
+    switch (order) {
+    case 0: return ragged_band<T, R, 0, MAT>(bs, ncx, ncy, order, stage, stage_cap, band, last, tb, tp, bb, bp, error);
+    case 1: return ragged_band<T, R, 1, MAT>(bs, ncx, ncy, order, stage, stage_cap, band, last, tb, tp, bb, bp, error);
+    case 2: return ragged_band<T, R, 2, MAT>(bs, ncx, ncy, order, stage, stage_cap, band, last, tb, tp, bb, bp, error);
+    case 3: return ragged_band<T, R, 3, MAT>(bs, ncx, ncy, order, stage, stage_cap, band, last, tb, tp, bb, bp, error);
+    default:
+        return ragged_band<T, R, 4, MAT>(bs, ncx, ncy, order, stage, stage_cap, band, last, tb, tp, bb, bp, error);
+    }
+}
+
+template <typename T, typename TIN, bool MAT>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) ragged_kernel(RaggedParams p)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -269,8 +323,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) ragged_kernel(RaggedParam
         const int R = p.pair_rows[b];
         const int nb = p.pair_bands[b];
         int64_t lx = p.x_len[b], ly = p.y_len[b];
-        const T *X = dxp + (p.x_off[b] - b) * d;
-        const T *Y = dyp + (p.y_off[b] - b) * d;
+        const T *X = MAT ? nullptr : dxp + (p.x_off[b] - b) * d;
+        const T *Y = MAT ? nullptr : dyp + (p.y_off[b] - b) * d;
         if (lx > ly) { // shorter path on the rows
             const T *t = X;
             X = Y;
@@ -291,6 +345,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) ragged_kernel(RaggedParam
                  p.pair_bnd_off[b] >= 0 && p.pair_bnd_off[b] + (int64_t)(nb - 1) * (m + 1) <= p.bnd_elems &&
                  m + 1 <= 0x7fffffff;
             if (ok && band > 0) ok = it >= 1 && p.item_pair[it - 1] == b && p.item_band[it - 1] == band - 1;
+            if (ok && MAT) { // the pair's increment block lies inside the matrix and is 16-byte aligned
+                const int64_t o = p.inc_off[b], ldb = (ncx + 3) & ~3LL;
+                ok = o >= 0 && (o & 3) == 0 && o + ncy * ldb <= p.inc_elems && *p.tc_err == 0;
+            }
         }
         if (!ok) {
             if (lane == 0) {
@@ -306,12 +364,19 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) ragged_kernel(RaggedParam
         const int *tp = band > 0 ? p.progress + it - 1 : nullptr;
         T *bb = last ? nullptr : base + (int64_t)band * (m + 1);
         int *bp = p.progress + it;
+        BandSource bs;
+        bs.dX = X;
+        bs.dY = Y;
+        bs.d = d;
+        bs.mat = MAT ? p.inc + p.inc_off[b] : nullptr;
+        bs.ld = (ncx + 3) & ~3LL;
+        const int cap = p.stage_elems_per_warp;
         T v;
         switch (R) {
-        case 2: v = ragged_band_by_o<T, 2>(X, Y, ncx, ncy, d, order, stage, p.stage_elems_per_warp, band, last, tb, tp, bb, bp, p.error); break;
-        case 4: v = ragged_band_by_o<T, 4>(X, Y, ncx, ncy, d, order, stage, p.stage_elems_per_warp, band, last, tb, tp, bb, bp, p.error); break;
-        case 8: v = ragged_band_by_o<T, 8>(X, Y, ncx, ncy, d, order, stage, p.stage_elems_per_warp, band, last, tb, tp, bb, bp, p.error); break;
-        default: v = ragged_band_by_o<T, 16>(X, Y, ncx, ncy, d, order, stage, p.stage_elems_per_warp, band, last, tb, tp, bb, bp, p.error); break;
+        case 2: v = ragged_band_by_o<T, 2, MAT>(bs, ncx, ncy, order, stage, cap, band, last, tb, tp, bb, bp, p.error); break;
+        case 4: v = ragged_band_by_o<T, 4, MAT>(bs, ncx, ncy, order, stage, cap, band, last, tb, tp, bb, bp, p.error); break;
+        case 8: v = ragged_band_by_o<T, 8, MAT>(bs, ncx, ncy, order, stage, cap, band, last, tb, tp, bb, bp, p.error); break;
+        default: v = ragged_band_by_o<T, 16, MAT>(bs, ncx, ncy, order, stage, cap, band, last, tb, tp, bb, bp, p.error); break;
         }
         if (last && lane == 0) out[b] = TIN(v);
     }

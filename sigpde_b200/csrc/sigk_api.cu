@@ -433,7 +433,7 @@ int tc_gemm(const TcGemmParams &gp, cudaStream_t stream)
     }
     CUtensorMap map;
     memset(&map, 0, sizeof(map));
-    if (gp.mode != kTcDiag) {
+    if (gp.mode == kTcAll || gp.mode == kTcLower) { // 2-D TMA stores into the Gram's increment matrix
         if ((gp.ld & 3) != 0 || ((uintptr_t)gp.out & 15) != 0)
             return fail(SIGK_EINVAL, "increment matrix rows must be 16-byte aligned");
         int st = encode_out_map(&map, gp.out, gp.ld, gp.n_rows);
@@ -1032,15 +1032,37 @@ extern "C" size_t sigk_ragged_workspace_size(int64_t npairs, int64_t x_points, i
     return ragged_plan(npairs, x_points, y_points, dim, nitems, bnd_elems, tsize_of(precision)).ws_bytes;
 }
 
-extern "C" int sigk_pairwise_ragged(const void *x_pack, const int64_t *x_off, const int64_t *x_len, int64_t x_points,
-                                    const void *y_pack, const int64_t *y_off, const int64_t *y_len, int64_t y_points,
-                                    const int *order, const int64_t *item_pair, const int *item_band, int64_t nitems,
-                                    const int *pair_rows, const int *pair_bands, const int64_t *pair_bnd_off,
-                                    int64_t bnd_elems, int64_t npairs, int64_t dim, int dtype, double static_scale,
-                                    const void *scale_x, const void *scale_y, void *out, int precision,
-                                    void *workspace, size_t workspace_bytes, sigk_stream_t stream_)
+namespace sigk {
+namespace {
+// Tensor-core layout of an uneven batch in the workspace, after the ragged
+// plan's counters and boundary pool: GEMM error word, A and B operand images
+// (hi, lo), the increment matrix.
+struct RaggedTcLayout {
+    int kp;
+    size_t err_off, a_off, a_bytes, b_off, b_bytes, inc_off, ws_bytes;
+};
+
+RaggedTcLayout ragged_tc_layout(size_t base, int64_t dim, const sigk_ragged_tc_plan &pl)
 {
-    cudaStream_t stream = (cudaStream_t)stream_;
+    RaggedTcLayout t{};
+    t.kp = (int)((dim + 7) / 8 * 8);
+    t.err_off = align256(base);
+    t.a_off = t.err_off + 256;
+    t.a_bytes = align256((size_t)pl.a_rows * t.kp * sizeof(float));
+    t.b_off = t.a_off + 2 * t.a_bytes;
+    t.b_bytes = align256((size_t)pl.b_rows * t.kp * sizeof(float));
+    t.inc_off = t.b_off + 2 * t.b_bytes;
+    t.ws_bytes = t.inc_off + align256((size_t)pl.inc_elems * sizeof(float));
+    return t;
+}
+
+int run_ragged(const void *x_pack, const int64_t *x_off, const int64_t *x_len, int64_t x_points, const void *y_pack,
+               const int64_t *y_off, const int64_t *y_len, int64_t y_points, const int *order,
+               const int64_t *item_pair, const int *item_band, int64_t nitems, const int *pair_rows,
+               const int *pair_bands, const int64_t *pair_bnd_off, int64_t bnd_elems, int64_t npairs, int64_t dim,
+               int dtype, double static_scale, const void *scale_x, const void *scale_y, void *out, int precision,
+               const sigk_ragged_tc_plan *tc, void *workspace, size_t workspace_bytes, cudaStream_t stream)
+{
     int st = check_common(dtype, precision, 0);
     if (st) return st;
     if (npairs < 1) return fail(SIGK_EINVAL, "npairs must be >= 1");
@@ -1059,31 +1081,106 @@ extern "C" int sigk_pairwise_ragged(const void *x_pack, const int64_t *x_off, co
         (st = check_dev(out, "out", false)) || (st = check_dev(scale_x, "scale_x", true)) ||
         (st = check_dev(scale_y, "scale_y", true)))
         return st;
+    if (tc) {
+        if (!is_tc(precision)) return fail(SIGK_EINVAL, "a tensor-core plan needs precision SIGK_PREC_TC32 or _TC64");
+        if (dim > 32) return fail(SIGK_EUNSUPPORTED, "tensor-core increments support dim <= 32 (got %lld)",
+                                  (long long)dim);
+        if (tc->a_rows < kTcM || tc->b_rows < kTcBN || tc->inc_elems < 4 || tc->ntiles < 1 ||
+            (tc->a_rows & 7) || (tc->b_rows & 7))
+            return fail(SIGK_EINVAL, "tensor-core plan sizes are inconsistent");
+        if ((st = check_dev(tc->a_row0, "plan.a_row0", false)) || (st = check_dev(tc->b_row0, "plan.b_row0", false)) ||
+            (st = check_dev(tc->inc_off, "plan.inc_off", false)) || (st = check_dev(tc->tiles, "plan.tiles", false)))
+            return st;
+    }
     const size_t ts = tsize_of(precision);
     const bool f64 = cell_prec(precision) == SIGK_PREC_FP64, in64 = dtype == SIGK_F64;
-    RaggedPlan pl = ragged_plan(npairs, x_points, y_points, dim, nitems, bnd_elems, ts);
-    if (!workspace || workspace_bytes < pl.ws_bytes)
-        return fail(SIGK_ENOMEM, "workspace of %zu bytes needed (got %zu)", pl.ws_bytes, workspace ? workspace_bytes : 0);
+    RaggedPlan pl = ragged_plan(npairs, tc ? 2 * npairs : x_points, tc ? 2 * npairs : y_points, dim, nitems,
+                                bnd_elems, ts);
+    RaggedTcLayout tl{};
+    size_t need = pl.ws_bytes;
+    if (tc) {
+        tl = ragged_tc_layout(pl.dx_off, dim, *tc);
+        need = tl.ws_bytes;
+    }
+    if (!workspace || workspace_bytes < need)
+        return fail(SIGK_ENOMEM, "workspace of %zu bytes needed (got %zu)", need, workspace ? workspace_bytes : 0);
     if (((uintptr_t)workspace & 255) != 0) return fail(SIGK_EINVAL, "workspace must be 256-byte aligned");
     unsigned char *wsb = reinterpret_cast<unsigned char *>(workspace);
-    // work counter, error flag and per-item progress start at zero
+    // work counter, error flag and per-item progress start at zero (and the GEMM's error word)
     cudaError_t e = cudaMemsetAsync(wsb, 0, pl.pool_off, stream);
+    if (e == cudaSuccess && tc) e = cudaMemsetAsync(wsb + tl.err_off, 0, 256, stream);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(counters)");
-
-    // scaled, dimension-major differences of both packs: static_scale * 4^-order * scale_x on x, scale_y on y.
-    // grid: y over paths (strided beyond 65535), x over one path's (len - 1) * dim values
-    RaggedDeltaFn delta = get_ragged_delta_kernel(f64, in64);
-    const dim3 dgrid(32, (unsigned)(npairs < 65535 ? npairs : 65535));
-    delta<<<dgrid, 256, 0, stream>>>(x_pack, x_off, x_len, order, static_scale, scale_x, npairs, dim, wsb + pl.dx_off);
-    count_launch();
-    delta<<<dgrid, 256, 0, stream>>>(y_pack, y_off, y_len, nullptr, 1.0, scale_y, npairs, dim, wsb + pl.dy_off);
-    count_launch();
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_fail(e, "ragged delta launch");
+    const int nsm = sm_count();
 
     RaggedParams p{};
-    p.dx_pack = wsb + pl.dx_off;
-    p.dy_pack = wsb + pl.dy_off;
+    if (!tc) {
+        // scaled, dimension-major differences of both packs: static_scale * 4^-order * scale_x on x, scale_y on y.
+        // grid: y over paths (strided beyond 65535), x over one path's (len - 1) * dim values
+        RaggedDeltaFn delta = get_ragged_delta_kernel(f64, in64);
+        const dim3 dgrid(32, (unsigned)(npairs < 65535 ? npairs : 65535));
+        delta<<<dgrid, 256, 0, stream>>>(x_pack, x_off, x_len, order, static_scale, scale_x, npairs, dim,
+                                         wsb + pl.dx_off);
+        count_launch();
+        delta<<<dgrid, 256, 0, stream>>>(y_pack, y_off, y_len, nullptr, 1.0, scale_y, npairs, dim, wsb + pl.dy_off);
+        count_launch();
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(e, "ragged delta launch");
+        p.dx_pack = wsb + pl.dx_off;
+        p.dy_pack = wsb + pl.dy_off;
+    } else {
+        float *a_hi = reinterpret_cast<float *>(wsb + tl.a_off), *a_lo = reinterpret_cast<float *>(wsb + tl.a_off + tl.a_bytes);
+        float *b_hi = reinterpret_cast<float *>(wsb + tl.b_off), *b_lo = reinterpret_cast<float *>(wsb + tl.b_off + tl.b_bytes);
+        float *inc = reinterpret_cast<float *>(wsb + tl.inc_off);
+        unsigned *gerr = reinterpret_cast<unsigned *>(wsb + tl.err_off);
+        TcRaggedImageFn image = get_tc_ragged_image_kernel(in64);
+        const dim3 igrid(8, (unsigned)(npairs < 65535 ? npairs : 65535));
+        for (int side = 0; side < 2; ++side) {
+            TcRaggedImageParams ip{};
+            ip.x_pack = x_pack;
+            ip.y_pack = y_pack;
+            ip.x_off = x_off;
+            ip.x_len = x_len;
+            ip.y_off = y_off;
+            ip.y_len = y_len;
+            ip.order = order;
+            ip.f = static_scale;
+            ip.sx = scale_x;
+            ip.sy = scale_y;
+            ip.row0 = side == 0 ? tc->a_row0 : tc->b_row0;
+            ip.rows_alloc = side == 0 ? tc->a_rows : tc->b_rows;
+            ip.npairs = npairs;
+            ip.d = dim;
+            ip.kp = tl.kp;
+            ip.side = side;
+            ip.hi = side == 0 ? a_hi : b_hi;
+            ip.lo = side == 0 ? a_lo : b_lo;
+            image<<<igrid, 256, 0, stream>>>(ip);
+            count_launch();
+        }
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(e, "ragged operand image launch");
+        TcGemmParams gp{};
+        gp.a_hi = a_hi;
+        gp.a_lo = a_lo;
+        gp.b_hi = b_hi;
+        gp.b_lo = b_lo;
+        gp.mtiles = tc->ntiles;
+        gp.ntiles = 1;
+        gp.kp = tl.kp;
+        gp.mode = kTcTable;
+        gp.out = inc;
+        gp.err = gerr;
+        gp.table = tc->tiles;
+        gp.ntable = tc->ntiles;
+        gp.a_rows = tc->a_rows;
+        gp.b_rows = tc->b_rows;
+        gp.out_elems = tc->inc_elems;
+        if ((st = tc_gemm(gp, stream))) return st;
+        p.inc = inc;
+        p.inc_off = tc->inc_off;
+        p.inc_elems = tc->inc_elems;
+        p.tc_err = gerr;
+    }
     p.x_off = x_off;
     p.x_len = x_len;
     p.y_off = y_off;
@@ -1103,17 +1200,59 @@ extern "C" int sigk_pairwise_ragged(const void *x_pack, const int64_t *x_off, co
     p.error = reinterpret_cast<int *>(wsb + pl.error_off);
     p.progress = reinterpret_cast<int *>(wsb + pl.progress_off);
     p.pool = wsb + pl.pool_off;
-    p.stage_elems_per_warp = (int)(kRaggedStageBytesPerWarp / ts);
-    RaggedFn fn = get_ragged_kernel(f64, in64);
-    const size_t smem = kRaggedStageBytesPerWarp * kWarpsPerBlock;
+    p.stage_elems_per_warp = tc ? 0 : (int)(kRaggedStageBytesPerWarp / ts);
+    RaggedFn fn = get_ragged_kernel(f64, in64, tc != nullptr);
+    const size_t smem = tc ? 0 : kRaggedStageBytesPerWarp * kWarpsPerBlock;
     int nb = 0;
     if ((st = blocks_per_sm((const void *)fn, smem, &nb))) return st;
     // persistent grid: never more blocks than can be resident at once (band waits rely on it)
-    int64_t blocks = (int64_t)sm_count() * nb;
+    int64_t blocks = (int64_t)nsm * nb;
     const int64_t want = (nitems + kWarpsPerBlock - 1) / kWarpsPerBlock;
     if (blocks > want) blocks = want;
     fn<<<(unsigned)blocks, kWarpsPerBlock * 32, smem, stream>>>(p);
     count_launch();
     e = cudaGetLastError();
     return e == cudaSuccess ? SIGK_OK : cuda_fail(e, "ragged kernel launch");
+}
+} // namespace
+} // namespace sigk
+
+extern "C" int sigk_pairwise_ragged(const void *x_pack, const int64_t *x_off, const int64_t *x_len, int64_t x_points,
+                                    const void *y_pack, const int64_t *y_off, const int64_t *y_len, int64_t y_points,
+                                    const int *order, const int64_t *item_pair, const int *item_band, int64_t nitems,
+                                    const int *pair_rows, const int *pair_bands, const int64_t *pair_bnd_off,
+                                    int64_t bnd_elems, int64_t npairs, int64_t dim, int dtype, double static_scale,
+                                    const void *scale_x, const void *scale_y, void *out, int precision,
+                                    void *workspace, size_t workspace_bytes, sigk_stream_t stream)
+{
+    if (is_tc(precision)) precision = cell_prec(precision); // no plan: CUDA-core increments, same cells
+    return run_ragged(x_pack, x_off, x_len, x_points, y_pack, y_off, y_len, y_points, order, item_pair, item_band,
+                      nitems, pair_rows, pair_bands, pair_bnd_off, bnd_elems, npairs, dim, dtype, static_scale,
+                      scale_x, scale_y, out, precision, nullptr, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+extern "C" size_t sigk_ragged_tc_workspace_size(int64_t npairs, int64_t dim, int64_t nitems, int64_t bnd_elems,
+                                                int precision, const sigk_ragged_tc_plan *plan)
+{
+    if (!plan || npairs < 1 || dim < 1 || dim > 32 || nitems < npairs || bnd_elems < 0 || plan->a_rows < 0 ||
+        plan->b_rows < 0 || plan->inc_elems < 0)
+        return 0;
+    RaggedPlan pl = ragged_plan(npairs, 2 * npairs, 2 * npairs, dim, nitems, bnd_elems, tsize_of(precision));
+    return ragged_tc_layout(pl.dx_off, dim, *plan).ws_bytes;
+}
+
+extern "C" int sigk_pairwise_ragged_tc(const void *x_pack, const int64_t *x_off, const int64_t *x_len,
+                                       int64_t x_points, const void *y_pack, const int64_t *y_off,
+                                       const int64_t *y_len, int64_t y_points, const int *order,
+                                       const int64_t *item_pair, const int *item_band, int64_t nitems,
+                                       const int *pair_rows, const int *pair_bands, const int64_t *pair_bnd_off,
+                                       int64_t bnd_elems, int64_t npairs, int64_t dim, int dtype,
+                                       double static_scale, const void *scale_x, const void *scale_y, void *out,
+                                       int precision, const sigk_ragged_tc_plan *plan, void *workspace,
+                                       size_t workspace_bytes, sigk_stream_t stream)
+{
+    if (!plan) return fail(SIGK_EINVAL, "plan is NULL");
+    return run_ragged(x_pack, x_off, x_len, x_points, y_pack, y_off, y_len, y_points, order, item_pair, item_band,
+                      nitems, pair_rows, pair_bands, pair_bnd_off, bnd_elems, npairs, dim, dtype, static_scale,
+                      scale_x, scale_y, out, precision, plan, workspace, workspace_bytes, (cudaStream_t)stream);
 }

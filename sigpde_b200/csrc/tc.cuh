@@ -37,7 +37,7 @@ namespace sigk {
 constexpr int kTcM = 128;          // MMA M (rows of A per tile)
 constexpr long kTcSpinLimit = 1L << 24;
 
-enum : int { kTcAll = 0, kTcLower = 1, kTcDiag = 2 };
+enum : int { kTcAll = 0, kTcLower = 1, kTcDiag = 2, kTcTable = 3 };
 
 // ------------------------------------------------------------------ TF32 split
 // Round a float to the nearest TF32 value (10 explicit mantissa bits), ties to
@@ -63,12 +63,19 @@ struct TcImageParams {
     float *hi, *lo;
 };
 
-// Image layout: element (row m, k) of tile t = m / tile_rows, r = m % tile_rows
-// sits at float offset ((t * kp/4 + k/4) * tile_rows + r) * 4 + k%4: for each
-// 16-byte chunk of K, the tile's rows are contiguous.  This is the canonical
-// K-major, no-swizzle operand layout of tcgen05.mma (8-row core matrices of
-// 16-byte rows; 128 bytes between row groups, tile_rows*16 bytes between K
-// chunks).
+// Image layout (group-major): element (row m, k) sits at float offset
+// ((m/8 * kp/4 + k/4) * 8 + m%8) * 4 + k%4.  A group of 8 rows holds all of K
+// as kp/4 core matrices of 8 rows x 16 bytes (128 bytes each), so any run of
+// rows that starts at a multiple of 8 is one contiguous block: an operand
+// tile is a single bulk copy wherever it starts.  For tcgen05.mma this is the
+// canonical K-major, no-swizzle layout with 128 bytes between the two K
+// chunks of one MMA (leading byte offset) and kp*32 bytes between 8-row
+// groups (stride byte offset).
+__host__ __device__ __forceinline__ int64_t image_offset(int64_t m, int64_t k, int kp)
+{
+    return (((m >> 3) * (kp >> 2) + (k >> 2)) * 8 + (m & 7)) * 4 + (k & 3);
+}
+
 template <typename TIN>
 __global__ void tc_image_kernel(TcImageParams p)
 {
@@ -79,12 +86,13 @@ __global__ void tc_image_kernel(TcImageParams p)
     const int64_t nc = p.len - 1;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
          e += (int64_t)gridDim.x * blockDim.x) {
+        // e enumerates the image in memory order: group, K chunk, row in group, k in chunk
         const int64_t k4 = e & 3;
-        const int64_t r = (e >> 2) % p.tile_rows;
-        const int64_t rest = (e >> 2) / p.tile_rows;
+        const int64_t r8 = (e >> 2) & 7;
+        const int64_t rest = e >> 5;
         const int64_t kc = rest % nkc;
-        const int64_t t = rest / nkc;
-        const int64_t m = t * p.tile_rows + r;
+        const int64_t g = rest / nkc;
+        const int64_t m = g * 8 + r8;
         const int64_t k = kc * 4 + k4;
         const int64_t path = m / p.rows_per_path;
         const int64_t c = m - path * p.rows_per_path;
@@ -98,6 +106,67 @@ __global__ void tc_image_kernel(TcImageParams p)
         }
         p.hi[e] = hi;
         p.lo[e] = lo;
+    }
+}
+
+// Operand images of an uneven batch: pair b's row path (the shorter of its
+// two paths, as the wavefront puts it on the rows) goes to the A image at
+// row0[b] (side 0), its column path to the B image (side 1).  Rows of a pair
+// are padded to a multiple of 8 with zeros.  The A side carries the static
+// scale and 4^-order of the pair; each side carries its own path's scale.
+struct TcRaggedImageParams {
+    const void *x_pack, *y_pack;
+    const int64_t *x_off, *x_len, *y_off, *y_len;
+    const int *order;
+    double f;
+    const void *sx, *sy;  // per pair, TIN, or null
+    const int64_t *row0;  // per pair: first image row (multiple of 8)
+    int64_t rows_alloc;
+    int64_t npairs, d;
+    int kp;
+    int side;
+    float *hi, *lo;
+};
+
+template <typename TIN>
+__global__ void tc_ragged_image_kernel(TcRaggedImageParams p)
+{
+    const int64_t nkc = p.kp / 4;
+    for (int64_t b = blockIdx.y; b < p.npairs; b += gridDim.y) {
+        const int64_t lx = p.x_len[b], ly = p.y_len[b];
+        const bool use_y = (p.side == 0) == (lx > ly);
+        const TIN *pack = reinterpret_cast<const TIN *>(use_y ? p.y_pack : p.x_pack);
+        const TIN *sc = reinterpret_cast<const TIN *>(use_y ? p.sy : p.sx);
+        const int64_t off = use_y ? p.y_off[b] : p.x_off[b];
+        const int64_t nc = (use_y ? ly : lx) - 1;
+        const int ord = p.order[b];
+        const int64_t r0 = p.row0[b];
+        const int64_t rows8 = (nc + 7) & ~7LL;
+        // a pair the plan cannot hold is skipped; the wavefront refuses it too
+        if (nc < 1 || ord < 0 || ord > 12 || r0 < 0 || (r0 & 7) != 0 || r0 + rows8 > p.rows_alloc) continue;
+        double g = sc ? (double)sc[b] : 1.0;
+        if (p.side == 0) g *= p.f * ldexp(1.0, -2 * ord);
+        const TIN *xp0 = pack + off * p.d;
+        float *hi = p.hi + r0 * p.kp, *lo = p.lo + r0 * p.kp;
+        const int64_t total = rows8 * p.kp;
+        for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+             e += (int64_t)gridDim.x * blockDim.x) {
+            const int64_t k4 = e & 3;
+            const int64_t r8 = (e >> 2) & 7;
+            const int64_t rest = e >> 5;
+            const int64_t kc = rest % nkc;
+            const int64_t c = (rest / nkc) * 8 + r8;
+            const int64_t k = kc * 4 + k4;
+            float h = 0.f, l = 0.f;
+            if (c < nc && k < p.d) {
+                const TIN *xp = xp0 + c * p.d + k;
+                const double v = ((double)xp[p.d] - (double)xp[0]) * g;
+                h = tf32_rne((float)v);
+                l = tf32_rne((float)(v - (double)h));
+            }
+            hi[e] = h;
+            lo[e] = l;
+        }
     }
 }
 
@@ -213,7 +282,16 @@ struct TcGemmParams {
     float *out;
     int64_t ld;               // kTcAll/kTcLower: out[n * ld + m]; kTcDiag: out[n * rows_x + m % rows_x]
     unsigned *err;
+    // kTcTable (uneven pairs): one entry of kTcTileWords per tile, {a_row, b_row, m_valid, n_valid,
+    // out_off, ld}: the tile's first A and B image rows (multiples of 8), its valid rows and columns,
+    // and where its (column-major, ld floats per column) block of increments starts in out
+    const int64_t *table;
+    int64_t ntable;
+    int64_t a_rows, b_rows;   // image rows allocated (tiles must lie inside)
+    int64_t out_elems;        // floats in out
 };
+
+constexpr int kTcTileWords = 6;
 
 template <int BN>
 __device__ __forceinline__ bool tc_tile_needed(const TcGemmParams &p, int64_t mt, int64_t nt)
@@ -229,12 +307,35 @@ __device__ __forceinline__ bool tc_tile_needed(const TcGemmParams &p, int64_t mt
     return j_lo <= i_hi && i_lo <= j_hi;
 }
 
+// A table entry that would read or write outside its buffers is refused
+// (error bit 4) and skipped by both warp roles alike.
+template <int BN>
+__device__ __forceinline__ bool tc_table_entry_ok(const TcGemmParams &p, const int64_t *e)
+{
+    const int64_t a_row = e[0], b_row = e[1], mv = e[2], nv = e[3], off = e[4], ld = e[5];
+    return a_row >= 0 && (a_row & 7) == 0 && a_row + kTcM <= p.a_rows && b_row >= 0 && (b_row & 7) == 0 &&
+           b_row + BN <= p.b_rows && mv >= 1 && mv <= kTcM && nv >= 1 && nv <= BN && ld >= 4 && (ld & 3) == 0 &&
+           ((mv + 3) & ~3LL) <= ld && off >= 0 && (off & 3) == 0 && off + (nv - 1) * ld + ((mv + 3) & ~3LL) <= p.out_elems;
+}
+
+template <int BN>
+__device__ __forceinline__ int64_t tc_total_tiles(const TcGemmParams &p)
+{
+    return p.mode == kTcTable ? p.ntable : p.mtiles * p.ntiles;
+}
+
 template <int BN>
 __device__ __forceinline__ int64_t tc_next_tile(const TcGemmParams &p, int64_t t)
 {
-    const int64_t total = p.mtiles * p.ntiles;
-    for (; t < total; t += gridDim.x)
-        if (tc_tile_needed<BN>(p, t / p.ntiles, t % p.ntiles)) return t;
+    const int64_t total = tc_total_tiles<BN>(p);
+    for (; t < total; t += gridDim.x) {
+        if (p.mode == kTcTable) {
+            if (tc_table_entry_ok<BN>(p, p.table + t * kTcTileWords)) return t;
+            if (threadIdx.x == 0) atomicOr(p.err, 4u);
+        } else if (tc_tile_needed<BN>(p, t / p.ntiles, t % p.ntiles)) {
+            return t;
+        }
+    }
     return total;
 }
 
@@ -246,6 +347,13 @@ __device__ __forceinline__ void named_bar(int id, int nthreads)
 __device__ __forceinline__ void mbar_arrive(uint32_t bar)
 {
     asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(bar) : "memory");
+}
+
+// Contiguous bulk copy shared -> global (TMA engine); 16-byte aligned, size a multiple of 16.
+__device__ __forceinline__ void bulk_s2g(void *dst, uint32_t src, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(src), "r"(bytes)
+                 : "memory");
 }
 
 // 2-D tiled TMA store of a shared-memory box (x = innermost coordinate).
@@ -328,7 +436,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(TcGemmParams p, 
         if (lane == 0) {
             const uint32_t idesc = tf32_idesc(kTcM, BN);
             int it = 0;
-            for (int64_t tile = tc_next_tile<BN>(p, blockIdx.x); tile < p.mtiles * p.ntiles;
+            for (int64_t tile = tc_next_tile<BN>(p, blockIdx.x); tile < tc_total_tiles<BN>(p);
                  tile = tc_next_tile<BN>(p, tile + gridDim.x), ++it) {
                 if (*abort_flag) break;
                 const int b = it & 1;
@@ -340,12 +448,19 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(TcGemmParams p, 
                     *abort_flag = 1;
                     break;
                 }
-                const int64_t mt = tile / p.ntiles, nt = tile % p.ntiles;
+                int64_t a_row, b_row; // first image rows of the tile (group-major: row r starts at float r * kp)
+                if (p.mode == kTcTable) {
+                    a_row = p.table[tile * kTcTileWords + 0];
+                    b_row = p.table[tile * kTcTileWords + 1];
+                } else {
+                    a_row = (tile / p.ntiles) * kTcM;
+                    b_row = (tile % p.ntiles) * BN;
+                }
                 mbar_expect_tx(bar_full, 2 * a_bytes + 2 * b_bytes);
-                bulk_g2s(s_ahi, p.a_hi + mt * (int64_t)kTcM * p.kp, a_bytes, bar_full);
-                bulk_g2s(s_alo, p.a_lo + mt * (int64_t)kTcM * p.kp, a_bytes, bar_full);
-                bulk_g2s(s_bhi, p.b_hi + nt * (int64_t)BN * p.kp, b_bytes, bar_full);
-                bulk_g2s(s_blo, p.b_lo + nt * (int64_t)BN * p.kp, b_bytes, bar_full);
+                bulk_g2s(s_ahi, p.a_hi + a_row * p.kp, a_bytes, bar_full);
+                bulk_g2s(s_alo, p.a_lo + a_row * p.kp, a_bytes, bar_full);
+                bulk_g2s(s_bhi, p.b_hi + b_row * p.kp, b_bytes, bar_full);
+                bulk_g2s(s_blo, p.b_lo + b_row * p.kp, b_bytes, bar_full);
                 if (!mbar_wait(bar_full, it & 1)) {
                     atomicOr(p.err, 1u);
                     *abort_flag = 1;
@@ -355,12 +470,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(TcGemmParams p, 
                 tc_fence_after();
                 const uint32_t d = tmem + (uint32_t)(b * BN);
                 // K step ks covers K chunks 2ks and 2ks+1 (8 TF32 values); small terms first
+                const uint32_t sbo = (uint32_t)p.kp * 32; // bytes between 8-row groups
                 for (int ks = 0; ks < p.kp / 8; ++ks) {
-                    const uint32_t ao = (uint32_t)ks * 2 * kTcM * 16, bo = (uint32_t)ks * 2 * BN * 16;
-                    const uint64_t ahi = smem_desc(s_ahi + ao, kTcM * 16, 128);
-                    const uint64_t alo = smem_desc(s_alo + ao, kTcM * 16, 128);
-                    const uint64_t bhi = smem_desc(s_bhi + bo, BN * 16, 128);
-                    const uint64_t blo = smem_desc(s_blo + bo, BN * 16, 128);
+                    const uint32_t ko = (uint32_t)ks * 256; // two 128-byte K chunks per step
+                    const uint64_t ahi = smem_desc(s_ahi + ko, 128, sbo);
+                    const uint64_t alo = smem_desc(s_alo + ko, 128, sbo);
+                    const uint64_t bhi = smem_desc(s_bhi + ko, 128, sbo);
+                    const uint64_t blo = smem_desc(s_blo + ko, 128, sbo);
                     mma_tf32(d, alo, bhi, idesc, ks > 0 ? 1u : 0u);
                     mma_tf32(d, ahi, blo, idesc, 1u);
                     mma_tf32(d, ahi, bhi, idesc, 1u);
@@ -377,7 +493,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(TcGemmParams p, 
         float *staging = reinterpret_cast<float *>(smem + L.staging);
         int ctr = 0; // chunks stored by this half (selects the staging buffer)
         int it = 0;
-        for (int64_t tile = tc_next_tile<BN>(p, blockIdx.x); tile < p.mtiles * p.ntiles;
+        for (int64_t tile = tc_next_tile<BN>(p, blockIdx.x); tile < tc_total_tiles<BN>(p);
              tile = tc_next_tile<BN>(p, tile + gridDim.x), ++it) {
             const int b = it & 1;
             bool ok = !*abort_flag && mbar_wait(bar_mma0 + 8 * b, (it >> 1) & 1);
@@ -394,6 +510,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(TcGemmParams p, 
             tc_fence_after();
             const int64_t mt = tile / p.ntiles, nt = tile % p.ntiles;
             const int64_t m = mt * kTcM + quarter * 32 + lane;
+            const int64_t *te = p.mode == kTcTable ? p.table + tile * kTcTileWords : nullptr;
             for (int c = 0; c < BN / 64; ++c, ++ctr) {
                 const int col = half * (BN / 2) + c * 32;
                 float v[32];
@@ -408,7 +525,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(TcGemmParams p, 
                     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                     named_bar(1 + half, 128); // buf complete
                     if (leader) {
-                        tma_store_2d(&out_map, smem_u32(buf), (int)(mt * kTcM), (int)n0);
+                        if (te) { // one bulk copy per valid column: rows 0 .. m_valid (rounded up to 4)
+                            const int64_t nv = te[3] - col;
+                            const uint32_t seg = (uint32_t)(((te[2] + 3) & ~3LL) * 4);
+                            for (int j = 0; j < 32 && j < nv; ++j)
+                                bulk_s2g(p.out + te[4] + (col + j) * te[5], smem_u32(buf + j * kTcM), seg);
+                        } else {
+                            tma_store_2d(&out_map, smem_u32(buf), (int)(mt * kTcM), (int)n0);
+                        }
                         asm volatile("cp.async.bulk.commit_group;" ::: "memory");
                     }
                 } else {
@@ -531,17 +655,6 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_inc_kernel(StreamI
     int q = 0, k = 0;
     int64_t item = 0, xi = 0, yj = 0;
     const float *base = p.inc;
-    // The lane's increments for its next active step are loaded one step
-    // ahead (software pipelining across the memory latency).
-    float pre[RC];
-    bool have_pre = false;
-    auto pair_base = [&](int64_t it) -> const float * {
-        int64_t a, b2;
-        stream_decode(sp, it, a, b2);
-        return p.op == kOpPairwise ? p.inc + (it - p.item0) * (int64_t)ncy * p.rows_x
-                                   : p.inc + b2 * (int64_t)ncy * p.ld + (a - p.x0) * p.rows_x;
-    };
-
     const int total = cnt * nsteps + 31;
     for (int s = 0; s < total; ++s) {
         T top[C];
@@ -555,33 +668,16 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_inc_kernel(StreamI
             if (q == 0) {
                 item = p.item0 + first + k;
                 stream_decode(sp, item, xi, yj);
-                base = pair_base(item);
+                base = p.op == kOpPairwise ? p.inc + (item - p.item0) * (int64_t)ncy * p.rows_x
+                                           : p.inc + yj * (int64_t)ncy * p.ld + (xi - p.x0) * p.rows_x;
 #pragma unroll
                 for (int r = 0; r < R; ++r) left[r] = T(1);
             }
             const T corner = (q == 0) ? T(1) : corner_next;
             corner_next = top[C - 1];
+            const int cj = (O <= 3) ? q : ((q * C) >> p.order);
             float cur[RC];
-            if (have_pre) {
-#pragma unroll
-                for (int rc = 0; rc < RC; ++rc) cur[rc] = pre[rc];
-            } else {
-                const int cj = (O <= 3) ? q : ((q * C) >> p.order);
-                load_incs<float, RC>(base + (int64_t)cj * row_ld, ci0, ncx, cur);
-            }
-            { // prefetch the next step's increments
-                int q2 = q + 1, k2 = k;
-                if (q2 == nsteps) {
-                    q2 = 0;
-                    ++k2;
-                }
-                have_pre = k2 < cnt;
-                if (have_pre) {
-                    const float *b2 = (q2 == 0) ? pair_base(p.item0 + first + k2) : base;
-                    const int cj2 = (O <= 3) ? q2 : ((q2 * C) >> p.order);
-                    load_incs<float, RC>(b2 + (int64_t)cj2 * row_ld, ci0, ncx, pre);
-                }
-            }
+            load_incs<float, RC>(base + (int64_t)cj * row_ld, ci0, ncx, cur);
             T A[RC], B[RC];
 #pragma unroll
             for (int rc = 0; rc < RC; ++rc) stencil_coefs(T(cur[rc]), A[rc], B[rc]);

@@ -62,6 +62,34 @@ def rows_per_lane(n, d, order, tsize):
     return R
 
 
+def tc_plan(x_lengths, y_lengths, tile_m=128, tile_n=256):
+    """Tensor-core plan of a ragged batch (sigk_ragged_tc_plan in include/sigk.h):
+    operand-image rows and increment-block offsets per pair, and the GEMM tiles."""
+    import numpy as np
+    lx = np.asarray(x_lengths, np.int64)
+    ly = np.asarray(y_lengths, np.int64)
+    rows = np.minimum(lx, ly) - 1       # the row path is the shorter one
+    cols = np.maximum(lx, ly) - 1
+    r8 = (rows + 7) // 8 * 8
+    c8 = (cols + 7) // 8 * 8
+    ld = (rows + 3) // 4 * 4
+    a_row0 = np.zeros_like(rows)
+    a_row0[1:] = np.cumsum(r8)[:-1]
+    b_row0 = np.zeros_like(cols)
+    b_row0[1:] = np.cumsum(c8)[:-1]
+    blk = cols * ld
+    inc_off = np.zeros_like(blk)
+    inc_off[1:] = np.cumsum(blk)[:-1]
+    tiles = []
+    for b in np.argsort(-(rows * cols).astype(np.float64), kind="stable"):
+        for i in range(int((rows[b] + tile_m - 1) // tile_m)):
+            for j in range(int((cols[b] + tile_n - 1) // tile_n)):
+                tiles.append((a_row0[b] + tile_m * i, b_row0[b] + tile_n * j, min(tile_m, rows[b] - tile_m * i),
+                              min(tile_n, cols[b] - tile_n * j), inc_off[b] + tile_n * j * ld[b] + tile_m * i, ld[b]))
+    return {"a_row0": a_row0, "b_row0": b_row0, "a_rows": int(r8.sum()) + tile_m, "b_rows": int(c8.sum()) + tile_n,
+            "inc_off": inc_off, "inc_elems": int(blk.sum()), "tiles": np.asarray(tiles, np.int64).reshape(-1, 6)}
+
+
 def plan(x_lengths, y_lengths, orders, dim, tsize):
     """Band plan of a ragged batch (see sigk_pairwise_ragged in include/sigk.h)."""
     import numpy as np
@@ -116,7 +144,7 @@ class RaggedPairwise:
         self.x_len, self.y_len = xl.to(self.device), yl.to(self.device)
         self.x_off, self.y_off = xo.to(self.device), yo.to(self.device)
         self.order = od.to(self.device)
-        pl = plan(x_lengths, y_lengths, orders, self.dim, 8 if precision == "fp64" else 4)
+        pl = plan(x_lengths, y_lengths, orders, self.dim, 8 if precision in ("fp64", "tc64") else 4)
         self.item_pair = torch.as_tensor(pl["item_pair"], device=self.device)
         self.item_band = torch.as_tensor(pl["item_band"], dtype=torch.int32, device=self.device)
         self.pair_rows = torch.as_tensor(pl["rows"], dtype=torch.int32, device=self.device)
@@ -129,8 +157,19 @@ class RaggedPairwise:
         self.out = torch.empty(self.n, dtype=dtype, device=self.device)
         self.x_points = int(xl.sum())
         self.y_points = int(yl.sum())
-        nws = _lib.lib().sigk_ragged_workspace_size(self.n, self.x_points, self.y_points, self.dim, self.nitems,
-                                                    self.bnd_elems, self.prec)
+        self.tc = None
+        if precision in ("tc32", "tc64") and self.dim <= 32:
+            tp = tc_plan(x_lengths, y_lengths)
+            self._tc_arrays = {k: torch.as_tensor(tp[k], device=self.device)
+                               for k in ("a_row0", "b_row0", "inc_off", "tiles")}
+            self.tc = _lib.RaggedTcPlan(_ptr(self._tc_arrays["a_row0"]), _ptr(self._tc_arrays["b_row0"]), tp["a_rows"],
+                                        tp["b_rows"], _ptr(self._tc_arrays["inc_off"]), tp["inc_elems"],
+                                        _ptr(self._tc_arrays["tiles"]), int(tp["tiles"].shape[0]))
+            nws = _lib.lib().sigk_ragged_tc_workspace_size(self.n, self.dim, self.nitems, self.bnd_elems, self.prec,
+                                                           self.tc)
+        else:
+            nws = _lib.lib().sigk_ragged_workspace_size(self.n, self.x_points, self.y_points, self.dim, self.nitems,
+                                                        self.bnd_elems, self.prec)
         self.ws = torch.empty(nws, dtype=torch.uint8, device=self.device)
         self.x_scale = None
         self.y_scale = None
@@ -140,16 +179,29 @@ class RaggedPairwise:
         """Copy new path values (same shapes) into the packed buffers."""
         torch.cat([p.to(self.device, self.dtype) for p in x_paths], 0, out=self.x_pack)
         torch.cat([p.to(self.device, self.dtype) for p in y_paths], 0, out=self.y_pack)
-        self.x_scale = None if x_scale is None else torch.as_tensor(x_scale, dtype=self.dtype, device=self.device)
-        self.y_scale = None if y_scale is None else torch.as_tensor(y_scale, dtype=self.dtype, device=self.device)
+        self.x_scale = self._scale_buffer(self.x_scale, x_scale)
+        self.y_scale = self._scale_buffer(self.y_scale, y_scale)
+
+    def _scale_buffer(self, buf, values):
+        # new values go into the existing buffer, so a captured graph keeps reading the right memory
+        if values is None:
+            return None
+        v = torch.as_tensor(values, dtype=self.dtype, device=self.device).reshape(-1)
+        if buf is not None and buf.shape == v.shape:
+            buf.copy_(v)
+            return buf
+        return v.clone()
 
     def _launch(self):
-        _lib.call("sigk_pairwise_ragged", _ptr(self.x_pack), _ptr(self.x_off), _ptr(self.x_len), self.x_points,
-                  _ptr(self.y_pack), _ptr(self.y_off), _ptr(self.y_len), self.y_points, _ptr(self.order),
-                  _ptr(self.item_pair), _ptr(self.item_band), self.nitems, _ptr(self.pair_rows),
-                  _ptr(self.pair_bands), _ptr(self.pair_bnd_off), self.bnd_elems, self.n, self.dim,
-                  _dtype_code(self.x_pack), self.static_scale, _ptr(self.x_scale), _ptr(self.y_scale),
-                  _ptr(self.out), self.prec, _ptr(self.ws), self.ws.numel(), _stream())
+        args = (_ptr(self.x_pack), _ptr(self.x_off), _ptr(self.x_len), self.x_points, _ptr(self.y_pack),
+                _ptr(self.y_off), _ptr(self.y_len), self.y_points, _ptr(self.order), _ptr(self.item_pair),
+                _ptr(self.item_band), self.nitems, _ptr(self.pair_rows), _ptr(self.pair_bands),
+                _ptr(self.pair_bnd_off), self.bnd_elems, self.n, self.dim, _dtype_code(self.x_pack),
+                self.static_scale, _ptr(self.x_scale), _ptr(self.y_scale), _ptr(self.out), self.prec)
+        if self.tc is not None:
+            _lib.call("sigk_pairwise_ragged_tc", *args, self.tc, _ptr(self.ws), self.ws.numel(), _stream())
+        else:
+            _lib.call("sigk_pairwise_ragged", *args, _ptr(self.ws), self.ws.numel(), _stream())
 
     def capture(self):
         """Capture the launch (counter reset + kernel) in a CUDA graph; later

@@ -55,6 +55,50 @@ def test_ragged_matches_oracle(sig, oracle, dtype):
     assert _rel(got, want) <= tol
 
 
+def _cs_err(oracle, X, Y, orders, got, sx=None, sy=None):
+    want = _want(oracle, X, Y, orders, sx, sy)
+    kxx = _want(oracle, X, X, orders, sx, sx)
+    kyy = _want(oracle, Y, Y, orders, sy, sy)
+    return float(np.max(np.abs(got - want) / np.sqrt(np.abs(kxx * kyy))))
+
+
+@pytest.mark.parametrize("prec", ["tc64", "tc32"])
+def test_ragged_tensor_core_increments(sig, oracle, prec):
+    """Increments from the grouped split-TF32 GEMM (tensor-core plan): CS-normalised
+    error <= 1e-5 with float64 cells, <= 4x the fp32-cell mode's own error with
+    float32 cells; the float64-cell run is also checked against fp64 mode."""
+    specs = SPECS + [(200, 300, 32, 1), (64, 64, 17, 3)]
+    for d in (4, 32, 17):
+        sp = [(a, b, d, o) for (a, b, _, o) in specs]
+        X, Y = _batch(oracle, sp, 11 + d, torch.float64)
+        orders = [s[3] for s in sp]
+        got = sig.ragged.pairwise(X, Y, orders, precision=prec).cpu().numpy()
+        err = _cs_err(oracle, X, Y, orders, got)
+        if prec == "tc64":
+            assert err <= 1e-5, err
+        else:
+            ref = sig.ragged.pairwise(X, Y, orders, precision="fp32").cpu().numpy()
+            assert err <= 4 * _cs_err(oracle, X, Y, orders, ref) + 1e-7, err
+
+
+def test_ragged_tensor_core_graph_replay_and_scales(sig, oracle):
+    specs = [(30 + 11 * i, 25 + 5 * i, 8, (i % 3) + 1) for i in range(20)] + [(600, 90, 8, 1)]
+    orders = [s[3] for s in specs]
+    solver = sig.ragged.RaggedPairwise([s[0] for s in specs], [s[1] for s in specs], orders, 8,
+                                       dtype=torch.float32, device="cuda", precision="tc64")
+    assert solver.tc is not None
+    sx = np.linspace(0.5, 1.5, len(specs))
+    sy = np.linspace(1.4, 0.6, len(specs))
+    for seed in (4, 5):
+        X, Y = _batch(oracle, specs, seed, torch.float32)
+        solver.load(X, Y, sx, sy)
+        if seed == 4:
+            solver.capture()
+        got = solver.solve().double().cpu().numpy()
+        assert _cs_err(oracle, X, Y, orders, got, sx, sy) <= 1e-5
+        assert solver.error_flag() == 0
+
+
 def test_ragged_scales_and_dimension(sig, oracle):
     specs = [(20 + 7 * i, 60 - 3 * i, 32, i % 4) for i in range(12)]
     X, Y = _batch(oracle, specs, 2, torch.float64)
