@@ -207,6 +207,20 @@ def timed_steps(torch, step, K, W, flush_buf, barrier):
     return [s.elapsed_time(e) for s, e in evs]
 
 
+def max_over_ranks(torch, dist, world, value, device=None):
+    """The largest of every rank's `value` (every rank calls this, in the same order)."""
+    if world <= 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world, units_per_rank, steps, slowest_ms):
+    """Whole-job throughput of weak-scaled replicas: every rank's units over the slowest rank's time."""
+    return world * units_per_rank * steps / (slowest_ms * 1e-3)
+
+
 def percentile(v, q):
     v = sorted(v)
     if not v:
@@ -330,12 +344,8 @@ def run_ours(args, w):
     times = timed_steps(torch, lambda: k.gram(X, Y), args.steps, args.warmup, flush, barrier)
     launches = LAUNCHES["last"]
     clk = clocks.stop()
-    total_ms = sum(times)
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * entries * args.steps / (total_ms * 1e-3)
+    total_ms = max_over_ranks(torch, dist, world, sum(times), dev)
+    value = job_rate(world, entries, args.steps, total_ms)
 
     # end to end through the public API: pinned host paths -> device -> Gram -> pinned host result
     Xh = X.cpu().pin_memory()
@@ -348,12 +358,8 @@ def run_ours(args, w):
         Rh.copy_(k.gram(Xd, Yd), non_blocking=True)
 
     e2e_times = timed_steps(torch, e2e_step, args.steps, args.warmup, flush, barrier)
-    e2e_ms = sum(e2e_times)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * entries * args.steps / (e2e_ms * 1e-3)
+    e2e_ms = max_over_ranks(torch, dist, world, sum(e2e_times), dev)
+    e2e_value = job_rate(world, entries, args.steps, e2e_ms)
 
     line = None
     if rank == 0:

@@ -88,10 +88,19 @@ struct RaggedParams {
 };
 
 // Increments read from a precomputed float matrix: c[rc] = m[cj * ld + ci0 + rc].
+// Each read also asks the L2 for the lane's rows kIncPrefetch columns ahead,
+// so the wavefront's loads find them there instead of waiting on HBM.
+constexpr int kIncPrefetch = 8;
+
+__device__ __forceinline__ void prefetch_l2(const void *p)
+{
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 template <typename T, int RC>
 struct MatIncs {
     const float *base;
-    int64_t ld;
+    int64_t ld, ncy;
     int ci0 = 0, ncx = 0;
     __device__ __forceinline__ void stage(int64_t ci0_, int64_t ncx_, int, bool)
     {
@@ -101,6 +110,7 @@ struct MatIncs {
     __device__ __forceinline__ void column(int64_t cj, int, T (&c)[RC]) const
     {
         const float *row = base + cj * ld;
+        if (cj + kIncPrefetch < ncy && ci0 < ncx) prefetch_l2(row + kIncPrefetch * ld + ci0);
         if constexpr (RC == 1) {
             c[0] = ci0 < ncx ? T(row[ci0]) : T(0);
         } else if constexpr (RC == 2) {
@@ -264,6 +274,7 @@ __device__ T ragged_band(const BandSource &bs, int64_t ncx, int64_t ncy, int ord
         MatIncs<T, BS::RC> src;
         src.base = bs.mat;
         src.ld = bs.ld;
+        src.ncy = ncy;
         return band_solve<T, R, O>(g, src, band, last, top_buf, top_prog, bot_buf, bot_prog, error);
     } else {
         DeltaIncs<T, BS::RC> src;

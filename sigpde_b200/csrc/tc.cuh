@@ -30,6 +30,7 @@
 
 #include <cuda.h> // CUtensorMap
 
+#include "ragged.cuh"
 #include "stream.cuh"
 
 namespace sigk {
@@ -489,7 +490,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(TcGemmParams p, 
     } else {
         // ---------------------------------------------------------- epilogue: TMEM -> HBM
         const int quarter = warp & 3, half = warp >> 2;
-        const bool leader = quarter == 0 && lane == 0; // issues this half's TMA stores
+        const bool leader = quarter == 0 && lane == 0; // issues this half's TMA tensor stores
+        // threads that issue bulk stores (and so wait on their groups): the leader, or with a tile table
+        // every lane of the half's first warp (one column each)
+        const bool issuer = p.mode == kTcTable ? quarter == 0 : leader;
         float *staging = reinterpret_cast<float *>(smem + L.staging);
         int ctr = 0; // chunks stored by this half (selects the staging buffer)
         int it = 0;
@@ -511,28 +515,38 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(TcGemmParams p, 
             const int64_t mt = tile / p.ntiles, nt = tile % p.ntiles;
             const int64_t m = mt * kTcM + quarter * 32 + lane;
             const int64_t *te = p.mode == kTcTable ? p.table + tile * kTcTileWords : nullptr;
-            for (int c = 0; c < BN / 64; ++c, ++ctr) {
+            for (int c = 0; c < BN / 64; ++c) {
                 const int col = half * (BN / 2) + c * 32;
+                if (te && col >= te[3]) continue; // no valid column in this chunk (the same for the whole half)
+                // table tiles: a lane quarter without valid rows skips its TMEM load (the warp still
+                // takes part in the half's barriers)
+                const bool rows_here = !te || quarter * 32 < te[2];
                 float v[32];
-                tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * BN + col), v);
+                if (rows_here) tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * BN + col), v);
                 const int64_t n0 = nt * BN + col;
                 if (p.mode != kTcDiag) {
                     float *buf = staging + (size_t)(half * 2 + (ctr & 1)) * (kTcStageCols * kTcM);
-                    if (leader) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+                    ++ctr;
+                    if (issuer) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
                     named_bar(1 + half, 128); // buf is no longer read by an earlier store
+                    if (rows_here) {
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) buf[j * kTcM + quarter * 32 + lane] = v[j];
+                        for (int j = 0; j < 32; ++j) buf[j * kTcM + quarter * 32 + lane] = v[j];
+                    }
                     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                     named_bar(1 + half, 128); // buf complete
-                    if (leader) {
-                        if (te) { // one bulk copy per valid column: rows 0 .. m_valid (rounded up to 4)
-                            const int64_t nv = te[3] - col;
-                            const uint32_t seg = (uint32_t)(((te[2] + 3) & ~3LL) * 4);
-                            for (int j = 0; j < 32 && j < nv; ++j)
-                                bulk_s2g(p.out + te[4] + (col + j) * te[5], smem_u32(buf + j * kTcM), seg);
-                        } else {
-                            tma_store_2d(&out_map, smem_u32(buf), (int)(mt * kTcM), (int)n0);
+                    if (te) {
+                        // one bulk copy per valid column, issued by lane j of the half's first warp:
+                        // rows 0 .. m_valid rounded up to 4 (the pair's own zero padding)
+                        if (quarter == 0) {
+                            if (lane < te[3] - col) {
+                                const uint32_t seg = (uint32_t)(((te[2] + 3) & ~3LL) * 4);
+                                bulk_s2g(p.out + te[4] + (col + lane) * te[5], smem_u32(buf + lane * kTcM), seg);
+                            }
+                            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
                         }
+                    } else if (leader) {
+                        tma_store_2d(&out_map, smem_u32(buf), (int)(mt * kTcM), (int)n0);
                         asm volatile("cp.async.bulk.commit_group;" ::: "memory");
                     }
                 } else {
@@ -550,7 +564,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(TcGemmParams p, 
             __syncwarp();
             if (lane == 0) mbar_arrive(bar_empty0 + 8 * b);
         }
-        if (leader) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+        if (issuer) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
     }
     __syncthreads();
     if (warp == kTcEpiWarps) {
