@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "tc32", "tc64"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target length of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--autotune", action="store_true", help="uneven batches: measure rows per lane per bucket "
+                    "before timing (sigpde_b200.torch.autotune)")
     ap.add_argument("--burst", action="store_true", help="serving traces: every request arrives at t=0 "
                     "(saturated throughput) instead of Poisson arrivals")
     return ap.parse_args()
@@ -574,7 +576,16 @@ def run_ours_ragged(args, w):
     cells = ragged_cells(lx, ly, orders)
     X = [torch.tensor(a, dtype=torch.float32, device=dev) for a in xs]
     Y = [torch.tensor(a, dtype=torch.float32, device=dev) for a in ys]
-    solver = sig.ragged.RaggedPairwise(lx, ly, orders, w["d"], torch.float32, dev, args.precision)
+    tuning = None
+    tuner = None
+    if args.autotune:  # rows per lane (bands per pair) measured per bucket, before and outside the timed region
+        import time as _time
+        t0 = _time.perf_counter()
+        tuner = sig.autotune.RaggedTuner(w["d"], args.precision, torch.float32, dev)
+        tuner.tune_for(lx, ly, orders)
+        tuning = {"seconds": _time.perf_counter() - t0,
+                  "rows_per_lane": {f"n<=2^{k[0]},o={k[1]}": r for k, r in sorted(tuner.table.items())}}
+    solver = sig.ragged.RaggedPairwise(lx, ly, orders, w["d"], torch.float32, dev, args.precision, tuner=tuner)
     solver.load(X, Y)
     solver.capture()
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
@@ -624,6 +635,8 @@ def run_ours_ragged(args, w):
                 "d2h_bytes_per_step": oh.numel() * oh.element_size(), "ms_per_step": statistics.mean(e2e_times)},
         "gpu_launches": launches, "clocks": clk, "lib": _lib.version(),
     }
+    if tuning is not None:
+        line["autotune"] = tuning
     if cpu is not None:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)

@@ -4,8 +4,8 @@
     k = sig.SigPDE(sig.kernels.LinearKernel(), dyadic_order=2)
     k.gram(x, y)
 """
-from . import ragged
+from . import autotune, ragged
 from . import static_kernels as kernels
 from .kernel import RobustSigPDE, SigPDE, gram_inner_product, log_normalizer, pairwise_inner_product
 
-__all__ = ["SigPDE", "RobustSigPDE", "kernels", "ragged", "log_normalizer", "pairwise_inner_product", "gram_inner_product"]
+__all__ = ["SigPDE", "RobustSigPDE", "kernels", "ragged", "autotune", "log_normalizer", "pairwise_inner_product", "gram_inner_product"]

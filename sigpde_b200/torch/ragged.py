@@ -48,11 +48,14 @@ def pack(paths, dtype=None, device=None):
 STAGE_BYTES_PER_WARP = 16 * 1024  # the kernel's dx staging budget per warp
 
 
-def rows_per_lane(n, d, order, tsize):
+def rows_per_lane(n, d, order, tsize, staged=True):
     """Rows per lane R for a pair with n refined rows: the smallest of 2, 4, 8,
-    16 covering the rows in one band of 32 R, shrunk while the lane's dx tile
-    (coarse rows per lane x d) does not fit the kernel's staging budget."""
+    16 covering the rows in one band of 32 R; with `staged` (increments formed
+    from staged differences) shrunk while the lane's dx tile (coarse rows per
+    lane x d) does not fit the kernel's staging budget."""
     R = 2 if n <= 64 else 4 if n <= 128 else 8 if n <= 256 else 16
+    if not staged:
+        return R
     cap = STAGE_BYTES_PER_WARP // tsize
     while R > 2:
         rc = 1 if order >= 4 else max(R >> order, 1)
@@ -60,6 +63,12 @@ def rows_per_lane(n, d, order, tsize):
             break
         R >>= 1
     return R
+
+
+def staging_fits(R, d, order, tsize):
+    """Whether the lane's dx tile of rows-per-lane R fits the staging budget."""
+    rc = 1 if order >= 4 else max(R >> order, 1)
+    return rc * d * 32 <= STAGE_BYTES_PER_WARP // tsize
 
 
 def tc_plan(x_lengths, y_lengths, tile_m=128, tile_n=256):
@@ -90,15 +99,18 @@ def tc_plan(x_lengths, y_lengths, tile_m=128, tile_n=256):
             "inc_off": inc_off, "inc_elems": int(blk.sum()), "tiles": np.asarray(tiles, np.int64).reshape(-1, 6)}
 
 
-def plan(x_lengths, y_lengths, orders, dim, tsize):
-    """Band plan of a ragged batch (see sigk_pairwise_ragged in include/sigk.h)."""
+def plan(x_lengths, y_lengths, orders, dim, tsize, staged=True, rows_fn=None):
+    """Band plan of a ragged batch (see sigk_pairwise_ragged in include/sigk.h).
+    `staged`: increments are formed from staged differences (CUDA-core modes);
+    `rows_fn(n, order)`: rows per lane chosen elsewhere (the autotuner), or None."""
     import numpy as np
     lx = np.asarray(x_lengths, np.int64)
     ly = np.asarray(y_lengths, np.int64)
     od = np.asarray(orders, np.int64)
     n = (np.minimum(lx, ly) - 1) << od
     m = (np.maximum(lx, ly) - 1) << od
-    rows = np.array([rows_per_lane(int(a), dim, int(o), tsize) for a, o in zip(n, od)], np.int64)
+    pick = rows_fn if rows_fn is not None else (lambda a, o: rows_per_lane(a, dim, o, tsize, staged))
+    rows = np.array([pick(int(a), int(o)) for a, o in zip(n, od)], np.int64)
     bands = (n + 32 * rows - 1) // (32 * rows)
     sizes = (bands - 1) * (m + 1)
     bnd_off = np.zeros_like(sizes)
@@ -113,10 +125,11 @@ def plan(x_lengths, y_lengths, orders, dim, tsize):
 class RaggedPairwise:
     """Solver for one ragged batch shape: packed inputs, work order and workspace
     are built once; `solve()` runs the launch (optionally replaying a captured
-    CUDA graph)."""
+    CUDA graph).  `tuner` (autotune.RaggedTuner) or `rows_fn(n, order)` choose
+    the rows per lane (hence bands) per pair instead of the default rule."""
 
     def __init__(self, x_lengths, y_lengths, orders, dim, dtype=torch.float32, device="cuda", precision="fp64",
-                 static_scale=1.0):
+                 static_scale=1.0, tuner=None, rows_fn=None):
         if precision not in _PREC:
             raise ValueError(f"precision must be one of {sorted(_PREC)}")
         x_lengths = [int(v) for v in x_lengths]
@@ -144,7 +157,12 @@ class RaggedPairwise:
         self.x_len, self.y_len = xl.to(self.device), yl.to(self.device)
         self.x_off, self.y_off = xo.to(self.device), yo.to(self.device)
         self.order = od.to(self.device)
-        pl = plan(x_lengths, y_lengths, orders, self.dim, 8 if precision in ("fp64", "tc64") else 4)
+        tsize = 8 if precision in ("fp64", "tc64") else 4
+        use_tc = precision in ("tc32", "tc64") and self.dim <= 32
+        if rows_fn is None and tuner is not None:  # rows per lane from measurements (autotune.py)
+            tuner.tune_for(x_lengths, y_lengths, orders)
+            rows_fn = tuner.rows_for
+        pl = plan(x_lengths, y_lengths, orders, self.dim, tsize, staged=not use_tc, rows_fn=rows_fn)
         self.item_pair = torch.as_tensor(pl["item_pair"], device=self.device)
         self.item_band = torch.as_tensor(pl["item_band"], dtype=torch.int32, device=self.device)
         self.pair_rows = torch.as_tensor(pl["rows"], dtype=torch.int32, device=self.device)
@@ -158,7 +176,7 @@ class RaggedPairwise:
         self.x_points = int(xl.sum())
         self.y_points = int(yl.sum())
         self.tc = None
-        if precision in ("tc32", "tc64") and self.dim <= 32:
+        if use_tc:
             tp = tc_plan(x_lengths, y_lengths)
             self._tc_arrays = {k: torch.as_tensor(tp[k], device=self.device)
                                for k in ("a_row0", "b_row0", "inc_off", "tiles")}
