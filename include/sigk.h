@@ -33,11 +33,11 @@
  *                   accumulate; ~1e-6 relative per increment), stored as a
  *                   float32 matrix in the workspace and read by the wavefront;
  *                   cells in float32 (TC32) or float64 (TC64).  Applies to
- *                   sigk_pairwise / sigk_gram / sigk_gram_sym when each pair
- *                   fits one band of rows ((len - 1) * 2^order <= 512) and
- *                   dim <= 32; other shapes, and the *_inc, ragged and
- *                   normalisation entry points, form increments on the CUDA
- *                   cores with the same cell precision.  The workspace holds
+ *                   sigk_pairwise / sigk_gram / sigk_gram_sym with dim <= 32
+ *                   and to sigk_pairwise_ragged_tc; larger dims, the *_inc,
+ *                   sigk_pairwise_ragged and normalisation entry points form
+ *                   increments on the CUDA cores with the same cell
+ *                   precision.  The workspace holds
  *                   the increment matrix: up to 6 GiB per call (the x paths
  *                   are processed in chunks beyond that; SIGK_TC_CHUNK_MB
  *                   sets the chunk size).

@@ -33,8 +33,9 @@ using DeltaFn = void (*)(const void *, int64_t, int64_t, int64_t, int64_t, doubl
 
 // f64cells: float64 cells (SIGK_PREC_FP64) vs float32; in64: float64 inputs;
 // R in {2,4,8,16} rows per lane; O = min(order, 4).
-PairFn get_pair_kernel_f64(bool in64, bool from_inc, int R, int O);
-PairFn get_pair_kernel_f32(bool in64, bool from_inc, int R, int O);
+// mode: kPairDelta (path differences), kPairGiven (caller's increments), kPairMat (increment matrix)
+PairFn get_pair_kernel_f64(bool in64, int mode, int R, int O);
+PairFn get_pair_kernel_f32(bool in64, int mode, int R, int O);
 // mode: kNormDelta, kNormGiven or kNormTile (sigk_kernels.cuh)
 NormFn get_norm_kernel(bool in64, int mode, int R, int O);
 // D: dimension padded to a power of two in {2,...,32}; returns null unless

@@ -4,7 +4,7 @@
 
 namespace sigk {
 namespace {
-template <typename TIN, int R, bool FI>
+template <typename TIN, int R, int FI>
 PairFn by_o(int O)
 {
     switch (O) {
@@ -15,7 +15,7 @@ PairFn by_o(int O)
     default: return pair_kernel<double, TIN, R, 4, FI>;
     }
 }
-template <typename TIN, bool FI>
+template <typename TIN, int FI>
 PairFn by_r(int R, int O)
 {
     switch (R) {
@@ -27,9 +27,13 @@ PairFn by_r(int R, int O)
 }
 } // namespace
 
-PairFn get_pair_kernel_f64(bool in64, bool from_inc, int R, int O)
+PairFn get_pair_kernel_f64(bool in64, int mode, int R, int O)
 {
-    if (in64) return from_inc ? by_r<double, true>(R, O) : by_r<double, false>(R, O);
-    return from_inc ? by_r<float, true>(R, O) : by_r<float, false>(R, O);
+    if (in64) {
+        if (mode == kPairMat) return by_r<double, kPairMat>(R, O);
+        return mode == kPairGiven ? by_r<double, kPairGiven>(R, O) : by_r<double, kPairDelta>(R, O);
+    }
+    if (mode == kPairMat) return by_r<float, kPairMat>(R, O);
+    return mode == kPairGiven ? by_r<float, kPairGiven>(R, O) : by_r<float, kPairDelta>(R, O);
 }
 } // namespace sigk

@@ -87,50 +87,6 @@ struct RaggedParams {
     const unsigned *tc_err;     // non-zero: the GEMM skipped a tile, the matrix is incomplete
 };
 
-// Increments read from a precomputed float matrix: c[rc] = m[cj * ld + ci0 + rc].
-// Each read also asks the L2 for the lane's rows kIncPrefetch columns ahead,
-// so the wavefront's loads find them there instead of waiting on HBM.
-constexpr int kIncPrefetch = 8;
-
-__device__ __forceinline__ void prefetch_l2(const void *p)
-{
-    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
-}
-
-template <typename T, int RC>
-struct MatIncs {
-    const float *base;
-    int64_t ld, ncy;
-    int ci0 = 0, ncx = 0;
-    __device__ __forceinline__ void stage(int64_t ci0_, int64_t ncx_, int, bool)
-    {
-        ci0 = (int)ci0_;
-        ncx = (int)ncx_;
-    }
-    __device__ __forceinline__ void column(int64_t cj, int, T (&c)[RC]) const
-    {
-        const float *row = base + cj * ld;
-        if (cj + kIncPrefetch < ncy && ci0 < ncx) prefetch_l2(row + kIncPrefetch * ld + ci0);
-        if constexpr (RC == 1) {
-            c[0] = ci0 < ncx ? T(row[ci0]) : T(0);
-        } else if constexpr (RC == 2) {
-            const float2 v = ci0 < ncx ? *reinterpret_cast<const float2 *>(row + ci0) : make_float2(0.f, 0.f);
-            c[0] = T(v.x);
-            c[1] = T(v.y);
-        } else {
-#pragma unroll
-            for (int q = 0; q < RC / 4; ++q) {
-                const float4 v = (ci0 + 4 * q < ncx) ? *reinterpret_cast<const float4 *>(row + ci0 + 4 * q)
-                                                     : make_float4(0.f, 0.f, 0.f, 0.f);
-                c[4 * q + 0] = T(v.x);
-                c[4 * q + 1] = T(v.y);
-                c[4 * q + 2] = T(v.z);
-                c[4 * q + 3] = T(v.w);
-            }
-        }
-    }
-};
-
 constexpr long long kProgressPollLimit = 1ll << 26; // ~4 s with 64 ns sleeps
 constexpr int kProgressStride = 16;                 // column blocks between publications
 

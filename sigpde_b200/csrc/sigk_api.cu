@@ -158,14 +158,20 @@ Plan make_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, int64_t
         pl.bnd_off = 0;
         pl.ws_bytes = (size_t)warp_cap() * (size_t)pl.bnd_stride * tsize;
     }
+    if (!from_inc && op != SIGK_OP_NORMALIZE) {
+        // the per-pair kernel reads precomputed, scaled, dimension-major differences (delta_kernel)
+        pl.dx_off = align256(pl.ws_bytes);
+        pl.dy_off = pl.dx_off + align256((size_t)nx * ncx * d * tsize);
+        pl.ws_bytes = pl.dy_off + align256((size_t)ny * ncy * d * tsize);
+    }
     return pl;
 }
 
-PairFn pick_pair(int precision, int dtype, bool from_inc, int R, int O)
+PairFn pick_pair(int precision, int dtype, int mode, int R, int O)
 {
     const bool in64 = (dtype == SIGK_F64);
-    return (precision == SIGK_PREC_FP64 || precision == SIGK_PREC_TC64) ? get_pair_kernel_f64(in64, from_inc, R, O)
-                                       : get_pair_kernel_f32(in64, from_inc, R, O);
+    return (precision == SIGK_PREC_FP64 || precision == SIGK_PREC_TC64) ? get_pair_kernel_f64(in64, mode, R, O)
+                                                                         : get_pair_kernel_f32(in64, mode, R, O);
 }
 
 
@@ -299,7 +305,10 @@ constexpr size_t kTcChunkBytes = size_t(6) << 30;
 
 struct TcPlan {
     bool ok;
-    int R, O;
+    bool stream;              // streaming consumer (one band, >= 32 column blocks); else the per-pair kernel
+    int R, O, nbands;
+    int64_t bnd_stride;
+    size_t bnd_off;
     int kp;
     int64_t rows_x, rows_y;   // matrix rows per x path (ncx rounded up to 4) and per y path
     int64_t chunk, nchunks;   // x paths per chunk
@@ -318,16 +327,23 @@ size_t tc_chunk_cap()
     return kTcChunkBytes;
 }
 
-TcPlan make_tc_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, int64_t d, int order)
+TcPlan make_tc_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, int64_t d, int order, size_t tsize)
 {
     TcPlan t{};
     const int64_t n = ncx << order, m = ncy << order;
     const int C = order >= 4 ? 8 : (1 << order);
     const int Rs = pick_rows(n);
-    if (d > 32 || n > 32 * Rs || m / C < 32 || env_flag("SIGK_NO_TC")) return t;
+    if (d > 32 || env_flag("SIGK_NO_TC")) return t;
     t.ok = true;
+    t.stream = n <= 32 * Rs && m / C >= 32;
     t.R = Rs;
     t.O = order >= 4 ? 4 : order;
+    t.nbands = (int)((n + 32 * Rs - 1) / (32 * Rs));
+    size_t bnd_bytes = 0;
+    if (!t.stream && t.nbands > 1) { // one boundary row per warp of the per-pair kernel
+        t.bnd_stride = ((m + 1 + 31) / 32) * 32;
+        bnd_bytes = align256((size_t)warp_cap() * (size_t)t.bnd_stride * tsize);
+    }
     t.kp = (int)((d + 7) / 8 * 8);
     t.rows_x = (ncx + 3) / 4 * 4;
     t.rows_y = ncy;
@@ -344,7 +360,8 @@ TcPlan make_tc_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, in
     t.a_bytes = align256((size_t)t.a_tiles * kTcM * t.kp * sizeof(float));
     t.b_bytes = align256((size_t)t.b_tiles * kTcBN * t.kp * sizeof(float));
     t.err_off = 0;
-    t.a_off = 256;
+    t.bnd_off = 256;
+    t.a_off = t.bnd_off + bnd_bytes;
     t.b_off = t.a_off + 2 * t.a_bytes;
     t.ct_off = t.b_off + 2 * t.b_bytes;
     t.ws_bytes = t.ct_off + align256((size_t)chunk * per_x);
@@ -474,9 +491,10 @@ int run_pairs_tc(const TcPlan &t, int op, const void *x, const void *y, int64_t 
             return st;
     }
     const bool f64 = cell_prec(precision) == SIGK_PREC_FP64;
-    StreamIncFn fn = get_stream_inc_kernel(f64, t.R, t.O);
+    StreamIncFn fn = t.stream ? get_stream_inc_kernel(f64, t.R, t.O) : nullptr;
+    PairFn pfn = t.stream ? nullptr : pick_pair(precision, dtype, kPairMat, t.R, t.O);
     int nb = 0;
-    if ((st = blocks_per_sm((const void *)fn, 0, &nb))) return st;
+    if (fn && (st = blocks_per_sm((const void *)fn, 0, &nb))) return st;
     const int64_t warps = (int64_t)sm_count() * nb * kWarpsPerBlock;
 
     for (int64_t c = 0; c < t.nchunks; ++c) {
@@ -540,6 +558,30 @@ int run_pairs_tc(const TcPlan &t, int op, const void *x, const void *y, int64_t 
             sp.item0 = i0 * (i0 + 1) / 2;
             sp.nitems = i1 * (i1 + 1) / 2 - sp.item0;
         }
+        if (!t.stream) { // several bands or few column blocks: one pair per warp reading the matrix
+            PairParams p{};
+            p.op = op;
+            p.nx = nx;
+            p.ny = ny;
+            p.ncx = ncx;
+            p.ncy = ncy;
+            p.d = d;
+            p.order = order;
+            p.fscale = 1.0;
+            p.out = out;
+            p.out_ld = out_ld;
+            p.nitems = sp.nitems;
+            p.item0 = sp.item0;
+            p.mat = ct;
+            p.mat_err = err;
+            p.mat_ld = gp.ld;
+            p.mat_rows_x = t.rows_x;
+            p.x0 = i0;
+            p.bnd = t.nbands > 1 ? wsb + t.bnd_off : nullptr;
+            p.bnd_stride = t.bnd_stride;
+            if ((st = launch(pfn, p, p.nitems, 0, stream))) return st;
+            continue;
+        }
         int64_t nw = warps < sp.nitems ? warps : sp.nitems;
         sp.per_warp = (sp.nitems + nw - 1) / nw;
         const int64_t used = (sp.nitems + sp.per_warp - 1) / sp.per_warp;
@@ -567,7 +609,7 @@ int run_pairs(int op, const void *x, const void *y, int64_t nx, int64_t ny, int6
         (st = check_dev(sx, "scale_x", true)) || (st = check_dev(sy, "scale_y", true)))
         return st;
     if (is_tc(precision)) {
-        TcPlan t = make_tc_plan(op, nx, ny, lx - 1, ly - 1, d, order);
+        TcPlan t = make_tc_plan(op, nx, ny, lx - 1, ly - 1, d, order, tsize_of(precision));
         if (t.ok) {
             if (!ws || ws_bytes < t.ws_bytes)
                 return fail(SIGK_ENOMEM, "workspace of %zu bytes needed (got %zu)", t.ws_bytes, ws ? ws_bytes : 0);
@@ -584,13 +626,13 @@ int run_pairs(int op, const void *x, const void *y, int64_t nx, int64_t ny, int6
     const bool in64 = dtype == SIGK_F64;
     const bool f64 = precision == SIGK_PREC_FP64;
 
-    if (pl.stream) {
+    {
         unsigned char *wsb = reinterpret_cast<unsigned char *>(ws);
         void *dx = wsb + pl.dx_off;
         void *dy = wsb + pl.dy_off;
         DeltaFn delta = get_delta_kernel(f64, in64);
         const int nsm = sm_count();
-        const int64_t dp = pl.D ? pl.D : d;
+        const int64_t dp = pl.stream && pl.D ? pl.D : d;
         auto run_delta = [&](const void *src, int64_t npaths, int64_t len, double f, const void *sc,
                              void *dst) -> int {
             const int64_t total = npaths * (len - 1) * dp;
@@ -616,6 +658,30 @@ int run_pairs(int op, const void *x, const void *y, int64_t nx, int64_t ny, int6
         } else {
             if ((st = run_delta(x, nx, lx, fs, sx, dx))) return st;
             if ((st = run_delta(y, ny, ly, 1.0, sy, dy))) return st;
+        }
+
+        if (!pl.stream) { // one pair per warp, any number of bands
+            PairParams p{};
+            p.op = op;
+            p.x = x;
+            p.y = y;
+            p.dx = dx;
+            p.dy = dy;
+            p.nx = nx;
+            p.ny = ny;
+            p.ncx = lx - 1;
+            p.ncy = ly - 1;
+            p.d = d;
+            p.order = order;
+            p.fscale = 1.0; // folded into the differences
+            p.out = out;
+            p.out_ld = out_ld;
+            p.nitems = nitems;
+            p.bnd = pl.nbands > 1 ? ws : nullptr;
+            p.bnd_stride = pl.bnd_stride;
+            p.stage_smem = pl.stage_bytes_per_warp > 0;
+            PairFn fn = pick_pair(precision, dtype, kPairDelta, pl.R, pl.O);
+            return launch(fn, p, p.nitems, pl.stage_bytes_per_warp * kWarpsPerBlock, stream);
         }
 
         StreamParams sp{};
@@ -648,28 +714,6 @@ int run_pairs(int op, const void *x, const void *y, int64_t nx, int64_t ny, int6
         cudaError_t e = cudaGetLastError();
         return e == cudaSuccess ? SIGK_OK : cuda_fail(e, "stream kernel launch");
     }
-
-    PairParams p{};
-    p.op = op;
-    p.x = x;
-    p.y = y;
-    p.nx = nx;
-    p.ny = ny;
-    p.ncx = lx - 1;
-    p.ncy = ly - 1;
-    p.d = d;
-    p.order = order;
-    p.fscale = static_scale * std::ldexp(1.0, -2 * order);
-    p.sx = sx;
-    p.sy = sy;
-    p.out = out;
-    p.out_ld = out_ld;
-    p.nitems = nitems;
-    p.bnd = pl.nbands > 1 ? ws : nullptr;
-    p.bnd_stride = pl.bnd_stride;
-    p.stage_smem = pl.stage_bytes_per_warp > 0;
-    PairFn fn = pick_pair(precision, dtype, false, pl.R, pl.O);
-    return launch(fn, p, p.nitems, pl.stage_bytes_per_warp * kWarpsPerBlock, stream);
 }
 
 // Normalisation plan: the increment source (a shared-memory tile of the
@@ -735,7 +779,7 @@ size_t sigk_workspace_size(int op, int64_t n_x, int64_t n_y, int64_t len_x, int6
     if (op == SIGK_OP_PAIRWISE) n_y = n_x;
     if (op == SIGK_OP_NORMALIZE) return norm_plan(n_x, len_x - 1, dim > 0 ? dim : 1, order, dim == 0).ws_bytes;
     if (is_tc(precision) && dim > 0) {
-        TcPlan t = make_tc_plan(op, n_x, n_y, len_x - 1, len_y - 1, dim, order);
+        TcPlan t = make_tc_plan(op, n_x, n_y, len_x - 1, len_y - 1, dim, order, tsize_of(precision));
         if (t.ok) return t.ws_bytes;
     }
     // dim == 0 selects the plan of the *_inc entry points (no dx staging)
@@ -910,7 +954,7 @@ static int run_inc(int op, const void *inc, int64_t nx, int64_t ny, int64_t ncx,
     p.bnd = pl.nbands > 1 ? ws : nullptr;
     p.bnd_stride = pl.bnd_stride;
     p.stage_smem = 0;
-    PairFn fn = pick_pair(precision, dtype, true, pl.R, pl.O);
+    PairFn fn = pick_pair(precision, dtype, kPairGiven, pl.R, pl.O);
     return launch(fn, p, p.nitems, 0, stream);
 }
 

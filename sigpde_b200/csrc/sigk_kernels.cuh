@@ -29,8 +29,17 @@ struct PairParams {
     double fscale;      // static_scale * 4^-order (path mode) or 1 (increment mode)
     const void *sx;
     const void *sy;
+    const void *dx;     // path mode: scaled differences (nx, d, ncx) in T, dimension-major (delta_kernel)
+    const void *dy;     // (ny, d, ncy)
     const void *inc;    // increment mode only
     int64_t is0, is1, is2, is3;
+    // matrix mode (tensor-core increments, tc.cuh): pair (xi, yj)'s increments start at
+    // mat + yj * ncy * mat_ld + (xi - x0) * mat_rows_x (Gram ops; pairwise: mat + (item - item0) * ncy *
+    // mat_rows_x), mat_ld (pairwise: mat_rows_x) floats per coarse column
+    const float *mat;
+    const unsigned *mat_err; // non-zero: the GEMM gave up a wait, the matrix is incomplete (results NaN)
+    int64_t mat_ld, mat_rows_x, x0;
+    int64_t item0;      // first item of this launch (matrix mode works in chunks of x paths)
     void *out;
     int64_t out_ld;
     int64_t nitems;
@@ -55,7 +64,9 @@ __device__ __forceinline__ double scale_at(const void *s, int64_t i)
     return s ? (double)reinterpret_cast<const TIN *>(s)[i] : 1.0;
 }
 
-template <typename T, typename TIN, int R, int O, bool FROM_INC>
+enum : int { kPairDelta = 0, kPairGiven = 1, kPairMat = 2 };
+
+template <typename T, typename TIN, int R, int O, int MODE>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) pair_kernel(PairParams p)
 {
     using BS = BlockShape<R, O>;
@@ -68,7 +79,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) pair_kernel(PairParams p)
     T *bnd = p.bnd ? reinterpret_cast<T *>(p.bnd) + gwarp * p.bnd_stride : nullptr;
     TIN *out = reinterpret_cast<TIN *>(p.out);
 
-    for (int64_t item = gwarp; item < p.nitems; item += nwarps) {
+    for (int64_t item0 = gwarp; item0 < p.nitems; item0 += nwarps) {
+        const int64_t item = p.item0 + item0;
         int64_t xi, yj;
         if (p.op == kOpPairwise) {
             xi = item;
@@ -84,7 +96,18 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) pair_kernel(PairParams p)
         if (p.sy) s *= scale_at<TIN>(p.sy, yj);
 
         T val;
-        if constexpr (FROM_INC) {
+        if constexpr (MODE == kPairMat) {
+            MatIncs<T, BS::RC> src;
+            if (p.op == kOpPairwise) {
+                src.base = p.mat + (item - p.item0) * p.ncy * p.mat_rows_x;
+                src.ld = p.mat_rows_x;
+            } else {
+                src.base = p.mat + yj * p.ncy * p.mat_ld + (xi - p.x0) * p.mat_rows_x;
+                src.ld = p.mat_ld;
+            }
+            src.ncy = p.ncy;
+            val = (*p.mat_err == 0) ? warp_solve<T, R, O>(g, src, bnd) : T(NAN);
+        } else if constexpr (MODE == kPairGiven) {
             GivenIncs<T, TIN, BS::RC> src;
             const TIN *base = reinterpret_cast<const TIN *>(p.inc);
             if (p.op == kOpPairwise) {
@@ -99,12 +122,12 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) pair_kernel(PairParams p)
             src.fscale = T(s);
             val = warp_solve<T, R, O>(g, src, bnd);
         } else {
-            PathIncs<T, TIN, BS::RC> src;
-            src.X = reinterpret_cast<const TIN *>(p.x) + xi * (p.ncx + 1) * p.d;
-            src.Y = reinterpret_cast<const TIN *>(p.y) + yj * (p.ncy + 1) * p.d;
+            DeltaIncs<T, BS::RC> src;
+            src.dX = reinterpret_cast<const T *>(p.dx) + xi * p.d * p.ncx;
+            src.dY = reinterpret_cast<const T *>(p.dy) + yj * p.d * p.ncy;
             src.d = p.d;
+            src.ncy = p.ncy;
             src.dxs = p.stage_smem ? reinterpret_cast<T *>(smem_raw) + (int64_t)wib * BS::RC * p.d * 32 : nullptr;
-            src.fscale = T(s);
             val = warp_solve<T, R, O>(g, src, bnd);
         }
         if (lane == 0) {

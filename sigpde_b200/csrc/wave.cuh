@@ -109,69 +109,47 @@ __device__ __forceinline__ SolveGeom make_geom(int64_t ncx, int64_t ncy, int ord
     return g;
 }
 
-// Source of increments computed from the two paths (linear static kernel):
-// c(ci, cj) = fscale * <x[ci+1]-x[ci], y[cj+1]-y[cj]>, differences taken in T
-// (exact for float32 paths when T is double).  Computing the differences
-// first avoids the cancellation of the reference's 4-term difference of the
-// static Gram (sigpde/torch/kernel.py:13-21); both are equal in exact
-// arithmetic.  The lane's dx rows live in shared memory as [rc][k][lane]
-// (conflict-free); without a staging area they are re-read from global.
-template <typename T, typename TIN, int RC>
-struct PathIncs {
-    const TIN *X;
-    const TIN *Y;
-    int64_t d;
-    T *dxs;      // this warp's staging area: RC * d * 32 values, or null
-    T fscale;
-    int64_t ci0 = 0, ncx = 0;
-    bool rc_per_row = false;
+// Increments read from a precomputed float matrix: c[rc] = m[cj * ld + ci0 + rc].
+// Each read also asks the L2 for the lane's rows kIncPrefetch columns ahead,
+// so the wavefront's loads find them there instead of waiting on HBM.
+constexpr int kIncPrefetch = 8;
 
-    __device__ __forceinline__ void stage(int64_t ci0_, int64_t ncx_, int lane, bool rc_per_row_)
+__device__ __forceinline__ void prefetch_l2(const void *p)
+{
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+template <typename T, int RC>
+struct MatIncs {
+    const float *base;
+    int64_t ld, ncy;
+    int ci0 = 0, ncx = 0;
+    __device__ __forceinline__ void stage(int64_t ci0_, int64_t ncx_, int, bool)
     {
-        ci0 = ci0_;
-        ncx = ncx_;
-        rc_per_row = rc_per_row_;
-        if (!dxs) return;
-        __syncwarp();
-        for (int rc = 0; rc < RC; ++rc) {
-            const int64_t ci = ci0 + (rc_per_row ? rc : 0);
-            const bool ok = ci < ncx;
-            const TIN *x0 = X + ci * d;
-            for (int64_t k = 0; k < d; ++k) {
-                T v = T(0);
-                if (ok) v = T(ld_in(x0 + d + k)) - T(ld_in(x0 + k));
-                dxs[(rc * d + k) * 32 + lane] = v;
-            }
-        }
-        __syncwarp();
+        ci0 = (int)ci0_;
+        ncx = (int)ncx_;
     }
-
-    __device__ __forceinline__ void column(int64_t cj, int lane, T (&c)[RC]) const
+    __device__ __forceinline__ void column(int64_t cj, int, T (&c)[RC]) const
     {
-#pragma unroll
-        for (int rc = 0; rc < RC; ++rc) c[rc] = T(0);
-        const TIN *y0 = Y + cj * d;
-        if (dxs) {
-            for (int64_t k = 0; k < d; ++k) {
-                const T dy = T(ld_in(y0 + d + k)) - T(ld_in(y0 + k));
-#pragma unroll
-                for (int rc = 0; rc < RC; ++rc) c[rc] = fma(dxs[(rc * d + k) * 32 + lane], dy, c[rc]);
-            }
+        const float *row = base + cj * ld;
+        if (cj + kIncPrefetch < ncy && ci0 < ncx) prefetch_l2(row + kIncPrefetch * ld + ci0);
+        if constexpr (RC == 1) {
+            c[0] = ci0 < ncx ? T(row[ci0]) : T(0);
+        } else if constexpr (RC == 2) {
+            const float2 v = ci0 < ncx ? *reinterpret_cast<const float2 *>(row + ci0) : make_float2(0.f, 0.f);
+            c[0] = T(v.x);
+            c[1] = T(v.y);
         } else {
-            for (int64_t k = 0; k < d; ++k) {
-                const T dy = T(ld_in(y0 + d + k)) - T(ld_in(y0 + k));
 #pragma unroll
-                for (int rc = 0; rc < RC; ++rc) {
-                    const int64_t ci = ci0 + (rc_per_row ? rc : 0);
-                    if (ci < ncx) {
-                        const TIN *x0 = X + ci * d;
-                        c[rc] = fma(T(ld_in(x0 + d + k)) - T(ld_in(x0 + k)), dy, c[rc]);
-                    }
-                }
+            for (int q = 0; q < RC / 4; ++q) {
+                const float4 v = (ci0 + 4 * q < ncx) ? *reinterpret_cast<const float4 *>(row + ci0 + 4 * q)
+                                                     : make_float4(0.f, 0.f, 0.f, 0.f);
+                c[4 * q + 0] = T(v.x);
+                c[4 * q + 1] = T(v.y);
+                c[4 * q + 2] = T(v.z);
+                c[4 * q + 3] = T(v.w);
             }
         }
-#pragma unroll
-        for (int rc = 0; rc < RC; ++rc) c[rc] *= fscale;
     }
 };
 
@@ -179,6 +157,12 @@ struct PathIncs {
 // T, stored dimension-major per path (dX[k * ncx + ci], dY[k * ncy + cj]): the
 // lanes of a warp read neighbouring columns cj of one dimension k together
 // (lane l is one column behind lane l-1), so the loads coalesce.
+// c(ci, cj) = <dX[ci], dY[cj]> (times fscale): taking the differences first
+// (exact in float64 for float32 paths) avoids the cancellation of the
+// reference's 4-term difference of the static Gram (sigpde/torch/kernel.py:
+// 13-21); both are equal in exact arithmetic.  The lane's dx rows live in
+// shared memory as [rc][k][lane] (conflict-free) when a staging area is
+// given, else they are re-read from global memory.
 template <typename T, int RC>
 struct DeltaIncs {
     const T *dX;
@@ -210,6 +194,7 @@ struct DeltaIncs {
         for (int rc = 0; rc < RC; ++rc) c[rc] = T(0);
         const T *dy = dY + cj;
         if (dxs) {
+#pragma unroll 4
             for (int64_t k = 0; k < d; ++k) {
                 const T v = dy[k * ncy];
 #pragma unroll

@@ -89,14 +89,20 @@ def tc_plan(x_lengths, y_lengths, tile_m=128, tile_n=256):
     blk = cols * ld
     inc_off = np.zeros_like(blk)
     inc_off[1:] = np.cumsum(blk)[:-1]
-    tiles = []
-    for b in np.argsort(-(rows * cols).astype(np.float64), kind="stable"):
-        for i in range(int((rows[b] + tile_m - 1) // tile_m)):
-            for j in range(int((cols[b] + tile_n - 1) // tile_n)):
-                tiles.append((a_row0[b] + tile_m * i, b_row0[b] + tile_n * j, min(tile_m, rows[b] - tile_m * i),
-                              min(tile_n, cols[b] - tile_n * j), inc_off[b] + tile_n * j * ld[b] + tile_m * i, ld[b]))
+    # tiles (i, j) of every pair, i over 128-row blocks, j over 256-column blocks; largest pairs first
+    ti = (rows + tile_m - 1) // tile_m
+    tj = (cols + tile_n - 1) // tile_n
+    order = np.argsort(-(rows * cols).astype(np.float64), kind="stable")
+    cnt = (ti * tj)[order]
+    pb = np.repeat(order, cnt)
+    local = np.arange(int(cnt.sum()), dtype=np.int64) - np.repeat(np.cumsum(cnt) - cnt, cnt)
+    i = local // tj[pb]
+    j = local - i * tj[pb]
+    tiles = np.stack([a_row0[pb] + tile_m * i, b_row0[pb] + tile_n * j, np.minimum(tile_m, rows[pb] - tile_m * i),
+                      np.minimum(tile_n, cols[pb] - tile_n * j), inc_off[pb] + tile_n * j * ld[pb] + tile_m * i,
+                      ld[pb]], axis=1).astype(np.int64)
     return {"a_row0": a_row0, "b_row0": b_row0, "a_rows": int(r8.sum()) + tile_m, "b_rows": int(c8.sum()) + tile_n,
-            "inc_off": inc_off, "inc_elems": int(blk.sum()), "tiles": np.asarray(tiles, np.int64).reshape(-1, 6)}
+            "inc_off": inc_off, "inc_elems": int(blk.sum()), "tiles": tiles.reshape(-1, 6)}
 
 
 def plan(x_lengths, y_lengths, orders, dim, tsize, staged=True, rows_fn=None):
@@ -109,8 +115,16 @@ def plan(x_lengths, y_lengths, orders, dim, tsize, staged=True, rows_fn=None):
     od = np.asarray(orders, np.int64)
     n = (np.minimum(lx, ly) - 1) << od
     m = (np.maximum(lx, ly) - 1) << od
-    pick = rows_fn if rows_fn is not None else (lambda a, o: rows_per_lane(a, dim, o, tsize, staged))
-    rows = np.array([pick(int(a), int(o)) for a, o in zip(n, od)], np.int64)
+    if rows_fn is not None:
+        rows = np.array([rows_fn(int(a), int(o)) for a, o in zip(n, od)], np.int64)
+    else:  # rows_per_lane, vectorised
+        rows = np.where(n <= 64, 2, np.where(n <= 128, 4, np.where(n <= 256, 8, 16))).astype(np.int64)
+        if staged:
+            cap = STAGE_BYTES_PER_WARP // tsize
+            for _ in range(3):
+                rc = np.where(od >= 4, 1, np.maximum(rows >> np.minimum(od, 4), 1))
+                shrink = (rows > 2) & (rc * dim * 32 > cap)
+                rows = np.where(shrink, rows >> 1, rows)
     bands = (n + 32 * rows - 1) // (32 * rows)
     sizes = (bands - 1) * (m + 1)
     bnd_off = np.zeros_like(sizes)
@@ -192,6 +206,13 @@ class RaggedPairwise:
         self.x_scale = None
         self.y_scale = None
         self.graph = None
+
+    def load_packed(self, x_pack, y_pack, x_scale=None, y_scale=None):
+        """Copy already packed paths ((x_points, dim) and (y_points, dim), same layout as `pack`)."""
+        self.x_pack.copy_(x_pack)
+        self.y_pack.copy_(y_pack)
+        self.x_scale = self._scale_buffer(self.x_scale, x_scale)
+        self.y_scale = self._scale_buffer(self.y_scale, y_scale)
 
     def load(self, x_paths, y_paths, x_scale=None, y_scale=None):
         """Copy new path values (same shapes) into the packed buffers."""

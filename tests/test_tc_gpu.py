@@ -7,11 +7,14 @@ Cauchy-Schwarz bound sqrt(k(x,x) k(y,y)) (the cells grow to that size, so a
 pointwise bound on near-zero entries is not available in float32 storage):
   * "tc64" (float64 cells): at most 1e-5, the accuracy target for the fast
     modes on Brownian paths;
-  * "tc32" (float32 cells): at most 4x the reference's own float32 GPU
-    numerics on the same inputs (as for "fp32"), plus 1e-7.
-Shapes outside the TC plan (several bands of rows per pair, dim > 32) form
-their increments on the CUDA cores; with float64 cells they meet the fp64
-bound of 1e-9 relative.
+  * "tc32" (float32 cells): at most 6x the reference's own float32 GPU
+    numerics on the same inputs, plus 1e-7 (the "fp32" bound of 4x, widened
+    for the split-TF32 increments' own ~2^-21 relative error, which adds to
+    the float32 cell rounding on long paths).
+Pairs of several bands of rows, or with fewer than 32 column blocks, read
+the same matrix from the per-pair kernel.  dim > 32 is outside the TC plan:
+those increments are formed on the CUDA cores and, with float64 cells, meet
+the fp64 bound of 1e-9 relative.
 """
 import numpy as np
 import pytest
@@ -57,7 +60,7 @@ def _check(oracle, got, x, y, order, prec, sx=None, sy=None, sym=False, pairwise
     if prec == "tc64":
         assert err <= CS_TC64, f"tc64 CS-normalised error {err:.3e}"
     else:
-        tol = 4.0 * cs(ref, want, kxx, kyy) + 1e-7
+        tol = 6.0 * cs(ref, want, kxx, kyy) + 1e-7
         assert err <= tol, f"tc32 CS-normalised error {err:.3e} > {tol:.3e}"
     return err
 
@@ -129,13 +132,26 @@ def test_tc_is_deterministic(sig, oracle):
     np.testing.assert_array_equal(a, b)
 
 
-@pytest.mark.parametrize("shape", [(3, 4, 600, 4, 0), (4, 3, 30, 40, 1)])
-def test_tc_modes_outside_the_plan_use_cuda_core_increments(sig, oracle, shape):
-    """Multi-band pairs and dim > 32 run CUDA-core increments with float64 cells."""
+@pytest.mark.parametrize("prec", ["tc64", "tc32"])
+@pytest.mark.parametrize("shape", [(3, 4, 600, 4, 0), (5, 4, 170, 32, 2), (6, 5, 20, 8, 0)])
+def test_tc_multi_band_and_short_pairs(sig, oracle, shape, prec):
+    """Pairs of several bands of rows (n > 512) or fewer than 32 column blocks read the
+    increment matrix from the per-pair kernel: Gram, symmetric Gram and pairwise."""
     nx, ny, L, d, o = shape
-    x = oracle.brownian(nx, L, d, 61)
-    y = oracle.brownian(ny, L, d, 62)
-    k = sig.SigPDE(sig.kernels.LinearKernel(), o, precision="tc64")
+    X = cuda(oracle.brownian(nx, L, d, 61))
+    Y = cuda(oracle.brownian(ny, L + 5, d, 62))
+    k = sig.SigPDE(sig.kernels.LinearKernel(), o, precision=prec)
+    _check(oracle, host(k.gram(X, Y)), host(X), host(Y), o, prec)
+    _check(oracle, host(k.gram(X)), host(X), None, o, prec, sym=True)
+    Yp = cuda(oracle.brownian(nx, L + 5, d, 63))
+    _check(oracle, host(k.pairwise(X, Yp)), host(X), host(Yp), o, prec, pairwise=True)
+
+
+def test_tc_modes_outside_the_plan_use_cuda_core_increments(sig, oracle):
+    """dim > 32 runs CUDA-core increments with float64 cells (fp64 bound)."""
+    x = oracle.brownian(4, 30, 40, 61)
+    y = oracle.brownian(3, 30, 40, 62)
+    k = sig.SigPDE(sig.kernels.LinearKernel(), 1, precision="tc64")
     got = host(k.gram(cuda(x, torch.float64), cuda(y, torch.float64)))
-    want = oracle.gram(x, y, o)
+    want = oracle.gram(x, y, 1)
     assert np.max(np.abs(got - want) / np.abs(want)) <= 1e-9
