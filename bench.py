@@ -883,9 +883,11 @@ def run_serve(args, w):
         for h in handles:
             h.wait(timeout=600)
         peak = srv.peak_inflight
+        batching = {"batches": srv.batches, "batched_requests": srv.batched_requests}
     clk = clocks.stop()
     served = summarize(handles, t0, max(h.t_done for h in handles))
     served["peak_inflight"] = peak
+    served["kernel_level_batching"] = batching
     # per-request plain launches, same arrivals
     for r in reqs:
         r.arrival = 0.0

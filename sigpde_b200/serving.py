@@ -9,6 +9,17 @@ them in arrival order as soon as two resources allow it:
   robust scratch), estimated before admission, fits in the HBM budget next to
   the footprints of the requests already on the device.
 
+With `batch_small=True`, small symmetric requests that wait together are
+batched at the kernel level: the lower triangles of their Grams become the
+pairs of ONE uneven-batch launch (sigpde_b200.torch.ragged: every pair with
+its own path length and dyadic order; a robust request's lambdas become
+per-pair scales), and the pair results are scattered back into each
+request's matrix.  Results are bitwise those of the requests alone.  It is
+off by default: the uneven-batch launch copies each path once per pair and
+(tensor-core modes) gives every pair its own GEMM tiles, so on the measured
+traces it is slower than running the small requests' own Gram launches
+concurrently.
+
 Among the requests waiting, the cheapest (fewest PDE cells) is admitted
 first; a request that has waited longer than `max_wait_s` goes first
 regardless, so nothing starves.  An admitted request is enqueued on its own
@@ -43,7 +54,8 @@ from . import _lib
 from .torch import kernel as _k
 from .torch import static_kernels as _sk
 
-__all__ = ["GramRequest", "RequestHandle", "GramServer", "serve_sequential", "footprint_bytes", "request_cells"]
+__all__ = ["GramRequest", "RequestHandle", "GramServer", "serve_sequential", "footprint_bytes", "request_cells",
+           "request_pairs", "batch_footprint_bytes"]
 
 
 @dataclasses.dataclass
@@ -114,15 +126,95 @@ def footprint_bytes(req: GramRequest, precision: str = "fp64") -> int:
 
 
 class _Inflight:
-    __slots__ = ("handle", "stream", "event", "bytes", "out_host", "keep")
+    """One admitted unit: a single request, or a batch of small requests solved by one launch."""
+    __slots__ = ("handles", "stream", "event", "bytes", "out_hosts", "keep")
 
-    def __init__(self, handle, stream, event, nbytes, out_host, keep):
-        self.handle = handle
+    def __init__(self, handles, stream, event, nbytes, out_hosts, keep):
+        self.handles = handles
         self.stream = stream
         self.event = event
         self.bytes = nbytes
-        self.out_host = out_host
+        self.out_hosts = out_hosts
         self.keep = keep
+
+
+def request_pairs(req: GramRequest) -> int:
+    """PDE solves of a request (the lower triangle, diagonal included, for a symmetric Gram)."""
+    nx = int(req.x.shape[0])
+    return nx * (nx + 1) // 2 if req.y is None else nx * int(req.y.shape[0])
+
+
+def batch_footprint_bytes(reqs, precision: str = "fp64") -> int:
+    """Device bytes of a batch of small symmetric requests solved by one ragged launch (an upper
+    estimate): the paths, the per-pair path packs and their differences or tensor-core operands and
+    increment blocks, the band boundary rows, the pair results and the Gram results."""
+    total = 0
+    tc = precision in ("tc32", "tc64")
+    for r in reqs:
+        N, L, d = r.x.shape
+        es = r.x.element_size()
+        P = N * (N + 1) // 2
+        n = (L - 1) << r.order
+        bands = -(-n // 512)
+        total += r.x.numel() * es + N * N * es + 2 * P * (es + 8) + 8 * P * 4
+        total += 2 * P * L * d * es                      # x and y packs
+        if tc:
+            kp = (d + 7) // 8 * 8
+            total += P * (L - 1) * ((L - 1 + 3) // 4 * 4) * 4 + 4 * P * (L + 8) * kp * 4
+        else:
+            total += 2 * P * (L - 1) * d * 8
+        total += P * max(bands - 1, 0) * (n + 1) * 8 + 4 * P * bands
+    return int(total + (64 << 20))  # plus the tile table, images' tile padding and counters
+
+
+def _solve_batch_on_stream(reqs, precision: str, device, stream):
+    """Enqueue several small symmetric requests as ONE uneven-batch launch on `stream`: the lower
+    triangle of every request's Gram becomes pairs of one ragged batch (paths of their own length
+    and dyadic order; robust requests bring their lambdas as per-pair scales), and the pair results
+    are scattered back into each request's matrix.  Returns (pinned host results, keep-alive)."""
+    import numpy as np
+    from .torch import ragged as _rg
+    with torch.cuda.stream(stream):
+        xs, parts_x, parts_y, sx_parts, sy_parts, lens, ords, tris = [], [], [], [], [], [], [], []
+        for r in reqs:
+            if r.kind not in ("gram", "robust") or r.y is not None:
+                raise ValueError("only symmetric gram / robust requests are batched")
+            x = r.x.to(device, non_blocking=True)
+            N, L, d = x.shape
+            ii, jj = torch.tril_indices(N, N, device=device)  # i >= j: x_i on the rows, as the symmetric Gram
+            if r.kind == "robust":
+                lam = _k.RobustSigPDE(_sk.LinearKernel(), r.order, precision=precision).normalization(x)
+                sx_parts.append(lam.index_select(0, ii))
+                sy_parts.append(lam.index_select(0, jj))
+            else:
+                one = torch.ones(ii.numel(), dtype=x.dtype, device=device)
+                sx_parts.append(one)
+                sy_parts.append(one)
+            parts_x.append(x.index_select(0, ii).reshape(-1, d))
+            parts_y.append(x.index_select(0, jj).reshape(-1, d))
+            P = int(ii.numel())
+            lens.append(np.full(P, L, np.int64))
+            ords.append(np.full(P, r.order, np.int64))
+            xs.append(x)
+            tris.append((N, ii, jj, P))
+        lens = np.concatenate(lens)
+        ords = np.concatenate(ords)
+        solver = _rg.RaggedPairwise(lens, lens, ords, xs[0].shape[2], xs[0].dtype, device, precision)
+        solver.load_packed(torch.cat(parts_x), torch.cat(parts_y), torch.cat(sx_parts), torch.cat(sy_parts))
+        out = solver.solve()
+        hosts, results = [], []
+        off = 0
+        for N, ii, jj, P in tris:
+            v = out[off:off + P]
+            off += P
+            res = torch.empty((N, N), dtype=out.dtype, device=device)
+            res[ii, jj] = v
+            res[jj, ii] = v
+            host = torch.empty((N, N), dtype=out.dtype, pin_memory=True)
+            host.copy_(res, non_blocking=True)
+            hosts.append(host)
+            results.append(res)
+    return hosts, (xs, parts_x, parts_y, sx_parts, sy_parts, solver, out, results, tris)
 
 
 def request_cells(req: GramRequest) -> int:
@@ -191,7 +283,8 @@ class GramServer:
 
     def __init__(self, device="cuda", max_inflight: int = 8, hbm_budget_bytes: Optional[int] = None,
                  precision: str = "fp64", poll_interval_s: float = 50e-6, chunk_cells: int = 2 * 10 ** 12,
-                 max_wait_s: float = 2.0):
+                 max_wait_s: float = 2.0, batch_small: bool = False, small_pairs: int = 8192,
+                 small_cells: int = 2 * 10 ** 9, batch_pairs: int = 1 << 17):
         self.device = torch.device(device)
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
@@ -204,6 +297,13 @@ class GramServer:
         self.poll = poll_interval_s
         self.chunk_cells = int(chunk_cells)
         self.max_wait_s = float(max_wait_s)
+        # kernel-level batching: small symmetric requests waiting together go into one ragged launch
+        self.batch_small = bool(batch_small)
+        self.small_pairs = int(small_pairs)
+        self.small_cells = int(small_cells)
+        self.batch_pairs = int(batch_pairs)
+        self.batches = 0
+        self.batched_requests = 0
         self._q: "queue.Queue[RequestHandle]" = queue.Queue()
         self._pending: collections.deque = collections.deque()
         self._inflight: list = []
@@ -253,9 +353,63 @@ class GramServer:
         pool = old if old else self._pending
         return min(pool, key=lambda h: (h.req.arrival if old else h.cost))
 
+    def _small(self, req) -> bool:
+        try:
+            return (self.batch_small and req.y is None and req.kind in ("gram", "robust") and req.x.dim() == 3
+                    and req.x.shape[1] >= 2 and req.x.shape[0] >= 1 and request_pairs(req) <= self.small_pairs
+                    and request_cells(req) <= self.small_cells)
+        except Exception:
+            return False
+
+    def _admit_batch(self, first) -> bool:
+        """Admit `first` with the other small waiting requests of the same dim and dtype as one
+        launch; False (nothing admitted) when memory is short."""
+        key = (int(first.req.x.shape[2]), first.req.x.dtype)
+        group = [first]
+        pairs = request_pairs(first.req)
+        for h in sorted(self._pending, key=lambda g: g.cost):
+            if h is first or not self._small(h.req) or (int(h.req.x.shape[2]), h.req.x.dtype) != key:
+                continue
+            p = request_pairs(h.req)
+            if pairs + p > self.batch_pairs:
+                continue
+            group.append(h)
+            pairs += p
+        need = batch_footprint_bytes([h.req for h in group], self.precision)
+        while len(group) > 1 and need > self.budget:
+            group.pop()
+            need = batch_footprint_bytes([h.req for h in group], self.precision)
+        if len(group) == 1 or self._used + need > self.budget:
+            return False
+        for h in group:
+            self._pending.remove(h)
+        stream = self._free_streams.pop()
+        now = time.perf_counter()
+        for h in group:
+            h.t_admit = now
+        try:
+            with torch.cuda.device(self.device):
+                hosts, keep = _solve_batch_on_stream([h.req for h in group], self.precision, self.device, stream)
+                ev = torch.cuda.Event()
+                ev.record(stream)
+        except Exception as e:
+            self._free_streams.append(stream)
+            for h in group:
+                h._finish(error=e)
+            return True
+        self._used += need
+        self._inflight.append(_Inflight(group, stream, ev, need, hosts, keep))
+        self.batches += 1
+        self.batched_requests += len(group)
+        self.peak_inflight = max(self.peak_inflight, len(self._inflight))
+        self.peak_bytes = max(self.peak_bytes, self._used)
+        return True
+
     def _admit(self):
         while self._pending and self._free_streams:
             h = self._next()
+            if self._small(h.req) and self._admit_batch(h):
+                continue
             try:
                 need = footprint_bytes(h.req, self.precision)
             except Exception as e:  # malformed request: fail it, keep serving
@@ -282,7 +436,7 @@ class GramServer:
                 h._finish(error=e)
                 continue
             self._used += need
-            self._inflight.append(_Inflight(h, stream, ev, need, out_host, keep))
+            self._inflight.append(_Inflight([h], stream, ev, need, [out_host], keep))
             self.peak_inflight = max(self.peak_inflight, len(self._inflight))
             self.peak_bytes = max(self.peak_bytes, self._used)
 
@@ -293,7 +447,8 @@ class GramServer:
                 self._used -= f.bytes
                 self._free_streams.append(f.stream)
                 f.keep = None
-                f.handle._finish(result=f.out_host)
+                for h, host in zip(f.handles, f.out_hosts):
+                    h._finish(result=host)
             else:
                 still.append(f)
         self._inflight = still

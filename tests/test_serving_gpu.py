@@ -3,7 +3,8 @@ HBM-footprint admission.
 
 * each request's result in a concurrent mix equals the same request solved
   alone through the API (the solves are deterministic and only read their own
-  buffers, so the tolerance is 0: bitwise equal);
+  buffers, so the tolerance is 0: bitwise equal), also when small requests are
+  batched into one uneven-batch launch (the same arithmetic per cell);
 * requests overlap on the device (more than one in flight at once);
 * the in-flight footprint never exceeds the HBM budget; a request larger than
   the whole budget fails alone with MemoryError;
@@ -70,6 +71,26 @@ def test_results_in_the_mix_equal_results_alone(oracle):
             yy = x if y is None else y
             want = oracle.gram(x, yy, r.order, pairs=[i * yy.shape[0] + j])[0]
         assert abs(float(got[i, j]) - want) <= 2.5e-7 * abs(want) + 1e-300
+
+
+@pytest.mark.parametrize("precision", ["fp64", "tc64"])
+def test_small_requests_are_batched_into_one_launch(oracle, precision):
+    """Small symmetric requests waiting together run as one uneven-batch launch; each
+    result equals the request solved alone through the API with the same precision."""
+    import sigpde_b200.torch as sig
+    from sigpde_b200.serving import GramServer
+    reqs = [r for r in _requests(oracle, 30, 7) if r.y is None]
+    with GramServer(max_inflight=2, precision=precision, batch_small=True) as srv:
+        handles = [srv.submit(r) for r in reqs]
+        results = [h.wait(timeout=120) for h in handles]
+        assert srv.batches >= 1 and srv.batched_requests >= 2
+    for r, got in zip(reqs, results):
+        x = r.x.cuda()
+        if r.kind == "robust":
+            want = sig.RobustSigPDE(sig.kernels.LinearKernel(), r.order, precision=precision).gram(x).cpu()
+        else:
+            want = sig.SigPDE(sig.kernels.LinearKernel(), r.order, precision=precision).gram(x).cpu()
+        np.testing.assert_array_equal(got.numpy(), want.numpy())
 
 
 def test_admission_respects_the_hbm_budget(oracle):
