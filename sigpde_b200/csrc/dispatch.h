@@ -38,6 +38,8 @@ PairFn get_pair_kernel_f64(bool in64, int mode, int R, int O);
 PairFn get_pair_kernel_f32(bool in64, int mode, int R, int O);
 // mode: kNormDelta, kNormGiven or kNormTile (sigk_kernels.cuh)
 NormFn get_norm_kernel(bool in64, int mode, int R, int O);
+// one CTA per path, its bands as a warp pipeline (norm_pipe.cuh)
+NormFn get_norm_pipe_kernel(bool in64, int mode, int R, int O);
 // D: dimension padded to a power of two in {2,...,32}; returns null unless
 // the lane's register tile (coarse rows per lane) * D <= 32.
 StreamFn get_stream_reg_kernel(bool f64cells, int R, int O, int D);

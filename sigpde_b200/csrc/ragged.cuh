@@ -117,9 +117,13 @@ __device__ __forceinline__ int wait_progress(const int *prog, int need)
 // One band of one pair.  top_buf / top_prog: the band above (null for band 0);
 // bot_buf / bot_prog: this band's bottom row and progress (bot_buf null for the
 // last band).  Returns K[n][m] in every lane if `last`, else 1.
+// prog_base: progress values of this solve are prog_base + (column blocks
+// done), so one set of counters serves consecutive solves (the pipelined
+// normalisation re-solves a path several times without resetting them);
+// pub_stride: column blocks between publications of the band's progress.
 template <typename T, int R, int O, class Src>
 __device__ T band_solve(const SolveGeom &g, Src &src, int band, bool last, const T *top_buf, const int *top_prog,
-                        T *bot_buf, int *bot_prog, int *error)
+                        T *bot_buf, int *bot_prog, int *error, int prog_base = 0, int pub_stride = kProgressStride)
 {
     using BS = BlockShape<R, O>;
     constexpr int C = BS::C;
@@ -152,7 +156,8 @@ __device__ T band_solve(const SolveGeom &g, Src &src, int band, bool last, const
                 for (int c = 0; c < C; ++c) top[c] = T(1);
             } else if (active) {
                 if (!poisoned && seen <= q) {
-                    const int v = wait_progress(top_prog, (int)q + 1);
+                    const int v0 = wait_progress(top_prog, prog_base + (int)q + 1);
+                    const int v = (v0 < 0 || v0 == 0x7fffffff) ? v0 : v0 - prog_base;
                     if (v < 0 || v == 0x7fffffff) { // ran out, or the band above was refused
                         poisoned = true;
                         if (v < 0) *error = 1;
@@ -190,9 +195,9 @@ __device__ T band_solve(const SolveGeom &g, Src &src, int band, bool last, const
             if (writer) {
 #pragma unroll
                 for (int c = 0; c < C; ++c) bot_buf[q * C + 1 + c] = bot[c];
-                if ((q + 1) % kProgressStride == 0 || q + 1 == g.nsteps) {
+                if ((q + 1) % pub_stride == 0 || q + 1 == g.nsteps) {
                     __threadfence();
-                    st_release(bot_prog, (int)q + 1);
+                    st_release(bot_prog, prog_base + (int)q + 1);
                 }
             }
         }

@@ -22,6 +22,7 @@
 #include "ragged.cuh"
 #include "stream.cuh"
 #include "tc.cuh"
+#include "norm_pipe.cuh"
 
 namespace sigk {
 namespace {
@@ -212,6 +213,10 @@ int blocks_per_sm(const void *fn, size_t smem, int *out)
         int optin = 0;
         e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
         if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
+        cudaFuncAttributes fa{};
+        e = cudaFuncGetAttributes(&fa, fn);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncGetAttributes");
+        optin -= (int)fa.sharedSizeBytes; // static shared memory counts against the same limit
         if (smem > (size_t)optin) return fail(SIGK_ELAUNCH, "kernel needs %zu bytes of shared memory (max %d)", smem, optin);
         e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
         if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
@@ -726,7 +731,14 @@ struct NormPlan {
     int mode, R, O, nbands;
     int64_t tile_pitch, bnd_stride;
     size_t smem_per_warp, bnd_bytes, dx_off, ws_bytes;
+    // pipelined kernel (one CTA per path, `nw` bands as warps): its shared memory per CTA and the
+    // workspace offsets of the progress counters, the wait flag and the band rows
+    bool pipe;
+    int nw;
+    size_t smem_cta, prog_off, err_off;
 };
+
+constexpr size_t kNormPipeSmemBytes = 160 * 1024;
 
 NormPlan norm_plan(int64_t n, int64_t nc, int64_t d, int order, bool from_inc)
 {
@@ -750,6 +762,48 @@ NormPlan norm_plan(int64_t n, int64_t nc, int64_t d, int order, bool from_inc)
     q.smem_per_warp = q.mode == kNormTile ? tile : q.mode == kNormDelta ? pl.stage_bytes_per_warp : 0;
     q.dx_off = q.bnd_bytes;
     q.ws_bytes = from_inc ? q.bnd_bytes : q.dx_off + align256((size_t)n * (size_t)d * (size_t)nc * sizeof(double));
+
+    // Pipelined variant (one CTA per path, R = 2 rows per lane grown until the bands fit one CTA).
+    // Measured on B200 it wins only where it can hold the path's increment tile in shared memory
+    // for the whole CTA while the one-warp-per-path kernel cannot (tile above 48 KB) and the
+    // increments are expensive to re-form (d >= 16): N=32 L=128 d=32 o=1, 1.64 ms vs 6.58 ms.
+    // Elsewhere its band hand-offs cost more than they save (N=512 L=64 d=16 o=1: 0.74 vs 0.29 ms;
+    // N=8 L=256 d=8 o=2: 8.5 vs 5.3 ms), so it is used for that case only (SIGK_NORM_PIPE=1 forces
+    // it when possible, SIGK_NO_NORM_PIPE=1 disables it).
+    const int64_t nref = nc << order;
+    int R = 2;
+    while (R < 16 && (nref + 32 * R - 1) / (32 * R) > kNormPipeMaxWarps) R <<= 1;
+    const int64_t nw = (nref + 32 * R - 1) / (32 * R);
+    const bool wins = !from_inc && d >= 16 && tile > kNormTileBytesPerWarp && tile <= kNormPipeSmemBytes;
+    if (nw >= 2 && nw <= kNormPipeMaxWarps && (wins || env_flag("SIGK_NORM_PIPE")) && !env_flag("SIGK_NO_NORM_PIPE")) {
+        const int rc = rows_per_coarse_lane(R, order);
+        int mode = q.mode;
+        size_t smem = 0;
+        if (mode == kNormTile || mode == kNormDelta) {
+            // one shared tile per CTA when it fits, else per-warp staged differences (or none)
+            mode = (tile <= kNormPipeSmemBytes && !env_flag("SIGK_NO_NORM_TILE")) ? kNormTile : kNormDelta;
+            if (mode == kNormTile) {
+                smem = tile;
+            } else {
+                const size_t st = (size_t)rc * (size_t)d * 32 * sizeof(double) * (size_t)nw;
+                smem = st <= kNormPipeSmemBytes ? st : 0;
+            }
+        }
+        const int64_t m = nc << order;
+        q.pipe = true;
+        q.mode = mode;
+        q.R = R;
+        q.nw = (int)nw;
+        q.smem_cta = smem;
+        q.bnd_stride = ((m + 1 + 31) / 32) * 32;
+        q.prog_off = 0;
+        q.err_off = align256((size_t)n * kNormPipeMaxWarps * sizeof(int));
+        q.bnd_bytes = q.err_off + 256; // counters and flag, zeroed before each launch
+        const size_t rows = align256((size_t)n * (size_t)(nw - 1) * (size_t)q.bnd_stride * sizeof(double));
+        q.dx_off = q.bnd_bytes + rows;
+        q.ws_bytes = from_inc ? q.dx_off
+                              : q.dx_off + align256((size_t)n * (size_t)d * (size_t)nc * sizeof(double));
+    }
     return q;
 }
 
@@ -874,6 +928,36 @@ static int normalize_impl(const void *x, const void *inc, int64_t n, int64_t nc,
     p.maxit = maxit;
     p.lam = lam;
     p.iters = iters;
+    if (q.pipe) {
+        cudaError_t e = cudaMemsetAsync(wsb, 0, q.bnd_bytes, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(progress)");
+        p.prog = reinterpret_cast<int *>(wsb + q.prog_off);
+        p.err = reinterpret_cast<int *>(wsb + q.err_off);
+        p.bnd = wsb + q.bnd_bytes;
+        p.bnd_stride = q.bnd_stride;
+        p.stage_smem = q.mode == kNormDelta && q.smem_cta > 0;
+        NormFn fn = get_norm_pipe_kernel(dtype == SIGK_F64, q.mode, q.R, q.O);
+        if (q.smem_cta > 48 * 1024) {
+            int dev = 0, optin = 0;
+            if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+            if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess)
+                return cuda_fail(e, "cudaDeviceGetAttribute");
+            cudaFuncAttributes fa{};
+            if ((e = cudaFuncGetAttributes(&fa, (const void *)fn)) != cudaSuccess)
+                return cuda_fail(e, "cudaFuncGetAttributes");
+            const int dyn_max = optin - (int)fa.sharedSizeBytes; // the kernel's static shared memory counts too
+            if ((size_t)dyn_max < q.smem_cta)
+                return fail(SIGK_ELAUNCH, "normalisation needs %zu bytes of shared memory", q.smem_cta);
+            if ((e = cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_max)) !=
+                cudaSuccess)
+                return cuda_fail(e, "cudaFuncSetAttribute");
+        }
+        const int64_t grid = n < 0x7fffffffLL ? n : 0x7fffffffLL; // one CTA per path (more paths: strided)
+        fn<<<(unsigned)grid, q.nw * 32, q.smem_cta, stream>>>(p);
+        count_launch();
+        e = cudaGetLastError();
+        return e == cudaSuccess ? SIGK_OK : cuda_fail(e, "pipelined normalisation launch");
+    }
     p.bnd = q.nbands > 1 ? ws : nullptr;
     p.bnd_stride = q.bnd_stride;
     p.stage_smem = q.smem_per_warp > 0;

@@ -163,12 +163,75 @@ struct NormParams {
     void *bnd;
     int64_t bnd_stride;
     int stage_smem;
+    // pipelined kernel (norm_pipe.cuh): per-CTA band progress counters (16 ints per CTA,
+    // zeroed before the launch) and the flag a band wait that ran out sets
+    int *prog;
+    int *err;
 };
 
-// The Chandrupatla iteration of sigpde/cuda_pairwise_kernels.py:100-178 with
+// k(x,x), f(k) and the Chandrupatla iteration for one path, given solve(s) =
+// k at increments scaled by s: sigpde/cuda_pairwise_kernels.py:100-178 with
 // the argument order of sigpde/torch/kernel.py:186-193: g(l) = k(l x) - f(k),
-// g(0) = 1 - f(k), g(1) = k - f(k).  All bracket state is float64 and
-// warp-uniform; the PDE solve returns the same value in every lane.
+// g(0) = 1 - f(k), g(1) = k - f(k).  All bracket state is float64 and uniform
+// across the threads that call it (solve returns the same value to all of
+// them); `writer` stores k(x,x).
+template <class Solve>
+__device__ __forceinline__ void normalize_path(const NormParams &p, int64_t b, bool writer, Solve &&solve,
+                                               double &out, int &it)
+{
+    double k, fk;
+    if (p.fnorm == nullptr) {
+        k = solve(1.0);
+        if (isnan(k)) k = __longlong_as_double(0x7ff0000000000000LL); // NaN -> +inf (kernel.py:183)
+        fk = 2.0 - 1.0 / (1.0 + log(k));                              // kernel.py:23-24
+        if (p.knorm && writer) p.knorm[b] = k;
+    } else {
+        k = p.knorm[b];
+        fk = p.fnorm[b];
+    }
+    out = 0.0;
+    it = 0;
+    if (k >= 1.0) { // lambda is forced to 0 for k < 1 (kernel.py:195), so the loop is skipped
+        double a = 0.0, c = 0.0, bb = 1.0;
+        double fa = 1.0 - fk;
+        double fb = k - fk;
+        double fc = fa;
+        double t = 0.5;
+        for (it = 0; it < p.maxit;) {
+            const double xt = a + t * (bb - a);
+            const double sol = solve(xt * xt);
+            const double ft = isnan(sol) ? __longlong_as_double(0x7ff0000000000000LL) : sol - fk;
+            ++it;
+            if (ft * fa >= 0) {
+                c = a;
+                fc = fa;
+            } else {
+                c = bb;
+                bb = a;
+                fc = fb;
+                fb = fa;
+            }
+            a = xt;
+            fa = ft;
+            if (fabs(fa) < fabs(fb)) {
+                out = a;
+                if (fabs(fa) < p.tol) break;
+            } else {
+                out = bb;
+                if (fabs(fb) < p.tol) break;
+            }
+            const double xi = (a - bb) / (c - bb);
+            const double phi = (fa - fb) / (fc - fb);
+            if (phi * phi < xi && (1 - phi) * (1 - phi) < 1 - xi)
+                t = fa / (fb - fa) * fc / (fb - fc) + (c - a) / (bb - a) * fa / (fc - fa) * fb / (fc - fb);
+            else
+                t = 0.5;
+            if (!(0 < t && t < 1)) t = 0.5;
+        }
+    }
+}
+
+// One path per warp: every bracket iteration re-solves the path's PDE on chip.
 template <typename TIN, int R, int O, int MODE>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) normalize_kernel(NormParams p)
 {
@@ -226,57 +289,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) normalize_kernel(NormPara
             }
         };
 
-        double k, fk;
-        if (p.fnorm == nullptr) {
-            k = solve(1.0);
-            if (isnan(k)) k = __longlong_as_double(0x7ff0000000000000LL); // NaN -> +inf (kernel.py:183)
-            fk = 2.0 - 1.0 / (1.0 + log(k));                              // kernel.py:23-24
-            if (p.knorm && lane == 0) p.knorm[b] = k;
-        } else {
-            k = p.knorm[b];
-            fk = p.fnorm[b];
-        }
-
         double out = 0.0;
         int it = 0;
-        if (k >= 1.0) { // lambda is forced to 0 for k < 1 (kernel.py:195), so the loop is skipped
-            double a = 0.0, c = 0.0, bb = 1.0;
-            double fa = 1.0 - fk;
-            double fb = k - fk;
-            double fc = fa;
-            double t = 0.5;
-            for (it = 0; it < p.maxit;) {
-                const double xt = a + t * (bb - a);
-                const double sol = solve(xt * xt);
-                const double ft = isnan(sol) ? __longlong_as_double(0x7ff0000000000000LL) : sol - fk;
-                ++it;
-                if (ft * fa >= 0) {
-                    c = a;
-                    fc = fa;
-                } else {
-                    c = bb;
-                    bb = a;
-                    fc = fb;
-                    fb = fa;
-                }
-                a = xt;
-                fa = ft;
-                if (fabs(fa) < fabs(fb)) {
-                    out = a;
-                    if (fabs(fa) < p.tol) break;
-                } else {
-                    out = bb;
-                    if (fabs(fb) < p.tol) break;
-                }
-                const double xi = (a - bb) / (c - bb);
-                const double phi = (fa - fb) / (fc - fb);
-                if (phi * phi < xi && (1 - phi) * (1 - phi) < 1 - xi)
-                    t = fa / (fb - fa) * fc / (fb - fc) + (c - a) / (bb - a) * fa / (fc - fa) * fb / (fc - fb);
-                else
-                    t = 0.5;
-                if (!(0 < t && t < 1)) t = 0.5;
-            }
-        }
+        normalize_path(p, b, lane == 0, solve, out, it);
         if (lane == 0) {
             if (lam_out) lam_out[b] = TIN(out);
             if (p.iters) p.iters[b] = it;

@@ -295,11 +295,12 @@ def test_robust_normalization_config3_shape(sig, oracle):
     np.testing.assert_allclose(lam, oracle.normalization(host(X), 1, nrm), rtol=LAM_RTOL, atol=1e-9)
 
 
-@pytest.mark.parametrize("L,d,order", [(70, 3, 3), (130, 2, 1), (12, 40, 2)])
+@pytest.mark.parametrize("L,d,order", [(70, 3, 3), (130, 2, 1), (12, 40, 2), (128, 32, 1)])
 def test_robust_normalization_increment_sources(sig, oracle, L, d, order, monkeypatch):
-    """The shared-memory increment tile (paths of up to 77 cells) and the
-    precomputed-difference source (longer paths, or SIGK_NO_NORM_TILE=1), with
-    one and several bands of rows, against the oracle and against each other."""
+    """The shared-memory increment tile and the precomputed-difference source
+    (longer paths, or SIGK_NO_NORM_TILE=1), one CTA per path with the bands as
+    a warp pipeline or one warp per path (SIGK_NO_NORM_PIPE=1), with one and
+    several bands of rows, against the oracle and against each other."""
     rng = np.random.default_rng(L + d)
     scales = np.exp(rng.uniform(np.log(0.5), np.log(4.0), 10))
     x = oracle.brownian(10, L, d, 61 + L, scale=scales)
@@ -309,9 +310,19 @@ def test_robust_normalization_increment_sources(sig, oracle, L, d, order, monkey
     want = oracle.normalization(x, order)
     np.testing.assert_allclose(lam, want, rtol=LAM_RTOL, atol=1e-9)
     assert (want > 0).sum() >= 3
+    monkeypatch.setenv("SIGK_NORM_PIPE", "1")  # the pipelined kernel wherever a path has >= 2 bands
+    np.testing.assert_array_equal(host(rk.normalization(X)), lam)
+    monkeypatch.delenv("SIGK_NORM_PIPE")
     monkeypatch.setenv("SIGK_NO_NORM_TILE", "1")
     lam_delta = host(rk.normalization(X))
     np.testing.assert_allclose(lam_delta, lam, rtol=1e-12, atol=1e-14)
+    # one warp per path (all bands in sequence) instead of one CTA per path (bands as a warp pipeline):
+    # the same cells from the same increments, so the same lambdas
+    monkeypatch.setenv("SIGK_NO_NORM_PIPE", "1")
+    lam_warp = host(rk.normalization(X))
+    np.testing.assert_array_equal(lam_warp, lam_delta)
+    monkeypatch.delenv("SIGK_NO_NORM_TILE")
+    np.testing.assert_array_equal(host(rk.normalization(X)), lam)
 
 
 def test_robust_normalization_alternating_shared_memory_sizes(sig, oracle):
