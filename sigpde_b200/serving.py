@@ -226,7 +226,7 @@ def request_cells(req: GramRequest) -> int:
     return int(x.shape[0]) * int(y.shape[0]) * n * m
 
 
-def _solve_on_stream(req: GramRequest, precision: str, device, stream, chunk_cells: int = 0):
+def _solve_on_stream(req: GramRequest, precision: str, device, stream, chunk_cells: int = 0, staging=None):
     """Enqueue copy-in, solve and copy-out of one request on `stream`.
     Returns (pinned host result, tensors to keep alive until the event).
     chunk_cells > 0 splits a large (non-symmetric or robust) Gram into row
@@ -267,7 +267,10 @@ def _solve_on_stream(req: GramRequest, precision: str, device, stream, chunk_cel
                     out[i0:i1] = k.gram(x[i0:i1], y, None if sx is None else sx[i0:i1], sy)
         else:
             out = k.gram(x, y, sx, sy if y is not None else None)
-        host = torch.empty(out.shape, dtype=out.dtype, pin_memory=True)
+        if staging is not None:  # the server's pinned buffer of this stream (no page-locked allocation per request)
+            host = staging(out.numel() * out.element_size()).view(out.dtype)[:out.numel()].view(out.shape)
+        else:
+            host = torch.empty(out.shape, dtype=out.dtype, pin_memory=True)
         host.copy_(out, non_blocking=True)
     return host, (x, y, out, sx, sy)
 
@@ -309,6 +312,9 @@ class GramServer:
         self._inflight: list = []
         self._streams = [torch.cuda.Stream(self.device) for _ in range(self.max_inflight)]
         self._free_streams = list(self._streams)
+        # one pinned staging buffer per stream for device-to-host result copies, grown by doubling:
+        # allocating page-locked memory per request (cudaHostAlloc) can stall behind work in flight
+        self._staging = {id(st): None for st in self._streams}
         self._used = 0
         self._stop = threading.Event()
         self._ids = 0
@@ -428,7 +434,7 @@ class GramServer:
             try:
                 with torch.cuda.device(self.device):
                     out_host, keep = _solve_on_stream(h.req, self.precision, self.device, stream,
-                                                      self.chunk_cells)
+                                                      self.chunk_cells, self._staging_for(stream))
                     ev = torch.cuda.Event()
                     ev.record(stream)
             except Exception as e:
@@ -440,6 +446,16 @@ class GramServer:
             self.peak_inflight = max(self.peak_inflight, len(self._inflight))
             self.peak_bytes = max(self.peak_bytes, self._used)
 
+    def _staging_for(self, stream):
+        def get(nbytes):
+            buf = self._staging[id(stream)]
+            if buf is None or buf.numel() < nbytes:
+                size = 1 << max(20, (int(nbytes) - 1).bit_length())
+                buf = torch.empty(size, dtype=torch.uint8, pin_memory=True)
+                self._staging[id(stream)] = buf
+            return buf[:nbytes]
+        return get
+
     def _reap(self):
         still = []
         for f in self._inflight:
@@ -448,7 +464,8 @@ class GramServer:
                 self._free_streams.append(f.stream)
                 f.keep = None
                 for h, host in zip(f.handles, f.out_hosts):
-                    h._finish(result=host)
+                    # results staged in the stream's pinned buffer are copied out before it is reused
+                    h._finish(result=host.clone())
             else:
                 still.append(f)
         self._inflight = still
