@@ -15,6 +15,7 @@ struct StreamIncParams;
 struct TcImageParams;
 struct TcGemmParams;
 struct TcRaggedImageParams;
+struct DgemmIncParams;
 }
 struct CUtensorMap_st; // cuda.h
 namespace sigk {
@@ -28,6 +29,7 @@ using RaggedDeltaFn = void (*)(const void *, const int64_t *, const int64_t *, c
 using StreamIncFn = void (*)(StreamIncParams);
 using TcImageFn = void (*)(TcImageParams);
 using TcRaggedImageFn = void (*)(TcRaggedImageParams);
+using DgemmIncFn = void (*)(DgemmIncParams);
 using TcGemmFn = void (*)(TcGemmParams, CUtensorMap_st);
 using DeltaFn = void (*)(const void *, int64_t, int64_t, int64_t, int64_t, double, const void *, void *);
 
@@ -56,6 +58,9 @@ constexpr int kTcBN = 256;
 TcImageFn get_tc_image_kernel(bool in64);
 TcGemmFn get_tc_gemm_kernel();
 TcRaggedImageFn get_tc_ragged_image_kernel(bool in64);
-StreamIncFn get_stream_inc_kernel(bool f64cells, int R, int O);
+// float64 increment matrix on the CUDA cores (dgemm_inc.cuh)
+DgemmIncFn get_dgemm_inc_kernel();
+// mat64: the increment matrix holds float64 (dgemm_inc_kernel) instead of float32 (tensor cores)
+StreamIncFn get_stream_inc_kernel(bool f64cells, int R, int O, bool mat64);
 
 } // namespace sigk

@@ -30,9 +30,11 @@ PairFn by_r(int R, int O)
 PairFn get_pair_kernel_f64(bool in64, int mode, int R, int O)
 {
     if (in64) {
+        if (mode == kPairMat64) return by_r<double, kPairMat64>(R, O);
         if (mode == kPairMat) return by_r<double, kPairMat>(R, O);
         return mode == kPairGiven ? by_r<double, kPairGiven>(R, O) : by_r<double, kPairDelta>(R, O);
     }
+    if (mode == kPairMat64) return by_r<float, kPairMat64>(R, O);
     if (mode == kPairMat) return by_r<float, kPairMat>(R, O);
     return mode == kPairGiven ? by_r<float, kPairGiven>(R, O) : by_r<float, kPairDelta>(R, O);
 }

@@ -1,40 +1,44 @@
 // Instantiations of the tensor-core increment kernels (tc.cuh).
 #include "dispatch.h"
+#include "dgemm_inc.cuh"
 #include "tc.cuh"
 
 namespace sigk {
 namespace {
-template <typename T, int R>
+template <typename T, int R, typename TM>
 StreamIncFn inc_by_o(int O)
 {
     switch (O) {
-    case 0: return stream_inc_kernel<T, R, 0>;
-    case 1: return stream_inc_kernel<T, R, 1>;
-    case 2: return stream_inc_kernel<T, R, 2>;
-    case 3: return stream_inc_kernel<T, R, 3>;
-    default: return stream_inc_kernel<T, R, 4>;
+    case 0: return stream_inc_kernel<T, R, 0, TM>;
+    case 1: return stream_inc_kernel<T, R, 1, TM>;
+    case 2: return stream_inc_kernel<T, R, 2, TM>;
+    case 3: return stream_inc_kernel<T, R, 3, TM>;
+    default: return stream_inc_kernel<T, R, 4, TM>;
     }
 }
-template <typename T>
+template <typename T, typename TM>
 StreamIncFn inc_by_r(int R, int O)
 {
     switch (R) {
-    case 2: return inc_by_o<T, 2>(O);
-    case 4: return inc_by_o<T, 4>(O);
-    case 8: return inc_by_o<T, 8>(O);
-    default: return inc_by_o<T, 16>(O);
+    case 2: return inc_by_o<T, 2, TM>(O);
+    case 4: return inc_by_o<T, 4, TM>(O);
+    case 8: return inc_by_o<T, 8, TM>(O);
+    default: return inc_by_o<T, 16, TM>(O);
     }
 }
 } // namespace
 
-StreamIncFn get_stream_inc_kernel(bool f64cells, int R, int O)
+StreamIncFn get_stream_inc_kernel(bool f64cells, int R, int O, bool mat64)
 {
-    return f64cells ? inc_by_r<double>(R, O) : inc_by_r<float>(R, O);
+    if (mat64) return inc_by_r<double, double>(R, O);
+    return f64cells ? inc_by_r<double, float>(R, O) : inc_by_r<float, float>(R, O);
 }
 
 TcImageFn get_tc_image_kernel(bool in64) { return in64 ? tc_image_kernel<double> : tc_image_kernel<float>; }
 
 TcGemmFn get_tc_gemm_kernel() { return tc_gemm_kernel<kTcBN>; }
+
+DgemmIncFn get_dgemm_inc_kernel() { return dgemm_inc_kernel<kDgTile>; }
 
 TcRaggedImageFn get_tc_ragged_image_kernel(bool in64)
 {

@@ -23,6 +23,7 @@
 #include "stream.cuh"
 #include "tc.cuh"
 #include "norm_pipe.cuh"
+#include "dgemm_inc.cuh"
 
 namespace sigk {
 namespace {
@@ -469,6 +470,84 @@ int tc_gemm(const TcGemmParams &gp, cudaStream_t stream)
     return e == cudaSuccess ? SIGK_OK : cuda_fail(e, "tensor-core GEMM launch");
 }
 
+
+// The wavefront over one chunk of x paths [i0, i1) reading an increment matrix
+// (out[n * ld + m], float32 from the tensor cores or float64 from
+// dgemm_inc_kernel): the streaming kernel for single-band pairs with enough
+// column blocks, else one pair per warp.
+int consume_matrix(const TcPlan &t, int op, const void *mat, bool mat64, int64_t ld, const unsigned *err, int64_t i0,
+                   int64_t i1, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, int64_t d, int order, void *out,
+                   int64_t out_ld, bool in64, int precision, int dtype, unsigned char *wsb, cudaStream_t stream)
+{
+    int st;
+    const int64_t nxc = i1 - i0;
+    int64_t item0, nitems;
+    if (op == kOpPairwise) {
+        item0 = i0;
+        nitems = nxc;
+    } else if (op == kOpGram) {
+        item0 = i0 * ny;
+        nitems = nxc * ny;
+    } else {
+        item0 = i0 * (i0 + 1) / 2;
+        nitems = i1 * (i1 + 1) / 2 - item0;
+    }
+    if (!t.stream) { // several bands or few column blocks: one pair per warp reading the matrix
+        PairParams p{};
+        p.op = op;
+        p.nx = nx;
+        p.ny = ny;
+        p.ncx = ncx;
+        p.ncy = ncy;
+        p.d = d;
+        p.order = order;
+        p.fscale = 1.0;
+        p.out = out;
+        p.out_ld = out_ld;
+        p.nitems = nitems;
+        p.item0 = item0;
+        p.mat = mat;
+        p.mat_err = err;
+        p.mat_ld = ld;
+        p.mat_rows_x = t.rows_x;
+        p.x0 = i0;
+        p.bnd = t.nbands > 1 ? wsb + t.bnd_off : nullptr;
+        p.bnd_stride = t.bnd_stride;
+        PairFn pfn = pick_pair(precision, dtype, mat64 ? kPairMat64 : kPairMat, t.R, t.O);
+        return launch(pfn, p, p.nitems, 0, stream);
+    }
+    const bool f64 = cell_prec(precision) == SIGK_PREC_FP64;
+    StreamIncFn fn = get_stream_inc_kernel(f64, t.R, t.O, mat64);
+    int nb = 0;
+    if ((st = blocks_per_sm((const void *)fn, 0, &nb))) return st;
+    const int64_t warps = (int64_t)sm_count() * nb * kWarpsPerBlock;
+    StreamIncParams sp{};
+    sp.op = op;
+    sp.in64 = in64;
+    sp.inc = mat;
+    sp.ld = ld;
+    sp.rows_x = t.rows_x;
+    sp.x0 = i0;
+    sp.nx = nx;
+    sp.ny = ny;
+    sp.ncx = ncx;
+    sp.ncy = ncy;
+    sp.order = order;
+    sp.out = out;
+    sp.out_ld = out_ld;
+    sp.err = err;
+    sp.item0 = item0;
+    sp.nitems = nitems;
+    const int64_t nw = warps < nitems ? warps : nitems;
+    sp.per_warp = (nitems + nw - 1) / nw;
+    const int64_t used = (nitems + sp.per_warp - 1) / sp.per_warp;
+    const int64_t blocks = (used + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    fn<<<(unsigned)blocks, kWarpsPerBlock * 32, 0, stream>>>(sp);
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? SIGK_OK : cuda_fail(e, "stream increment kernel launch");
+}
+
 int run_pairs_tc(const TcPlan &t, int op, const void *x, const void *y, int64_t nx, int64_t ny, int64_t lx, int64_t ly,
                  int64_t d, int dtype, int order, double static_scale, const void *sx, const void *sy, void *out,
                  int64_t out_ld, int precision, void *ws, cudaStream_t stream)
@@ -495,12 +574,6 @@ int run_pairs_tc(const TcPlan &t, int op, const void *x, const void *y, int64_t 
                            b_hi, b_lo, stream)))
             return st;
     }
-    const bool f64 = cell_prec(precision) == SIGK_PREC_FP64;
-    StreamIncFn fn = t.stream ? get_stream_inc_kernel(f64, t.R, t.O) : nullptr;
-    PairFn pfn = t.stream ? nullptr : pick_pair(precision, dtype, kPairMat, t.R, t.O);
-    int nb = 0;
-    if (fn && (st = blocks_per_sm((const void *)fn, 0, &nb))) return st;
-    const int64_t warps = (int64_t)sm_count() * nb * kWarpsPerBlock;
 
     for (int64_t c = 0; c < t.nchunks; ++c) {
         const int64_t i0 = c * t.chunk, i1 = (i0 + t.chunk < nx) ? i0 + t.chunk : nx, nxc = i1 - i0;
@@ -538,63 +611,121 @@ int run_pairs_tc(const TcPlan &t, int op, const void *x, const void *y, int64_t 
         gp.err = err;
         if ((st = tc_gemm(gp, stream))) return st;
 
-        StreamIncParams sp{};
-        sp.op = op;
-        sp.in64 = in64;
-        sp.inc = ct;
-        sp.ld = gp.ld;
-        sp.rows_x = t.rows_x;
-        sp.x0 = i0;
-        sp.nx = nx;
-        sp.ny = ny;
-        sp.ncx = ncx;
-        sp.ncy = ncy;
-        sp.order = order;
-        sp.out = out;
-        sp.out_ld = out_ld;
-        sp.err = err;
-        if (op == kOpPairwise) {
-            sp.item0 = i0;
-            sp.nitems = nxc;
-        } else if (op == kOpGram) {
-            sp.item0 = i0 * ny;
-            sp.nitems = nxc * ny;
-        } else {
-            sp.item0 = i0 * (i0 + 1) / 2;
-            sp.nitems = i1 * (i1 + 1) / 2 - sp.item0;
-        }
-        if (!t.stream) { // several bands or few column blocks: one pair per warp reading the matrix
-            PairParams p{};
-            p.op = op;
-            p.nx = nx;
-            p.ny = ny;
-            p.ncx = ncx;
-            p.ncy = ncy;
-            p.d = d;
-            p.order = order;
-            p.fscale = 1.0;
-            p.out = out;
-            p.out_ld = out_ld;
-            p.nitems = sp.nitems;
-            p.item0 = sp.item0;
-            p.mat = ct;
-            p.mat_err = err;
-            p.mat_ld = gp.ld;
-            p.mat_rows_x = t.rows_x;
-            p.x0 = i0;
-            p.bnd = t.nbands > 1 ? wsb + t.bnd_off : nullptr;
-            p.bnd_stride = t.bnd_stride;
-            if ((st = launch(pfn, p, p.nitems, 0, stream))) return st;
-            continue;
-        }
-        int64_t nw = warps < sp.nitems ? warps : sp.nitems;
-        sp.per_warp = (sp.nitems + nw - 1) / nw;
-        const int64_t used = (sp.nitems + sp.per_warp - 1) / sp.per_warp;
-        const int64_t blocks = (used + kWarpsPerBlock - 1) / kWarpsPerBlock;
-        fn<<<(unsigned)blocks, kWarpsPerBlock * 32, 0, stream>>>(sp);
+        if ((st = consume_matrix(t, op, ct, false, gp.ld, err, i0, i1, nx, ny, ncx, ncy, d, order, out, out_ld,
+                                 in64, precision, dtype, wsb, stream)))
+            return st;
+    }
+    return SIGK_OK;
+}
+
+
+// ------------------------------------------------------------------ float64 increment matrix
+// fp64 mode, Gram ops, dim >= kDgMinDim: the increments of all pairs from one
+// FP64 GEMM on the CUDA cores (dgemm_inc.cuh), then the wavefront reads them;
+// bitwise the results of the fused kernels, faster when the d FMAs per coarse
+// cell dominate.  Workspace: a zero word (the consumers' error flag), boundary
+// rows, the scaled differences of both sides, the matrix (x paths in chunks of
+// at most kTcChunkBytes).
+constexpr int kDgMinDim = 16;
+
+TcPlan make_mat64_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, int64_t d, int order)
+{
+    TcPlan t{};
+    if (op == kOpPairwise || d < kDgMinDim || env_flag("SIGK_NO_DGEMM_INC")) return t;
+    const int64_t n = ncx << order, m = ncy << order;
+    const int C = order >= 4 ? 8 : (1 << order);
+    const int Rs = pick_rows(n);
+    t.ok = true;
+    t.stream = n <= 32 * Rs && m / C >= 32;
+    t.R = Rs;
+    t.O = order >= 4 ? 4 : order;
+    t.nbands = (int)((n + 32 * Rs - 1) / (32 * Rs));
+    size_t bnd_bytes = 0;
+    if (!t.stream && t.nbands > 1) {
+        t.bnd_stride = ((m + 1 + 31) / 32) * 32;
+        bnd_bytes = align256((size_t)warp_cap() * (size_t)t.bnd_stride * sizeof(double));
+    }
+    t.rows_x = (ncx + 3) / 4 * 4;
+    t.rows_y = ncy;
+    const int64_t ny_paths = op == kOpGram ? ny : nx;
+    const size_t per_x = (size_t)t.rows_x * (size_t)(ny_paths * ncy) * sizeof(double);
+    int64_t chunk = (int64_t)(tc_chunk_cap() / per_x);
+    if (chunk < 1) chunk = 1;
+    if (chunk > nx) chunk = nx;
+    t.chunk = chunk;
+    t.nchunks = (nx + chunk - 1) / chunk;
+    t.err_off = 0;
+    t.bnd_off = 256;
+    t.a_off = t.bnd_off + bnd_bytes;                                     // x differences
+    t.b_off = t.a_off + align256((size_t)nx * ncx * d * sizeof(double)); // y differences
+    t.ct_off = t.b_off + align256((size_t)ny_paths * ncy * d * sizeof(double));
+    t.ws_bytes = t.ct_off + align256((size_t)chunk * per_x);
+    return t;
+}
+
+int run_pairs_mat64(const TcPlan &t, int op, const void *x, const void *y, int64_t nx, int64_t ny, int64_t lx,
+                    int64_t ly, int64_t d, int dtype, int order, double static_scale, const void *sx, const void *sy,
+                    void *out, int64_t out_ld, int precision, void *ws, cudaStream_t stream)
+{
+    int st;
+    const bool in64 = dtype == SIGK_F64;
+    const int64_t ncx = lx - 1, ncy = ly - 1;
+    unsigned char *wsb = reinterpret_cast<unsigned char *>(ws);
+    unsigned *err = reinterpret_cast<unsigned *>(wsb + t.err_off);
+    double *dx = reinterpret_cast<double *>(wsb + t.a_off);
+    double *dy = reinterpret_cast<double *>(wsb + t.b_off);
+    double *mat = reinterpret_cast<double *>(wsb + t.ct_off);
+    cudaError_t e = cudaMemsetAsync(err, 0, sizeof(unsigned), stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+    // scaled differences, as the fused path: static scale * 4^-order * scale_x on x, scale_y on y
+    // (the symmetric Gram: both from x, scale_x on each side)
+    DeltaFn delta = get_delta_kernel(true, in64);
+    auto run_delta = [&](const void *src, int64_t npaths, int64_t len, double f, const void *sc, double *dst) -> int {
+        const int64_t total = npaths * (len - 1) * d;
+        int64_t blocks = (total + 255) / 256;
+        if (blocks > (int64_t)sm_count() * 8) blocks = (int64_t)sm_count() * 8;
+        delta<<<(unsigned)blocks, 256, 0, stream>>>(src, npaths, len, d, d, f, sc, dst);
+        count_launch();
+        cudaError_t e2 = cudaGetLastError();
+        return e2 == cudaSuccess ? SIGK_OK : cuda_fail(e2, "delta kernel launch");
+    };
+    const double fs = static_scale * std::ldexp(1.0, -2 * order);
+    const bool sym = op == kOpGramSym;
+    if ((st = run_delta(x, nx, lx, fs, sx, dx))) return st;
+    if (sym) {
+        if (fs == 1.0)
+            dy = dx;
+        else if ((st = run_delta(x, nx, lx, 1.0, sx, dy)))
+            return st;
+    } else if ((st = run_delta(y, ny, ly, 1.0, sy, dy))) {
+        return st;
+    }
+    for (int64_t c = 0; c < t.nchunks; ++c) {
+        const int64_t i0 = c * t.chunk, i1 = (i0 + t.chunk < nx) ? i0 + t.chunk : nx, nxc = i1 - i0;
+        DgemmIncParams gp{};
+        gp.dx = dx + i0 * d * ncx;
+        gp.dy = dy;
+        gp.npaths_x = nxc;
+        gp.ncx = ncx;
+        gp.rows_x = t.rows_x;
+        gp.npaths_y = sym ? i1 : ny;
+        gp.ncy = ncy;
+        gp.d = d;
+        gp.mode = sym ? kTcLower : kTcAll;
+        gp.x0 = i0;
+        gp.out = mat;
+        gp.ld = nxc * t.rows_x;
+        const int64_t mt = (gp.ld + kDgTile - 1) / kDgTile;
+        int64_t nt = (gp.npaths_y * ncy + kDgTile - 1) / kDgTile;
+        if (nt > 65535) nt = 65535;
+        if (mt > 0x7fffffffLL) return fail(SIGK_EUNSUPPORTED, "increment matrix too large");
+        get_dgemm_inc_kernel()<<<dim3((unsigned)mt, (unsigned)nt), 256, 0, stream>>>(gp);
         count_launch();
         e = cudaGetLastError();
-        if (e != cudaSuccess) return cuda_fail(e, "stream increment kernel launch");
+        if (e != cudaSuccess) return cuda_fail(e, "float64 increment GEMM launch");
+        if ((st = consume_matrix(t, op, mat, true, gp.ld, err, i0, i1, nx, ny, ncx, ncy, d, order, out, out_ld, in64,
+                                 precision, dtype, wsb, stream)))
+            return st;
     }
     return SIGK_OK;
 }
@@ -623,6 +754,16 @@ int run_pairs(int op, const void *x, const void *y, int64_t nx, int64_t ny, int6
                                 precision, ws, stream);
         }
         precision = cell_prec(precision); // shapes outside the TC plan: CUDA-core increments, same cells
+    }
+    if (precision == SIGK_PREC_FP64) {
+        TcPlan t = make_mat64_plan(op, nx, ny, lx - 1, ly - 1, d, order);
+        if (t.ok) {
+            if (!ws || ws_bytes < t.ws_bytes)
+                return fail(SIGK_ENOMEM, "workspace of %zu bytes needed (got %zu)", t.ws_bytes, ws ? ws_bytes : 0);
+            if (((uintptr_t)ws & 255) != 0) return fail(SIGK_EINVAL, "workspace must be 256-byte aligned");
+            return run_pairs_mat64(t, op, x, y, nx, ny, lx, ly, d, dtype, order, static_scale, sx, sy, out, out_ld,
+                                   precision, ws, stream);
+        }
     }
     const size_t ts = tsize_of(precision);
     const int64_t nitems = op == kOpPairwise ? nx : (op == kOpGram ? nx * ny : nx * (nx + 1) / 2);
@@ -834,6 +975,12 @@ size_t sigk_workspace_size(int op, int64_t n_x, int64_t n_y, int64_t len_x, int6
     if (op == SIGK_OP_NORMALIZE) return norm_plan(n_x, len_x - 1, dim > 0 ? dim : 1, order, dim == 0).ws_bytes;
     if (is_tc(precision) && dim > 0) {
         TcPlan t = make_tc_plan(op, n_x, n_y, len_x - 1, len_y - 1, dim, order, tsize_of(precision));
+        if (t.ok) return t.ws_bytes;
+        precision = cell_prec(precision); // as the entry points: CUDA-core increments, same cells
+    }
+    if (precision == SIGK_PREC_FP64 && dim > 0) {
+        const int kop = op == SIGK_OP_PAIRWISE ? kOpPairwise : op == SIGK_OP_GRAM ? kOpGram : kOpGramSym;
+        TcPlan t = make_mat64_plan(kop, n_x, n_y, len_x - 1, len_y - 1, dim, order);
         if (t.ok) return t.ws_bytes;
     }
     // dim == 0 selects the plan of the *_inc entry points (no dx staging)

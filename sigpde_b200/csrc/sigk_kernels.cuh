@@ -10,6 +10,8 @@
 // x_i and read neighbouring y_j (L1/L2 reuse).
 #pragma once
 
+#include <type_traits>
+
 #include "wave.cuh"
 
 namespace sigk {
@@ -36,7 +38,7 @@ struct PairParams {
     // matrix mode (tensor-core increments, tc.cuh): pair (xi, yj)'s increments start at
     // mat + yj * ncy * mat_ld + (xi - x0) * mat_rows_x (Gram ops; pairwise: mat + (item - item0) * ncy *
     // mat_rows_x), mat_ld (pairwise: mat_rows_x) floats per coarse column
-    const float *mat;
+    const void *mat;         // float (tensor-core increments) or double (dgemm_inc_kernel) elements
     const unsigned *mat_err; // non-zero: the GEMM gave up a wait, the matrix is incomplete (results NaN)
     int64_t mat_ld, mat_rows_x, x0;
     int64_t item0;      // first item of this launch (matrix mode works in chunks of x paths)
@@ -64,7 +66,7 @@ __device__ __forceinline__ double scale_at(const void *s, int64_t i)
     return s ? (double)reinterpret_cast<const TIN *>(s)[i] : 1.0;
 }
 
-enum : int { kPairDelta = 0, kPairGiven = 1, kPairMat = 2 };
+enum : int { kPairDelta = 0, kPairGiven = 1, kPairMat = 2, kPairMat64 = 3 };
 
 template <typename T, typename TIN, int R, int O, int MODE>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) pair_kernel(PairParams p)
@@ -96,17 +98,19 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) pair_kernel(PairParams p)
         if (p.sy) s *= scale_at<TIN>(p.sy, yj);
 
         T val;
-        if constexpr (MODE == kPairMat) {
-            MatIncs<T, BS::RC> src;
+        if constexpr (MODE == kPairMat || MODE == kPairMat64) {
+            using TM = typename std::conditional<MODE == kPairMat64, double, float>::type;
+            MatIncs<T, BS::RC, TM> src;
+            const TM *mat = reinterpret_cast<const TM *>(p.mat);
             if (p.op == kOpPairwise) {
-                src.base = p.mat + (item - p.item0) * p.ncy * p.mat_rows_x;
+                src.base = mat + (item - p.item0) * p.ncy * p.mat_rows_x;
                 src.ld = p.mat_rows_x;
             } else {
-                src.base = p.mat + yj * p.ncy * p.mat_ld + (xi - p.x0) * p.mat_rows_x;
+                src.base = mat + yj * p.ncy * p.mat_ld + (xi - p.x0) * p.mat_rows_x;
                 src.ld = p.mat_ld;
             }
             src.ncy = p.ncy;
-            val = (*p.mat_err == 0) ? warp_solve<T, R, O>(g, src, bnd) : T(NAN);
+            val = (p.mat_err == nullptr || *p.mat_err == 0) ? warp_solve<T, R, O>(g, src, bnd) : T(NAN);
         } else if constexpr (MODE == kPairGiven) {
             GivenIncs<T, TIN, BS::RC> src;
             const TIN *base = reinterpret_cast<const TIN *>(p.inc);

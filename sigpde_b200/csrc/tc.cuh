@@ -585,7 +585,7 @@ __host__ __forceinline__ size_t tc_gemm_smem(int bn, int kp)
 struct StreamIncParams {
     int op;           // kOpPairwise / kOpGram / kOpGramSym
     int in64;         // output dtype
-    const float *inc; // increment matrix (see tc_gemm_kernel)
+    const void *inc;  // increment matrix (see tc_gemm_kernel, dgemm_inc_kernel), TM elements
     int64_t ld;       // Gram ops: floats between rows cj of the matrix
     int64_t rows_x;   // rows per x path in the matrix (ncx rounded up to 4)
     int64_t x0;       // first x path of this chunk (Gram ops)
@@ -600,32 +600,7 @@ struct StreamIncParams {
     const unsigned *err; // non-zero: the GEMM gave up a wait; results are NaN
 };
 
-// The lane's RC coarse rows at coarse column cj of the pair's block: RC
-// consecutive floats (vector loads, 16-byte aligned because rows_x, ld and
-// the lane's first row are multiples of 4 when RC >= 4).
-template <typename T, int RC>
-__device__ __forceinline__ void load_incs(const float *row, int ci0, int ncx, T (&c)[RC])
-{
-    if constexpr (RC == 1) {
-        c[0] = ci0 < ncx ? T(row[ci0]) : T(0);
-    } else if constexpr (RC == 2) {
-        float2 v = ci0 < ncx ? *reinterpret_cast<const float2 *>(row + ci0) : make_float2(0.f, 0.f);
-        c[0] = T(v.x);
-        c[1] = T(v.y);
-    } else {
-#pragma unroll
-        for (int q = 0; q < RC / 4; ++q) {
-            float4 v = (ci0 + 4 * q < ncx) ? *reinterpret_cast<const float4 *>(row + ci0 + 4 * q)
-                                           : make_float4(0.f, 0.f, 0.f, 0.f);
-            c[4 * q + 0] = T(v.x);
-            c[4 * q + 1] = T(v.y);
-            c[4 * q + 2] = T(v.z);
-            c[4 * q + 3] = T(v.w);
-        }
-    }
-}
-
-template <typename T, int R, int O>
+template <typename T, int R, int O, typename TM>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_inc_kernel(StreamIncParams p)
 {
     using BS = BlockShape<R, O>;
@@ -668,7 +643,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_inc_kernel(StreamI
     T corner_next = T(1);
     int q = 0, k = 0;
     int64_t item = 0, xi = 0, yj = 0;
-    const float *base = p.inc;
+    const TM *inc = reinterpret_cast<const TM *>(p.inc);
+    const TM *base = inc;
     const int total = cnt * nsteps + 31;
     for (int s = 0; s < total; ++s) {
         T top[C];
@@ -682,19 +658,19 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_inc_kernel(StreamI
             if (q == 0) {
                 item = p.item0 + first + k;
                 stream_decode(sp, item, xi, yj);
-                base = p.op == kOpPairwise ? p.inc + (item - p.item0) * (int64_t)ncy * p.rows_x
-                                           : p.inc + yj * (int64_t)ncy * p.ld + (xi - p.x0) * p.rows_x;
+                base = p.op == kOpPairwise ? inc + (item - p.item0) * (int64_t)ncy * p.rows_x
+                                           : inc + yj * (int64_t)ncy * p.ld + (xi - p.x0) * p.rows_x;
 #pragma unroll
                 for (int r = 0; r < R; ++r) left[r] = T(1);
             }
             const T corner = (q == 0) ? T(1) : corner_next;
             corner_next = top[C - 1];
             const int cj = (O <= 3) ? q : ((q * C) >> p.order);
-            float cur[RC];
-            load_incs<float, RC>(base + (int64_t)cj * row_ld, ci0, ncx, cur);
+            T cur[RC];
+            load_mat_vals<T, TM, RC>(base + (int64_t)cj * row_ld, ci0, ncx, cur);
             T A[RC], B[RC];
 #pragma unroll
-            for (int rc = 0; rc < RC; ++rc) stencil_coefs(T(cur[rc]), A[rc], B[rc]);
+            for (int rc = 0; rc < RC; ++rc) stencil_coefs(cur[rc], A[rc], B[rc]);
             stream_block<T, R, O>(left, top, corner, A, B, bot);
             if (q == nsteps - 1 && lane == lstar) stream_store(sp, item, xi, yj, pick_row(left, rstar));
             if (++q == nsteps) {

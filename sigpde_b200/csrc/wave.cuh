@@ -119,9 +119,42 @@ __device__ __forceinline__ void prefetch_l2(const void *p)
     asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
-template <typename T, int RC>
+// RC consecutive values row[ci0 .. ci0+RC) of a float or double matrix as T,
+// with 16-byte vector loads (the caller keeps rows and ci0 aligned); chunks
+// starting at or beyond ncx read as 0.
+template <typename T, typename TM, int RC>
+__device__ __forceinline__ void load_mat_vals(const TM *row, int ci0, int ncx, T (&c)[RC])
+{
+    if constexpr (RC == 1) {
+        c[0] = ci0 < ncx ? T(row[ci0]) : T(0);
+    } else if constexpr (sizeof(TM) == 8) {
+#pragma unroll
+        for (int q = 0; q < RC / 2; ++q) {
+            const double2 v = (ci0 + 2 * q < ncx) ? *reinterpret_cast<const double2 *>(row + ci0 + 2 * q)
+                                                  : make_double2(0.0, 0.0);
+            c[2 * q + 0] = T(v.x);
+            c[2 * q + 1] = T(v.y);
+        }
+    } else if constexpr (RC == 2) {
+        const float2 v = ci0 < ncx ? *reinterpret_cast<const float2 *>(row + ci0) : make_float2(0.f, 0.f);
+        c[0] = T(v.x);
+        c[1] = T(v.y);
+    } else {
+#pragma unroll
+        for (int q = 0; q < RC / 4; ++q) {
+            const float4 v = (ci0 + 4 * q < ncx) ? *reinterpret_cast<const float4 *>(row + ci0 + 4 * q)
+                                                 : make_float4(0.f, 0.f, 0.f, 0.f);
+            c[4 * q + 0] = T(v.x);
+            c[4 * q + 1] = T(v.y);
+            c[4 * q + 2] = T(v.z);
+            c[4 * q + 3] = T(v.w);
+        }
+    }
+}
+
+template <typename T, int RC, typename TM = float>
 struct MatIncs {
-    const float *base;
+    const TM *base;
     int64_t ld, ncy;
     int ci0 = 0, ncx = 0;
     __device__ __forceinline__ void stage(int64_t ci0_, int64_t ncx_, int, bool)
@@ -131,25 +164,9 @@ struct MatIncs {
     }
     __device__ __forceinline__ void column(int64_t cj, int, T (&c)[RC]) const
     {
-        const float *row = base + cj * ld;
+        const TM *row = base + cj * ld;
         if (cj + kIncPrefetch < ncy && ci0 < ncx) prefetch_l2(row + kIncPrefetch * ld + ci0);
-        if constexpr (RC == 1) {
-            c[0] = ci0 < ncx ? T(row[ci0]) : T(0);
-        } else if constexpr (RC == 2) {
-            const float2 v = ci0 < ncx ? *reinterpret_cast<const float2 *>(row + ci0) : make_float2(0.f, 0.f);
-            c[0] = T(v.x);
-            c[1] = T(v.y);
-        } else {
-#pragma unroll
-            for (int q = 0; q < RC / 4; ++q) {
-                const float4 v = (ci0 + 4 * q < ncx) ? *reinterpret_cast<const float4 *>(row + ci0 + 4 * q)
-                                                     : make_float4(0.f, 0.f, 0.f, 0.f);
-                c[4 * q + 0] = T(v.x);
-                c[4 * q + 1] = T(v.y);
-                c[4 * q + 2] = T(v.z);
-                c[4 * q + 3] = T(v.w);
-            }
-        }
+        load_mat_vals<T, TM, RC>(row, ci0, ncx, c);
     }
 };
 

@@ -325,6 +325,26 @@ def test_robust_normalization_increment_sources(sig, oracle, L, d, order, monkey
     np.testing.assert_array_equal(host(rk.normalization(X)), lam)
 
 
+@pytest.mark.parametrize("shape", [(7, 6, 40, 16, 2), (9, 9, 64, 32, 0), (5, 4, 300, 24, 1), (6, 6, 12, 16, 4)])
+def test_fp64_wide_paths_use_a_float64_increment_matrix(sig, oracle, shape, monkeypatch):
+    """fp64 Grams with d >= 16 first write the float64 increments of all pairs with one GEMM on the
+    CUDA cores and the wavefront reads them; each increment is summed in the fused kernels' order, so
+    the results are bitwise those of the fused path (SIGK_NO_DGEMM_INC=1), and meet the fp64 bound."""
+    nx, ny, L, d, o = shape
+    X = cuda(oracle.brownian(nx, L, d, 71 + L), torch.float64)
+    Y = cuda(oracle.brownian(ny, L + 7, d, 72 + L), torch.float64)
+    s = cuda(np.linspace(0.6, 1.4, nx), torch.float64)
+    k = sig.SigPDE(sig.kernels.LinearKernel(1.3), o)
+    got = [host(k.gram(X, Y)), host(k.gram(X)), host(k.gram(X, None, s))]
+    monkeypatch.setenv("SIGK_NO_DGEMM_INC", "1")
+    fused = [host(k.gram(X, Y)), host(k.gram(X)), host(k.gram(X, None, s))]
+    for a, b in zip(got, fused):
+        np.testing.assert_array_equal(a, b)
+    x, y = host(X) * np.sqrt(1.3), host(Y) * np.sqrt(1.3)
+    assert_rel(got[0], oracle.gram(x, y, o), RTOL64, "gram")
+    assert_rel(got[1], oracle.gram(x, None, o), RTOL64, "sym")
+
+
 def test_robust_normalization_alternating_shared_memory_sizes(sig, oracle):
     """One kernel instance launched with large, then smaller, then large
     shared-memory tiles (the per-function opt-in must cover all of them)."""
