@@ -34,7 +34,7 @@ struct DgemmIncParams {
 };
 
 template <int TILE = kDgTile>
-__global__ void __launch_bounds__(256) dgemm_inc_kernel(DgemmIncParams p)
+__global__ void __launch_bounds__(256, 3) dgemm_inc_kernel(DgemmIncParams p)
 {
     static_assert(TILE == 64, "4x4 outputs per thread of a 16x16 block");
     __shared__ double As[kDgK][TILE + 1];
@@ -53,18 +53,24 @@ __global__ void __launch_bounds__(256) dgemm_inc_kernel(DgemmIncParams p)
         for (int i = 0; i < 4; ++i)
 #pragma unroll
             for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+        // this thread stages row mm = threadIdx.x % 64 of the A and B tiles (K rows threadIdx.x / 64 + 4r):
+        // its path and cell are fixed for the tile, so the divisions happen once
+        const int mm = threadIdx.x & (TILE - 1), kq = threadIdx.x / TILE;
+        const int64_t m = m0 + mm, n = n0 + mm;
+        const int64_t px = m / p.rows_x, cx = m - px * p.rows_x;
+        const int64_t qy = n / p.ncy, cy = n - qy * p.ncy;
+        const bool a_ok = px < p.npaths_x && cx < p.ncx, b_ok = qy < p.npaths_y;
+        const double *a_src = p.dx + (a_ok ? px * p.d * p.ncx + cx : 0);
+        const double *b_src = p.dy + (b_ok ? qy * p.d * p.ncy + cy : 0);
         for (int64_t k0 = 0; k0 < p.d; k0 += kDgK) {
             // stage A[m][k] and B[n][k] for k in [k0, k0 + 16): threads run over m (n), which are
             // contiguous within a path in the dimension-major differences
-            for (int e = threadIdx.x; e < kDgK * TILE; e += 256) {
-                const int kk = e / TILE, mm = e - kk * TILE;
+#pragma unroll
+            for (int r = 0; r < kDgK * TILE / 256; ++r) {
+                const int kk = kq + r * (256 / TILE);
                 const int64_t k = k0 + kk;
-                const int64_t m = m0 + mm;
-                const int64_t px = m / p.rows_x, cx = m - px * p.rows_x;
-                As[kk][mm] = (k < p.d && px < p.npaths_x && cx < p.ncx) ? p.dx[(px * p.d + k) * p.ncx + cx] : 0.0;
-                const int64_t n = n0 + mm;
-                const int64_t qy = n / p.ncy, cy = n - qy * p.ncy;
-                Bs[kk][mm] = (k < p.d && qy < p.npaths_y) ? p.dy[(qy * p.d + k) * p.ncy + cy] : 0.0;
+                As[kk][mm] = (a_ok && k < p.d) ? a_src[k * p.ncx] : 0.0;
+                Bs[kk][mm] = (b_ok && k < p.d) ? b_src[k * p.ncy] : 0.0;
             }
             __syncthreads();
             const int kn = (int)((p.d - k0) < kDgK ? (p.d - k0) : kDgK);
