@@ -25,7 +25,8 @@
 //                       cp.async.bulk.tensor, to HBM);
 //   stream_inc_kernel   the streaming wavefront of stream.cuh reading its
 //                       increments from that matrix (vector loads of the
-//                       lane's coarse rows) instead of forming dot products.
+//                       lane's coarse rows, or for long steps a cp.async ring
+//                       two steps ahead) instead of forming dot products.
 #pragma once
 
 #include <cuda.h> // CUtensorMap
@@ -582,6 +583,84 @@ __host__ __forceinline__ size_t tc_gemm_smem(int bn, int kp)
 }
 
 // ------------------------------------------------------------------ wavefront
+// Prefetch ring of stream_inc_kernel: each lane keeps the matrix values of its
+// next PF steps in flight as cp.async copies into its own shared-memory slots
+// (zero-filled where the lane's coarse rows start at or beyond ncx, as
+// load_mat_vals reads them), so a step waits for a copy issued PF steps
+// earlier rather than for a fresh global load.  Only the issuing lane reads a
+// slot, after cp.async.wait_group has made its copy visible to it.
+constexpr int kIncRingLaneBytes = 160; // shared memory per lane for the ring
+
+template <typename TM, int RC, int CELLS>
+struct IncRing {
+    static constexpr int VB = RC * (int)sizeof(TM);   // bytes per lane per step
+    static constexpr int CP = VB < 16 ? VB : 16;      // bytes per copy
+    // steps of lead: two for long steps (32 or more cells a lane); shorter steps measured slower
+    // with a ring (its bookkeeping costs more than the load latency it hides there)
+    static constexpr int STEPS = CELLS >= 32 ? 2 : 0;
+    static constexpr int CAP = kIncRingLaneBytes / VB - 1;
+    static constexpr int PF = STEPS < CAP ? STEPS : (CAP > 0 ? CAP : 0); // 0: plain loads (load_mat_vals)
+    static constexpr int SLOTS = PF + 1;
+};
+
+template <int SZ>
+__device__ __forceinline__ void cp_async_zfill(uint32_t dst, const void *src, int src_bytes)
+{
+    if constexpr (SZ == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(dst), "l"(src), "n"(SZ), "r"(src_bytes)
+                     : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Copy the lane's RC values of one matrix row (chunks starting at or beyond
+// ncx are zero-filled without a read) into a ring slot.
+template <typename TM, int RC>
+__device__ __forceinline__ void ring_fill(uint32_t dst, const TM *row, int ci0, int ncx)
+{
+    constexpr int VB = RC * (int)sizeof(TM);
+    constexpr int CP = VB < 16 ? VB : 16;
+    constexpr int EPC = CP / (int)sizeof(TM);
+#pragma unroll
+    for (int q = 0; q < VB / CP; ++q) {
+        const bool ok = ci0 + q * EPC < ncx;
+        cp_async_zfill<CP>(dst + q * CP, ok ? row + ci0 + q * EPC : row, ok ? CP : 0);
+    }
+}
+
+template <typename T, typename TM, int RC>
+__device__ __forceinline__ void ring_read(const unsigned char *src, T (&c)[RC])
+{
+    if constexpr (RC == 1) {
+        c[0] = T(*reinterpret_cast<const TM *>(src));
+    } else if constexpr (sizeof(TM) == 8) {
+#pragma unroll
+        for (int q = 0; q < RC / 2; ++q) {
+            const double2 v = reinterpret_cast<const double2 *>(src)[q];
+            c[2 * q + 0] = T(v.x);
+            c[2 * q + 1] = T(v.y);
+        }
+    } else if constexpr (RC == 2) {
+        const float2 v = *reinterpret_cast<const float2 *>(src);
+        c[0] = T(v.x);
+        c[1] = T(v.y);
+    } else {
+#pragma unroll
+        for (int q = 0; q < RC / 4; ++q) {
+            const float4 v = reinterpret_cast<const float4 *>(src)[q];
+            c[4 * q + 0] = T(v.x);
+            c[4 * q + 1] = T(v.y);
+            c[4 * q + 2] = T(v.z);
+            c[4 * q + 3] = T(v.w);
+        }
+    }
+}
+
 struct StreamIncParams {
     int op;           // kOpPairwise / kOpGram / kOpGramSym
     int in64;         // output dtype
@@ -646,6 +725,43 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_inc_kernel(StreamI
     const TM *inc = reinterpret_cast<const TM *>(p.inc);
     const TM *base = inc;
     const int total = cnt * nsteps + 31;
+
+    // prefetch ring: the copy for the lane's step t + PF is issued at step t
+    using Ring = IncRing<TM, RC, R * C>;
+    constexpr int PF = Ring::PF;
+    __shared__ __align__(16) unsigned char ring_mem[PF > 0 ? kWarpsPerBlock * Ring::SLOTS * 32 * Ring::VB : 16];
+    unsigned char *ring = ring_mem + ((size_t)wib * Ring::SLOTS * 32 + lane) * Ring::VB;
+    constexpr int kSlot = 32 * Ring::VB; // bytes between the slots of one lane
+    int rd = 0, wr = 0;                  // slots to read / fill next
+    int tp = 0, kp = 0, qp = 0;          // step, item and column of the next copy
+    const TM *bp = inc;
+    const int tsteps = cnt * nsteps;
+    auto issue = [&]() {
+        if (tp < tsteps) {
+            if (qp == 0) {
+                int64_t a, b;
+                const int64_t it = p.item0 + first + kp;
+                stream_decode(sp, it, a, b);
+                bp = p.op == kOpPairwise ? inc + (it - p.item0) * (int64_t)ncy * p.rows_x
+                                         : inc + b * (int64_t)ncy * p.ld + (a - p.x0) * p.rows_x;
+            }
+            const int cj = (O <= 3) ? qp : ((qp * C) >> p.order);
+            ring_fill<TM, RC>((uint32_t)__cvta_generic_to_shared(ring + wr * kSlot), bp + (int64_t)cj * row_ld, ci0,
+                              ncx);
+            if (++qp == nsteps) {
+                qp = 0;
+                ++kp;
+            }
+            ++tp;
+        }
+        cp_async_commit(); // empty groups past the end keep the count uniform
+        if (++wr == Ring::SLOTS) wr = 0;
+    };
+    if constexpr (PF > 0) {
+#pragma unroll 1
+        for (int i = 0; i < PF; ++i) issue();
+    }
+
     for (int s = 0; s < total; ++s) {
         T top[C];
 #pragma unroll
@@ -658,16 +774,24 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_inc_kernel(StreamI
             if (q == 0) {
                 item = p.item0 + first + k;
                 stream_decode(sp, item, xi, yj);
-                base = p.op == kOpPairwise ? inc + (item - p.item0) * (int64_t)ncy * p.rows_x
-                                           : inc + yj * (int64_t)ncy * p.ld + (xi - p.x0) * p.rows_x;
+                if constexpr (PF == 0)
+                    base = p.op == kOpPairwise ? inc + (item - p.item0) * (int64_t)ncy * p.rows_x
+                                               : inc + yj * (int64_t)ncy * p.ld + (xi - p.x0) * p.rows_x;
 #pragma unroll
                 for (int r = 0; r < R; ++r) left[r] = T(1);
             }
             const T corner = (q == 0) ? T(1) : corner_next;
             corner_next = top[C - 1];
-            const int cj = (O <= 3) ? q : ((q * C) >> p.order);
             T cur[RC];
-            load_mat_vals<T, TM, RC>(base + (int64_t)cj * row_ld, ci0, ncx, cur);
+            if constexpr (PF > 0) {
+                cp_async_wait<PF - 1>(); // this step's copy has landed
+                ring_read<T, TM, RC>(ring + rd * kSlot, cur);
+                if (++rd == Ring::SLOTS) rd = 0;
+                issue();
+            } else {
+                const int cj = (O <= 3) ? q : ((q * C) >> p.order);
+                load_mat_vals<T, TM, RC>(base + (int64_t)cj * row_ld, ci0, ncx, cur);
+            }
             T A[RC], B[RC];
 #pragma unroll
             for (int rc = 0; rc < RC; ++rc) stencil_coefs(cur[rc], A[rc], B[rc]);
@@ -679,6 +803,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_inc_kernel(StreamI
             }
         }
     }
+    if constexpr (PF > 0) cp_async_wait<0>();
 }
 
 } // namespace sigk
