@@ -48,6 +48,10 @@ WORKLOADS = {
     # the same stream with N and L capped at 256 (service-sized requests)
     "serve_light": dict(kind="serve", requests=400, rate=200.0, nmin=8, nmax=256, lmin=32, lmax=256, dims=(2, 8, 32),
                         orders=(0, 1, 2), robust=0.3, seed=6),
+    # SigPDE.gram(x, y) with RBFKernel(sigma=1): the gram256 paths and shape, static kernel evaluated on
+    # the device from the points
+    "rbf256": dict(kind="static", nx=256, ny=256, L=128, d=8, order=2, seed_x=2001, seed_y=2002, static="rbf",
+                   sigma=1.0),
     "uneven4096": dict(kind="ragged", npairs=4096, lmin=16, lmax=512, d=32, orders=(0, 1, 2, 3), seed=4096),
 }
 
@@ -83,6 +87,21 @@ def workload_units(w):
     # (the increment dot product and the stencil coefficients)
     flops = 4 * cells + (2 * w["d"] + 8) * coarse
     return entries, cells, flops
+
+
+def workload_name(w):
+    kern = {"linear": "LinearKernel", "rbf": f"RBFKernel(sigma={w.get('sigma')})",
+            "l1rbf": f"L1RBFKernel(sigma={w.get('sigma')})"}[w.get("static", "linear")]
+    return f"SigPDE.gram {w['nx']}x{w['ny']}, L={w['L']}, d={w['d']}, dyadic_order={w['order']}, {kern}"
+
+
+def static_kernel_of(kernels, w):
+    st = w.get("static", "linear")
+    if st == "rbf":
+        return kernels.RBFKernel(w["sigma"])
+    if st == "l1rbf":
+        return kernels.L1RBFKernel(w["sigma"])
+    return kernels.LinearKernel()
 
 
 def make_inputs(w, device=None, dtype=None):
@@ -264,7 +283,7 @@ def cpu_oracle_rate(w, target_s, seed=7, max_entries=None):
     while True:
         flat = rng.choice(w["nx"] * w["ny"], n, replace=False)
         t0 = time.perf_counter()
-        oracle.gram(x, y, w["order"], pairs=flat)
+        oracle.gram(x, y, w["order"], pairs=flat, static=w.get("static", "linear"), static_param=w.get("sigma", 1.0))
         dt = time.perf_counter() - t0
         if dt >= target_s or n >= w["nx"] * w["ny"] or (max_entries and n >= max_entries):
             break
@@ -301,8 +320,8 @@ def run_reference(args, w, rank):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic Brownian paths (seeded), float32 inputs upcast to float64",
-        "config": {"workload": "SigPDE.gram 256x256, L=128, d=8, dyadic_order=2, LinearKernel", "global_batch":
-                   entries, "seq_len": w["L"], "parallelism": "cpu", "l2": "n/a (CPU)"},
+        "config": {"workload": workload_name(w), "global_batch": entries, "seq_len": w["L"], "parallelism": "cpu",
+                   "l2": "n/a (CPU)"},
         "cells_per_s": value * cells / entries,
         "cpu_baseline": {"value": value, "unit": "entries/s", "cores": cores, "kind": "port",
                          "sample": f"per step: {sample}; float64 C restatement of the reference solver"},
@@ -444,6 +463,88 @@ def run_ours(args, w):
         print(json.dumps(line), flush=True)
 
 
+def run_ours_static(args, w):
+    """Gram with an RBF / L1-RBF static kernel evaluated on the device from the
+    points (sigk_gram_static).  Beside it, the reference's route on this
+    library's solver: torch builds the float32 static Gram and its 4-term
+    difference per 32x32 tile of paths, the CUDA wavefront reads them."""
+    import numpy as np
+    import torch
+    import sigpde_b200.torch as sig
+    from sigpde_b200 import _lib
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    entries, cells, _ = workload_units(w)
+    coarse = entries * (w["L"] - 1) ** 2
+    flops = 4 * cells + 8 * coarse  # the wavefront's stencil and coefficients
+    X, Y = make_inputs(w, device=dev)
+    k = sig.SigPDE(static_kernel_of(sig.kernels, w), w["order"], precision=args.precision)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    out = k.gram(X, Y)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    times = timed_steps(torch, lambda: k.gram(X, Y), args.steps, args.warmup, flush, lambda: None)
+    launches = LAUNCHES["last"]
+    clk = clocks.stop()
+    kg = sig.SigPDE(static_kernel_of(sig.kernels, w), w["order"], precision=args.precision)
+    kg._device_static = False
+    out_g = kg.gram(X, Y)
+    t_generic = timed_steps(torch, lambda: kg.gram(X, Y), max(1, args.steps // 4), 1, flush, lambda: None)
+    Xh, Yh = X.cpu().pin_memory(), Y.cpu().pin_memory()
+    Rh = torch.empty((w["nx"], w["ny"]), dtype=X.dtype).pin_memory()
+
+    def e2e_step():
+        Rh.copy_(k.gram(Xh.to(dev, non_blocking=True), Yh.to(dev, non_blocking=True)), non_blocking=True)
+
+    e2e_times = timed_steps(torch, e2e_step, args.steps, args.warmup, flush, lambda: None)
+    ms = statistics.mean(times)
+    acc = cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle
+        st = dict(static=w["static"], static_param=w["sigma"])
+        rng = np.random.default_rng(1)
+        flat = rng.choice(entries, 64, replace=False)
+        xin, yin = X.double().cpu().numpy(), Y.double().cpu().numpy()
+        want = oracle.gram(xin, yin, w["order"], pairs=flat, **st)
+        kxx = oracle.pairwise(xin[flat // w["ny"]], None, w["order"], **st)
+        kyy = oracle.pairwise(yin[flat % w["ny"]], None, w["order"], **st)
+        acc = {}
+        for name, G in (("device_static", out), ("generic_route", out_g)):
+            got = G.double().cpu().numpy().reshape(-1)[flat]
+            acc[name] = {"max_rel_err": float(np.max(np.abs(got - want) / np.abs(want))),
+                         "max_cs_err": float(np.max(np.abs(got - want) / np.sqrt(kxx * kyy)))}
+        acc["sample"] = "64 random entries vs the float64 oracle"
+        rate, cores, sample = cpu_oracle_rate(w, args.cpu_seconds)
+        cpu = {"value": rate, "unit": "entries/s", "cores": cores, "kind": "port",
+               "sample": f"{sample}; float64 C restatement of the reference solver (OpenMP), numpy static Gram"}
+    peak = device_peak_tflops(torch, torch.float64)
+    achieved = flops / (ms * 1e-3) / 1e12
+    line = {
+        "metric": "gram_entries_per_s", "value": entries / (ms * 1e-3), "unit": "entries/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "p50_ms": percentile(times, 0.5),
+        "p99_ms": percentile(times, 0.99), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic Brownian paths (seeded PCG64), float32",
+        "config": {"workload": workload_name(w), "global_batch": entries, "seq_len": w["L"],
+                   "parallelism": "single GPU", "precision": args.precision,
+                   "l2": "flushed between timed steps (256 MB write)"},
+        "cells_per_s": cells / (ms * 1e-3),
+        "generic_route_ms_per_step": statistics.mean(t_generic),
+        "accuracy": acc,
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "traffic": None, "scope": "whole step (static-kernel increments + wavefront): the stencil's "
+                     "4 FLOPs per refined cell and 8 per coarse cell over the step time",
+                     "peak_source": "measured cuBLAS DGEMM 4096^3 on this device"},
+        "e2e": {"value": entries / (statistics.mean(e2e_times) * 1e-3), "unit": "entries/s",
+                "h2d_bytes_per_step": 2 * Xh.numel() * Xh.element_size(),
+                "d2h_bytes_per_step": Rh.numel() * Rh.element_size(), "ms_per_step": statistics.mean(e2e_times)},
+        "gpu_launches": launches, "clocks": clk, "lib": _lib.version(),
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+
+
 def run_reference_gpu(args, w):
     """The reference's own GPU path: stojl/SigPDE installed unmodified under
     baseline/_ref, called through its public API (sigpde.torch.SigPDE.gram with
@@ -469,7 +570,7 @@ def run_reference_gpu(args, w):
         return
     dev = torch.device("cuda", 0)
     X, Y = make_inputs(w, device=dev)
-    k = refsig.SigPDE(refsig.kernels.LinearKernel(), w["order"])
+    k = refsig.SigPDE(static_kernel_of(refsig.kernels, w), w["order"])
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
     try:
         out = k.gram(X, Y)
@@ -495,10 +596,11 @@ def run_reference_gpu(args, w):
         rng = np.random.default_rng(1)
         flat = rng.choice(entries, 64, replace=False)
         xin, yin = X.double().cpu().numpy(), Y.double().cpu().numpy()
-        want = oracle.gram(xin, yin, w["order"], pairs=flat)
+        st = dict(static=w.get("static", "linear"), static_param=w.get("sigma", 1.0))
+        want = oracle.gram(xin, yin, w["order"], pairs=flat, **st)
         got = G.reshape(-1)[flat]
-        kxx = oracle.pairwise(xin[flat // w["ny"]], None, w["order"])
-        kyy = oracle.pairwise(yin[flat % w["ny"]], None, w["order"])
+        kxx = oracle.pairwise(xin[flat // w["ny"]], None, w["order"], **st)
+        kyy = oracle.pairwise(yin[flat % w["ny"]], None, w["order"], **st)
         acc = {"max_rel_err": float(np.max(np.abs(got - want) / np.abs(want))),
                "max_cs_err": float(np.max(np.abs(got - want) / np.sqrt(kxx * kyy))),
                "sample": "64 random entries vs the float64 oracle"}
@@ -506,9 +608,8 @@ def run_reference_gpu(args, w):
                 ms_per_step=ms, p50_ms=percentile(times, 0.5), p99_ms=percentile(times, 0.99),
                 higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32 storage / f64 arithmetic",
                 data="synthetic Brownian paths (seeded PCG64), float32",
-                config={"workload": "SigPDE.gram 256x256, L=128, d=8, dyadic_order=2, LinearKernel",
-                        "global_batch": entries, "seq_len": w["L"], "parallelism": "single GPU",
-                        "l2": "flushed between timed calls (256 MB write)"},
+                config={"workload": workload_name(w), "global_batch": entries, "seq_len": w["L"],
+                        "parallelism": "single GPU", "l2": "flushed between timed calls (256 MB write)"},
                 cells_per_s=cells / (ms * 1e-3), accuracy=acc,
                 note="unmodified stojl/SigPDE (Numba CUDA) through sigpde.torch.SigPDE.gram, host-timed "
                      "(the reference synchronises inside each call)")
@@ -983,6 +1084,10 @@ def main():
         return
     if ragged:
         run_ours_ragged(args, w)
+        return
+    if w.get("kind") == "static":
+        if int(os.environ.get("RANK", "0")) == 0:
+            run_ours_static(args, w)
         return
     run_ours(args, w)
 

@@ -73,6 +73,11 @@ typedef enum { SIGK_F32 = 0, SIGK_F64 = 1 } sigk_dtype;
 
 typedef enum { SIGK_PREC_FP64 = 0, SIGK_PREC_FP32 = 1, SIGK_PREC_TC32 = 2, SIGK_PREC_TC64 = 3 } sigk_precision;
 
+/* Static kernels that sigk_gram_static evaluates on the device
+ * (sigpde/torch/static_kernels.py:3-53); param is LinearKernel's scale or the
+ * RBF kernels' sigma. */
+typedef enum { SIGK_STATIC_LINEAR = 0, SIGK_STATIC_RBF = 1, SIGK_STATIC_L1RBF = 2 } sigk_static_kind;
+
 typedef enum {
     SIGK_OP_PAIRWISE = 0,     /* out[b]    = k(x_b, y_b)                                */
     SIGK_OP_GRAM = 1,         /* out[i][j] = k(x_i, y_j)                                */
@@ -138,6 +143,31 @@ SIGK_API int sigk_gram(const void *x, const void *y, int64_t n_x, int64_t n_y, i
 SIGK_API int sigk_gram_sym(const void *x, int64_t n, int64_t len, int64_t dim, int dtype, int order, double static_scale,
                   const void *scale, void *out, int precision, void *workspace, size_t workspace_bytes,
                   sigk_stream_t stream);
+
+/*
+ * Gram matrix (op = SIGK_OP_GRAM) or symmetric Gram (op = SIGK_OP_GRAM_SYM,
+ * y = NULL, n_y / len_y / scale_y ignored) with a static kernel evaluated from
+ * the path points on the device:
+ *   SIGK_STATIC_LINEAR  param * <x, y>: the sigk_gram / sigk_gram_sym path;
+ *   SIGK_STATIC_RBF     exp(-(|x|^2 + |y|^2 - 2<x, y>) / param);
+ *   SIGK_STATIC_L1RBF   exp(-|x - y|_1 / param).
+ * Replaces, for RBFKernel / L1RBFKernel, SigPDE._gram / _gram_sym's tile loop
+ * with the static Gram, the 4-term difference and the solver
+ * (sigpde/torch/kernel.py:18-21,75-171, sigpde/torch/static_kernels.py:13-53,
+ * sigpde/cuda_gram_kernels.py:8-164).  The static Gram is evaluated in
+ * float64 (the reference uses the input dtype) and each increment is written
+ * once to a float64 matrix in the workspace, which the wavefront reads; the
+ * cells are float64, so precision must be SIGK_PREC_FP64 or SIGK_PREC_TC64,
+ * and dim <= 32 (SIGK_EUNSUPPORTED otherwise: sigk_gram_inc takes any
+ * increments).  Workspace: sigk_static_workspace_size(op, kind, ...) bytes,
+ * 256-byte aligned.
+ */
+SIGK_API size_t sigk_static_workspace_size(int op, int kind, int64_t n_x, int64_t n_y, int64_t len_x, int64_t len_y,
+                                           int64_t dim, int order, int dtype, int precision);
+SIGK_API int sigk_gram_static(int op, int kind, double param, const void *x, const void *y, int64_t n_x, int64_t n_y,
+                              int64_t len_x, int64_t len_y, int64_t dim, int dtype, int order, const void *scale_x,
+                              const void *scale_y, void *out, int precision, void *workspace,
+                              size_t workspace_bytes, sigk_stream_t stream);
 
 /*
  * Self norms k(x_b, x_b) in float64, NaN mapped to +inf.

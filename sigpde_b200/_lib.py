@@ -32,6 +32,9 @@ SIGK_OP_PAIRWISE = 0
 SIGK_OP_GRAM = 1
 SIGK_OP_GRAM_SYM = 2
 SIGK_OP_NORMALIZE = 3
+SIGK_STATIC_LINEAR = 0
+SIGK_STATIC_RBF = 1
+SIGK_STATIC_L1RBF = 2
 
 # Exported symbol -> (restype, argtypes).  Kept in the order of include/sigk.h.
 _vp = ctypes.c_void_p
@@ -59,6 +62,9 @@ SIGNATURES = {
     "sigk_gram": (_int, [_vp, _vp, _i64, _i64, _i64, _i64, _i64, _int, _int, _dbl, _vp, _vp, _vp, _int, _vp, _sz,
                          _vp]),
     "sigk_gram_sym": (_int, [_vp, _i64, _i64, _i64, _int, _int, _dbl, _vp, _vp, _int, _vp, _sz, _vp]),
+    "sigk_static_workspace_size": (_sz, [_int, _int, _i64, _i64, _i64, _i64, _i64, _int, _int, _int]),
+    "sigk_gram_static": (_int, [_int, _int, _dbl, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _int, _int, _vp, _vp, _vp,
+                                _int, _vp, _sz, _vp]),
     "sigk_self_norms": (_int, [_vp, _i64, _i64, _i64, _int, _int, _dbl, _vp, _vp, _sz, _vp]),
     "sigk_normalize": (_int, [_vp, _i64, _i64, _i64, _int, _int, _dbl, _vp, _vp, _dbl, _int, _vp, _vp, _vp, _sz,
                               _vp]),

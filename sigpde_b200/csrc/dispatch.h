@@ -16,6 +16,7 @@ struct TcImageParams;
 struct TcGemmParams;
 struct TcRaggedImageParams;
 struct DgemmIncParams;
+struct StaticIncParams;
 }
 struct CUtensorMap_st; // cuda.h
 namespace sigk {
@@ -30,6 +31,7 @@ using StreamIncFn = void (*)(StreamIncParams);
 using TcImageFn = void (*)(TcImageParams);
 using TcRaggedImageFn = void (*)(TcRaggedImageParams);
 using DgemmIncFn = void (*)(DgemmIncParams);
+using StaticIncFn = void (*)(StaticIncParams);
 using TcGemmFn = void (*)(TcGemmParams, CUtensorMap_st);
 using DeltaFn = void (*)(const void *, int64_t, int64_t, int64_t, int64_t, double, const void *, void *);
 
@@ -60,6 +62,9 @@ TcGemmFn get_tc_gemm_kernel();
 TcRaggedImageFn get_tc_ragged_image_kernel(bool in64);
 // float64 increment matrix on the CUDA cores (dgemm_inc.cuh)
 DgemmIncFn get_dgemm_inc_kernel();
+// float64 increment matrix of the RBF / L1-RBF static kernel from the path points (static_inc.cuh);
+// null for dim > 32
+StaticIncFn get_static_inc_kernel(int kind, int64_t dim);
 // mat64: the increment matrix holds float64 (dgemm_inc_kernel) instead of float32 (tensor cores)
 StreamIncFn get_stream_inc_kernel(bool f64cells, int R, int O, bool mat64);
 

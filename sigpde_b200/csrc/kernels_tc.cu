@@ -1,6 +1,7 @@
 // Instantiations of the tensor-core increment kernels (tc.cuh).
 #include "dispatch.h"
 #include "dgemm_inc.cuh"
+#include "static_inc.cuh"
 #include "tc.cuh"
 
 namespace sigk {
@@ -39,6 +40,26 @@ TcImageFn get_tc_image_kernel(bool in64) { return in64 ? tc_image_kernel<double>
 TcGemmFn get_tc_gemm_kernel() { return tc_gemm_kernel<kTcBN>; }
 
 DgemmIncFn get_dgemm_inc_kernel() { return dgemm_inc_kernel<kDgTile>; }
+
+namespace {
+template <int KIND>
+StaticIncFn static_by_dim(int64_t d)
+{
+    if (d <= 2) return static_inc_kernel<KIND, 2>;
+    if (d <= 4) return static_inc_kernel<KIND, 4>;
+    if (d <= 8) return static_inc_kernel<KIND, 8>;
+    if (d <= 16) return static_inc_kernel<KIND, 16>;
+    if (d <= 32) return static_inc_kernel<KIND, 32>;
+    return nullptr;
+}
+} // namespace
+
+StaticIncFn get_static_inc_kernel(int kind, int64_t dim)
+{
+    if (kind == kStaticRbf) return static_by_dim<kStaticRbf>(dim);
+    if (kind == kStaticL1Rbf) return static_by_dim<kStaticL1Rbf>(dim);
+    return nullptr;
+}
 
 TcRaggedImageFn get_tc_ragged_image_kernel(bool in64)
 {

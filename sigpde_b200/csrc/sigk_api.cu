@@ -24,6 +24,7 @@
 #include "tc.cuh"
 #include "norm_pipe.cuh"
 #include "dgemm_inc.cuh"
+#include "static_inc.cuh"
 
 namespace sigk {
 namespace {
@@ -628,10 +629,11 @@ int run_pairs_tc(const TcPlan &t, int op, const void *x, const void *y, int64_t 
 // at most kTcChunkBytes).
 constexpr int kDgMinDim = 16;
 
-TcPlan make_mat64_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, int64_t d, int order)
+// Layout of a float64 increment matrix plan; diffs: room for the scaled
+// differences of both sides (the linear kernel's GEMM operands).
+TcPlan mat64_layout(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, int64_t d, int order, bool diffs)
 {
     TcPlan t{};
-    if (op == kOpPairwise || d < kDgMinDim || env_flag("SIGK_NO_DGEMM_INC")) return t;
     const int64_t n = ncx << order, m = ncy << order;
     const int C = order >= 4 ? 8 : (1 << order);
     const int Rs = pick_rows(n);
@@ -656,11 +658,28 @@ TcPlan make_mat64_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy,
     t.nchunks = (nx + chunk - 1) / chunk;
     t.err_off = 0;
     t.bnd_off = 256;
-    t.a_off = t.bnd_off + bnd_bytes;                                     // x differences
-    t.b_off = t.a_off + align256((size_t)nx * ncx * d * sizeof(double)); // y differences
-    t.ct_off = t.b_off + align256((size_t)ny_paths * ncy * d * sizeof(double));
+    t.a_off = t.bnd_off + bnd_bytes; // x differences
+    t.b_off = t.a_off + (diffs ? align256((size_t)nx * ncx * d * sizeof(double)) : 0); // y differences
+    t.ct_off = t.b_off + (diffs ? align256((size_t)ny_paths * ncy * d * sizeof(double)) : 0);
     t.ws_bytes = t.ct_off + align256((size_t)chunk * per_x);
     return t;
+}
+
+TcPlan make_mat64_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, int64_t d, int order)
+{
+    if (op == kOpPairwise || d < kDgMinDim || env_flag("SIGK_NO_DGEMM_INC")) return TcPlan{};
+    return mat64_layout(op, nx, ny, ncx, ncy, d, order, true);
+}
+
+// RBF / L1-RBF Grams (fp64 cells, dim <= kStaticMaxDim): the increments of
+// all pairs straight from the path points (static_inc.cuh) into the same
+// matrix layout, read by the same wavefront kernels.
+constexpr int64_t kStaticMaxDim = 32;
+
+TcPlan make_static_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, int64_t d, int order)
+{
+    if (op == kOpPairwise || d > kStaticMaxDim) return TcPlan{};
+    return mat64_layout(op, nx, ny, ncx, ncy, d, order, false);
 }
 
 int run_pairs_mat64(const TcPlan &t, int op, const void *x, const void *y, int64_t nx, int64_t ny, int64_t lx,
@@ -725,6 +744,59 @@ int run_pairs_mat64(const TcPlan &t, int op, const void *x, const void *y, int64
         if (e != cudaSuccess) return cuda_fail(e, "float64 increment GEMM launch");
         if ((st = consume_matrix(t, op, mat, true, gp.ld, err, i0, i1, nx, ny, ncx, ncy, d, order, out, out_ld, in64,
                                  precision, dtype, wsb, stream)))
+            return st;
+    }
+    return SIGK_OK;
+}
+
+int run_pairs_static(const TcPlan &t, int op, int kind, double param, const void *x, const void *y, int64_t nx,
+                     int64_t ny, int64_t lx, int64_t ly, int64_t d, int dtype, int order, const void *sx,
+                     const void *sy, void *out, int64_t out_ld, void *ws, cudaStream_t stream)
+{
+    int st;
+    const bool in64 = dtype == SIGK_F64;
+    const size_t es = in64 ? 8 : 4;
+    const int64_t ncx = lx - 1, ncy = ly - 1;
+    unsigned char *wsb = reinterpret_cast<unsigned char *>(ws);
+    unsigned *err = reinterpret_cast<unsigned *>(wsb + t.err_off);
+    double *mat = reinterpret_cast<double *>(wsb + t.ct_off);
+    StaticIncFn fn = get_static_inc_kernel(kind, d);
+    if (!fn) return fail(SIGK_EUNSUPPORTED, "no static-kernel increment kernel for kind %d, dim %lld", kind,
+                         (long long)d);
+    cudaError_t e = cudaMemsetAsync(err, 0, sizeof(unsigned), stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+    const bool sym = op == kOpGramSym;
+    for (int64_t c = 0; c < t.nchunks; ++c) {
+        const int64_t i0 = c * t.chunk, i1 = (i0 + t.chunk < nx) ? i0 + t.chunk : nx, nxc = i1 - i0;
+        StaticIncParams sp{};
+        sp.x = reinterpret_cast<const unsigned char *>(x) + (size_t)i0 * lx * d * es;
+        sp.y = sym ? x : y;
+        sp.in64 = in64;
+        sp.npaths_x = nxc;
+        sp.lx = lx;
+        sp.rows_x = t.rows_x;
+        sp.npaths_y = sym ? i1 : ny;
+        sp.ly = ly;
+        sp.d = d;
+        sp.inv_param = 1.0 / param;
+        sp.f = std::ldexp(1.0, -2 * order);
+        sp.sx = sx ? reinterpret_cast<const unsigned char *>(sx) + (size_t)i0 * es : nullptr;
+        sp.sy = sym ? sx : sy;
+        sp.mode = sym ? kTcLower : kTcAll;
+        sp.x0 = i0;
+        sp.out = mat;
+        sp.ld = nxc * t.rows_x;
+        const int64_t warps = (nxc * lx + kStRowsPerWarp - 1) / kStRowsPerWarp;
+        const int64_t bx = (warps + kStWarps - 1) / kStWarps;
+        int64_t by = (sp.npaths_y * ncy + kStTileN - 1) / kStTileN;
+        if (by > 65535) by = 65535;
+        if (bx > 0x7fffffffLL) return fail(SIGK_EUNSUPPORTED, "increment matrix too large");
+        fn<<<dim3((unsigned)bx, (unsigned)by), kStWarps * 32, 0, stream>>>(sp);
+        count_launch();
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(e, "static-kernel increment launch");
+        if ((st = consume_matrix(t, op, mat, true, sp.ld, err, i0, i1, nx, ny, ncx, ncy, d, order, out, out_ld, in64,
+                                 SIGK_PREC_FP64, dtype, wsb, stream)))
             return st;
     }
     return SIGK_OK;
@@ -1010,6 +1082,69 @@ int sigk_gram_sym(const void *x, int64_t n, int64_t len, int64_t dim, int dtype,
 {
     return run_pairs(kOpGramSym, x, x, n, n, len, len, dim, dtype, order, static_scale, scale, scale, out, n,
                      precision, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+size_t sigk_static_workspace_size(int op, int kind, int64_t n_x, int64_t n_y, int64_t len_x, int64_t len_y,
+                                  int64_t dim, int order, int dtype, int precision)
+{
+    if (kind == SIGK_STATIC_LINEAR) return sigk_workspace_size(op, n_x, n_y, len_x, len_y, dim, order, dtype, precision);
+    if (kind != SIGK_STATIC_RBF && kind != SIGK_STATIC_L1RBF) return 0;
+    if (op != SIGK_OP_GRAM && op != SIGK_OP_GRAM_SYM) return 0;
+    if (len_x < 2 || len_y < 2 || order < 0 || order > 12 || dim < 1 || n_x < 1 || n_y < 1) return 0;
+    if (op == SIGK_OP_GRAM_SYM) {
+        n_y = n_x;
+        len_y = len_x;
+    }
+    TcPlan t = make_static_plan(op == SIGK_OP_GRAM ? kOpGram : kOpGramSym, n_x, n_y, len_x - 1, len_y - 1, dim, order);
+    return t.ok ? t.ws_bytes : 0;
+}
+
+int sigk_gram_static(int op, int kind, double param, const void *x, const void *y, int64_t n_x, int64_t n_y,
+                     int64_t len_x, int64_t len_y, int64_t dim, int dtype, int order, const void *scale_x,
+                     const void *scale_y, void *out, int precision, void *workspace, size_t workspace_bytes,
+                     sigk_stream_t stream)
+{
+    if (op != SIGK_OP_GRAM && op != SIGK_OP_GRAM_SYM)
+        return fail(SIGK_EINVAL, "op must be SIGK_OP_GRAM or SIGK_OP_GRAM_SYM (got %d)", op);
+    const bool sym = op == SIGK_OP_GRAM_SYM;
+    if (sym) {
+        if (y && y != x) return fail(SIGK_EINVAL, "SIGK_OP_GRAM_SYM takes y = NULL (or y = x)");
+        y = x;
+        n_y = n_x;
+        len_y = len_x;
+        scale_y = scale_x;
+    }
+    const int kop = sym ? kOpGramSym : kOpGram;
+    if (kind == SIGK_STATIC_LINEAR)
+        return run_pairs(kop, x, y, n_x, n_y, len_x, len_y, dim, dtype, order, param, scale_x, scale_y, out, n_y,
+                         precision, workspace, workspace_bytes, (cudaStream_t)stream);
+    if (kind != SIGK_STATIC_RBF && kind != SIGK_STATIC_L1RBF)
+        return fail(SIGK_EINVAL, "unknown static kernel kind %d", kind);
+    int st = check_common(dtype, precision, order);
+    if (st) return st;
+    if (!(param > 0.0) || !std::isfinite(param)) return fail(SIGK_EINVAL, "sigma must be finite and > 0");
+    if (precision != SIGK_PREC_FP64 && precision != SIGK_PREC_TC64)
+        return fail(SIGK_EUNSUPPORTED, "RBF / L1-RBF increments from points need float64 cells (SIGK_PREC_FP64 or "
+                                       "SIGK_PREC_TC64); use sigk_gram_inc for float32 cells");
+    if (n_x < 1 || n_y < 1) return fail(SIGK_EINVAL, "path counts must be >= 1 (got %lld, %lld)", (long long)n_x,
+                                        (long long)n_y);
+    if (len_x < 2 || len_y < 2) return fail(SIGK_EINVAL, "path lengths must be >= 2 (got %lld, %lld)",
+                                            (long long)len_x, (long long)len_y);
+    if (dim < 1) return fail(SIGK_EINVAL, "dim must be >= 1");
+    if (dim > kStaticMaxDim)
+        return fail(SIGK_EUNSUPPORTED, "RBF / L1-RBF increments from points take dim <= %lld (got %lld); use "
+                                       "sigk_gram_inc", (long long)kStaticMaxDim, (long long)dim);
+    if ((st = check_dev(x, "x", false)) || (st = check_dev(y, "y", false)) || (st = check_dev(out, "out", false)) ||
+        (st = check_dev(scale_x, "scale_x", true)) || (st = check_dev(scale_y, "scale_y", true)))
+        return st;
+    TcPlan t = make_static_plan(kop, n_x, n_y, len_x - 1, len_y - 1, dim, order);
+    if (!t.ok) return fail(SIGK_EUNSUPPORTED, "no static-kernel plan");
+    if (!workspace || workspace_bytes < t.ws_bytes)
+        return fail(SIGK_ENOMEM, "workspace of %zu bytes needed (got %zu)", t.ws_bytes,
+                    workspace ? workspace_bytes : 0);
+    if (((uintptr_t)workspace & 255) != 0) return fail(SIGK_EINVAL, "workspace must be 256-byte aligned");
+    return run_pairs_static(t, kop, kind, param, x, y, n_x, n_y, len_x, len_y, dim, dtype, order, scale_x, scale_y,
+                            out, n_y, workspace, (cudaStream_t)stream);
 }
 
 // Shared body of sigk_normalize, sigk_normalize_inc and sigk_self_norms

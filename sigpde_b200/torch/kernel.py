@@ -89,6 +89,21 @@ def _is_fused_linear(static_kernel) -> bool:
                                                                           (int, float))
 
 
+def _static_kind(static_kernel):
+    """(kind, sigma) for an RBF or L1-RBF kernel whose static Gram the device
+    evaluates from the points (ours, or the reference's classes of the same
+    name with a float sigma), else None."""
+    name = type(static_kernel).__name__
+    kind = {"RBFKernel": _lib.SIGK_STATIC_RBF, "L1RBFKernel": _lib.SIGK_STATIC_L1RBF}.get(name)
+    sigma = getattr(static_kernel, "sigma", None)
+    if kind is None or isinstance(sigma, bool) or not isinstance(sigma, (int, float)):
+        return None
+    if not (isinstance(static_kernel, (static_kernels.RBFKernel, static_kernels.L1RBFKernel)) or
+            type(static_kernel).__module__.startswith("sigpde")):
+        return None
+    return kind, float(sigma)
+
+
 def pairwise_inner_product(x, y, static_kernel, dyadic_order):
     """Coarse increments of each pair: 4-term second difference of the static
     Gram divided by 4^order (sigpde/torch/kernel.py:13-16)."""
@@ -206,6 +221,9 @@ class SigPDE:
                           self.dyadic_order, float(self.static_kernel.scale), _ptr(sx), _ptr(sy), _ptr(result),
                           prec, _ptr(ws), nws, _stream())
                 return result
+            if self._static_on_device(x):
+                self._gram_static(_lib.SIGK_OP_GRAM, x, y, sx, sy, result)
+                return result
             tile = math.ceil(math.sqrt(max_batch))  # sigpde/torch/kernel.py:68
             for y0, y1 in _batches(Ny, tile):
                 for x0, x1 in _batches(Nx, tile):
@@ -231,6 +249,9 @@ class SigPDE:
                 _lib.call("sigk_gram_sym", _ptr(x), N, x.shape[1], x.shape[2], dt, self.dyadic_order,
                           float(self.static_kernel.scale), _ptr(sx), _ptr(result), prec, _ptr(ws), nws, _stream())
                 return result
+            if self._static_on_device(x):
+                self._gram_static(_lib.SIGK_OP_GRAM_SYM, x, None, sx, None, result)
+                return result
             tile = math.ceil(math.sqrt(max_batch))
             for y0, y1 in _batches(N, tile):
                 for x0, x1 in _batches(N, tile):
@@ -242,6 +263,26 @@ class SigPDE:
                     if x0 != y0:
                         result[y0:y1, x0:x1] = result[x0:x1, y0:y1].t()
         return result
+
+    def _static_on_device(self, x):
+        """RBF / L1-RBF Grams with float64 cells and dim <= 32 evaluate the
+        static kernel from the points on the device (sigk_gram_static);
+        other cases build the increments with torch (the reference's route)."""
+        return (getattr(self, "_device_static", True) and _static_kind(self.static_kernel) is not None
+                and self.precision in ("fp64", "tc64") and x.shape[2] <= 32)
+
+    def _gram_static(self, op, x, y, sx, sy, result):
+        kind, sigma = _static_kind(self.static_kernel)
+        x = x.contiguous()
+        y = x if y is None else y.contiguous()
+        dt = _dtype_code(x)
+        prec = _PREC[self.precision]
+        n = _lib.lib().sigk_static_workspace_size(op, kind, x.shape[0], y.shape[0], x.shape[1], y.shape[1],
+                                                  x.shape[2], self.dyadic_order, dt, prec)
+        ws = torch.empty(n, dtype=torch.uint8, device=x.device) if n else None
+        _lib.call("sigk_gram_static", op, kind, sigma, _ptr(x), None if op == _lib.SIGK_OP_GRAM_SYM else _ptr(y),
+                  x.shape[0], y.shape[0], x.shape[1], y.shape[1], x.shape[2], dt, self.dyadic_order, _ptr(sx),
+                  _ptr(sy), _ptr(result), prec, _ptr(ws), n, _stream())
 
     def _solve_gram_inc(self, inc, sx, sy, result, x0, y0, symmetric):
         inc = inc.to(result.dtype)

@@ -101,3 +101,47 @@ def test_static_kernels_match_oracle(oracle, name, param):
     p = k.pairwise(torch.tensor(x[:2]), torch.tensor(y[:2])).numpy()
     want = oracle.static_gram(kind, x[:2], y[:2], param)
     np.testing.assert_allclose(p, np.stack([want[0, 0], want[1, 1]]), rtol=1e-10, atol=1e-13)
+
+
+def test_static_kernel_detection():
+    """RBF / L1-RBF kernels (ours or classes of the reference's names from a
+    sigpde module) go to sigk_gram_static; other objects keep the generic route."""
+    from sigpde_b200 import _lib
+    from sigpde_b200.torch import kernels
+    from sigpde_b200.torch.kernel import _static_kind
+    assert _static_kind(kernels.RBFKernel(0.5)) == (_lib.SIGK_STATIC_RBF, 0.5)
+    assert _static_kind(kernels.L1RBFKernel(2)) == (_lib.SIGK_STATIC_L1RBF, 2.0)
+    assert _static_kind(kernels.LinearKernel(2.0)) is None
+
+    class RBFKernel:  # same name, foreign module: may compute anything else
+        sigma = 1.0
+    assert _static_kind(RBFKernel()) is None
+    ref_like = type("RBFKernel", (), {"__module__": "sigpde.torch.static_kernels", "sigma": 0.25})
+    assert _static_kind(ref_like()) == (_lib.SIGK_STATIC_RBF, 0.25)
+    assert _static_kind(type("L1RBFKernel", (), {"__module__": "sigpde.torch.static_kernels",
+                                                  "sigma": torch.tensor(1.0)})()) is None
+
+
+def test_static_gram_argument_checks(built_lib):
+    """sigk_gram_static rejects bad arguments before any device call."""
+    from sigpde_b200 import _lib
+    L = _lib.lib()
+
+    def call(op=_lib.SIGK_OP_GRAM, kind=_lib.SIGK_STATIC_RBF, param=1.0, dim=4, prec=_lib.SIGK_PREC_FP64, y=None):
+        return L.sigk_gram_static(op, kind, param, None, y, 3, 3, 10, 10, dim, _lib.SIGK_F32, 1, None, None, None,
+                                  prec, None, 0, None)
+
+    assert call(op=_lib.SIGK_OP_PAIRWISE) == _lib.SIGK_EINVAL
+    assert call(kind=7) == _lib.SIGK_EINVAL
+    assert call(param=0.0) == _lib.SIGK_EINVAL
+    assert call(param=float("nan")) == _lib.SIGK_EINVAL
+    assert call(prec=_lib.SIGK_PREC_FP32) == _lib.SIGK_EUNSUPPORTED
+    assert "float64 cells" in _lib.last_error()
+    assert call(prec=_lib.SIGK_PREC_TC32) == _lib.SIGK_EUNSUPPORTED
+    assert call(dim=33) == _lib.SIGK_EUNSUPPORTED
+    assert "dim <= 32" in _lib.last_error()
+    assert call(op=_lib.SIGK_OP_GRAM_SYM, y=1024) == _lib.SIGK_EINVAL
+    assert L.sigk_static_workspace_size(_lib.SIGK_OP_PAIRWISE, _lib.SIGK_STATIC_RBF, 3, 3, 10, 10, 4, 1,
+                                        _lib.SIGK_F32, _lib.SIGK_PREC_FP64) == 0
+    assert L.sigk_static_workspace_size(_lib.SIGK_OP_GRAM, 9, 3, 3, 10, 10, 4, 1, _lib.SIGK_F32,
+                                        _lib.SIGK_PREC_FP64) == 0
