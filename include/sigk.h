@@ -170,6 +170,27 @@ SIGK_API int sigk_gram_static(int op, int kind, double param, const void *x, con
                               size_t workspace_bytes, sigk_stream_t stream);
 
 /*
+ * Backward pass (no counterpart in the reference, whose Numba kernels end
+ * autograd): gradients of  L = sum_b grad_out[b] k(x_b, y_b)  (op =
+ * SIGK_OP_PAIRWISE, n_y = n_x) or  L = sum_ij grad_out[i][j] k(x_i, y_j)
+ * (op = SIGK_OP_GRAM) with respect to the points of x and y, for the linear
+ * static kernel (static_scale) with per-path scales scale_x / scale_y (held
+ * constant), by the adjoint of the float64 scheme.
+ *   grad_out: (n_x,) or (n_x, n_y) row-major, in dtype
+ *   grad_x: (n_x, len_x, dim), grad_y: (n_y, len_y, dim), in dtype; either may
+ *   be NULL (not computed).  For a symmetric Gram pass y = x and add the two.
+ * Dyadic order <= 4 (SIGK_EUNSUPPORTED above).  Workspace:
+ * sigk_backward_workspace_size(...) bytes, 256-byte aligned (pairs are taken
+ * in chunks of x paths so that it stays near 4 GiB plus the inputs' size).
+ */
+SIGK_API size_t sigk_backward_workspace_size(int op, int64_t n_x, int64_t n_y, int64_t len_x, int64_t len_y,
+                                             int64_t dim, int order, int dtype);
+SIGK_API int sigk_backward(int op, const void *x, const void *y, int64_t n_x, int64_t n_y, int64_t len_x,
+                           int64_t len_y, int64_t dim, int dtype, int order, double static_scale,
+                           const void *scale_x, const void *scale_y, const void *grad_out, void *grad_x,
+                           void *grad_y, void *workspace, size_t workspace_bytes, sigk_stream_t stream);
+
+/*
  * Self norms k(x_b, x_b) in float64, NaN mapped to +inf.
  * First half of RobustSigPDE._norm_factors (sigpde/torch/kernel.py:181-183);
  * used when the normaliser is a user callable that the host applies.

@@ -13,6 +13,8 @@ and adds the small pieces of host logic the reference keeps in Python:
                                                              sigpde/torch/kernel.py:180-230
 * RobustSigPDE.pairwise / gram                               sigpde/torch/kernel.py:232-301
 * static-kernel Grams (linear / RBF / L1-RBF) in float64     sigpde/torch/static_kernels.py:3-53
+* gradients of pairwise / Gram (LinearKernel) by the adjoint of the solve (no
+  reference counterpart; pinned by central differences of the solve in tests/)
 
 Inputs are upcast to float64 before anything is computed, so the rounding of
 float32 inputs is not charged to the kernel under test.  Parity of this
@@ -65,6 +67,9 @@ def lib():
             L.sko_chandrupatla.argtypes = [_pd, _i64, _int, _d, _d, _d, _int, _int, _pint]
             L.sko_chandrupatla.restype = _d
             L.sko_chandrupatla_batch.argtypes = [_pd, _i64, _i64, _int, _pd, _pd, _d, _int, _int, _pd, _pint]
+            L.sko_grad_solve.argtypes = [_pd, _i64, _i64, _int, _d, _d, _pd]
+            L.sko_grad_solve.restype = _d
+            L.sko_grad_solve_batch.argtypes = [_pd, _i64, _i64, _i64, _int, _pd, _pd, _pd, _pd]
             L.sko_num_threads.restype = _int
             L.sko_set_num_threads.argtypes = [_int]
             _lib = L
@@ -256,6 +261,87 @@ def gram(x, y=None, order: int = 0, x_scale=None, y_scale=None, static: str = "l
     vy = None if sy is None else sy[flat % Ny]
     vals = solve_increments(incs, order, vx, vy, store_f32)
     return vals if pairs is not None else vals.reshape(Nx, Ny)
+
+
+# --------------------------------------------------------------------------- gradients
+def grad_increments(incs, order: int, scale=None, w=None):
+    """w * dk/dc for a batch of increment blocks (npairs, ncx, ncy), c = inc * scale:
+    the adjoint of the solve (sko_grad_solve).  Returns (G, k)."""
+    incs = _f64(incs)
+    if incs.ndim == 2:
+        incs = incs[None]
+    B, ncx, ncy = incs.shape
+    scale = None if scale is None else _f64(scale).reshape(B)
+    w = None if w is None else _f64(w).reshape(B)
+    G = np.empty((B, ncx, ncy), np.float64)
+    k = np.empty(B, np.float64)
+    lib().sko_grad_solve_batch(_ptr(incs), B, ncx, ncy, int(order), _ptr(scale), _ptr(w), _ptr(G), _ptr(k))
+    return G, k
+
+
+def _chain_linear(H, x, y):
+    """Gradients of sum_ij H_ij <dx_i, dy_j> with respect to the points of x and y."""
+    dx = np.diff(x, axis=0)
+    dy = np.diff(y, axis=0)
+    hx = H @ dy          # (ncx, d): d/d dx_i
+    hy = H.T @ dx        # (ncy, d): d/d dy_j
+    gx = np.zeros_like(x)
+    gy = np.zeros_like(y)
+    gx[1:] += hx
+    gx[:-1] -= hx
+    gy[1:] += hy
+    gy[:-1] -= hy
+    return gx, gy
+
+
+def grad_pairwise(x, y, order: int, grad_out, x_scale=None, y_scale=None, static_scale: float = 1.0):
+    """Gradients of sum_b grad_out[b] * k(x_b, y_b) (LinearKernel) with respect to x and y,
+    float64, by the adjoint of each solve and the chain rule through the increments
+    inc_ij = static_scale * <dx_i, dy_j> / 4^order, c = inc * x_scale * y_scale."""
+    x = _f64(x)
+    y = _f64(y)
+    B = x.shape[0]
+    w = _f64(grad_out).reshape(B)
+    sx = _scale_vec(x_scale, B)
+    sy = _scale_vec(y_scale, B)
+    s = np.ones(B) * (1.0 if sx is None else sx) * (1.0 if sy is None else sy)
+    incs = np.stack([increments_linear(x[b], y[b], order, static_scale) for b in range(B)])
+    G, _ = grad_increments(incs, order, s, w)
+    gx = np.zeros_like(x)
+    gy = np.zeros_like(y)
+    f = static_scale / float(4 ** order)
+    for b in range(B):
+        gx[b], gy[b] = _chain_linear(G[b] * (s[b] * f), x[b], y[b])
+    return gx, gy
+
+
+def grad_gram(x, y, order: int, grad_out, x_scale=None, y_scale=None, static_scale: float = 1.0):
+    """Gradients of sum_ij grad_out[i, j] * k(x_i, y_j) (LinearKernel Gram) with respect to x
+    and y (y=None: the symmetric Gram of x, both sides' contributions to x)."""
+    sym = y is None
+    x = _f64(x)
+    y = x if sym else _f64(y)
+    Nx, Ny = x.shape[0], y.shape[0]
+    w = _f64(grad_out).reshape(Nx, Ny)
+    sx = _scale_vec(x_scale, Nx)
+    sy = sx if sym else _scale_vec(y_scale, Ny)
+    sxv = np.ones(Nx) if sx is None else sx
+    syv = np.ones(Ny) if sy is None else sy
+    ii, jj = np.meshgrid(np.arange(Nx), np.arange(Ny), indexing="ij")
+    ii, jj = ii.reshape(-1), jj.reshape(-1)
+    incs = np.stack([increments_linear(x[i], y[j], order, static_scale) for i, j in zip(ii, jj)])
+    s = sxv[ii] * syv[jj]
+    G, _ = grad_increments(incs, order, s, w.reshape(-1))
+    gx = np.zeros_like(x)
+    gy = np.zeros_like(y)
+    f = static_scale / float(4 ** order)
+    for t, (i, j) in enumerate(zip(ii, jj)):
+        a, b = _chain_linear(G[t] * (s[t] * f), x[i], y[j])
+        gx[i] += a
+        gy[j] += b
+    if sym:
+        return gx + gy
+    return gx, gy
 
 
 # --------------------------------------------------------------------------- robust

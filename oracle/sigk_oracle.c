@@ -18,6 +18,9 @@
  *       (4-term second difference of the static Gram, divided by 4^order)
  *   - the Chandrupatla lambda loop sigpde/cuda_pairwise_kernels.py:100-178
  *       with the argument order of sigpde/torch/kernel.py:180-195
+ *   - the gradient of a solve with respect to its increments (the adjoint of
+ *     the scheme; the reference has none): sko_grad_solve, checked against
+ *     central differences of sko_solve by the tests
  *
  * Arithmetic follows the reference expression order exactly and must be
  * compiled without FMA contraction (-ffp-contract=off), so that float64
@@ -254,6 +257,66 @@ void sko_chandrupatla_batch(const double *incs, int64_t B, int64_t nc, int order
                                     iters ? iters + b : NULL);
         lam[b] = (k[b] < 1) ? 0.0 : l;
     }
+}
+
+/*
+ * Gradient of one solve with respect to its coarse increments: the adjoint of
+ * the scheme above (the reference has no backward pass; this restates the
+ * calculus of pde_step, sigpde/cuda_device_functions.py:3-5).
+ *   c = inc * scale,  A(c) = 1 + c/2 + c^2/12,  B(c) = 1 - c^2/12,
+ *   K[p][q] = (K[p][q-1] + K[p-1][q]) A(c_pq) - K[p-1][q-1] B(c_pq).
+ * Lambda = w * dK[lx-1][ly-1] / dK over the nodes, in reverse row-major order:
+ *   Lambda[p][q] = A(c_p,q+1) Lambda[p][q+1] + A(c_p+1,q) Lambda[p+1][q]
+ *                  - B(c_p+1,q+1) Lambda[p+1][q+1]        (absent terms are 0)
+ * with Lambda[lx-1][ly-1] = w, and each cell adds
+ *   Lambda[p][q] * ((K[p][q-1] + K[p-1][q]) A'(c) - K[p-1][q-1] B'(c)),
+ *   A'(c) = 1/2 + c/6, B'(c) = -c/6,
+ * to G at its coarse cell.  G = w * dK / dc (ncx x ncy); returns K[lx-1][ly-1].
+ */
+static inline double coef_a(double c) { return 1. + 0.5 * c + (1. / 12) * (c * c); }
+static inline double coef_b(double c) { return 1. - (1. / 12) * (c * c); }
+
+double sko_grad_solve(const double *inc, int64_t ncx, int64_t ncy, int order, double scale, double w, double *G)
+{
+    const int64_t lx = (ncx << order) + 1, ly = (ncy << order) + 1;
+    double *K = (double *)malloc(sizeof(double) * (size_t)(lx * ly));
+    double *Lm = (double *)calloc((size_t)(lx * ly), sizeof(double));
+#define CELL(p, q) (inc[(((p) - 1) >> order) * ncy + (((q) - 1) >> order)] * scale)
+    for (int64_t q = 0; q < ly; ++q) K[q] = 1.0;
+    for (int64_t p = 1; p < lx; ++p) {
+        K[p * ly] = 1.0;
+        for (int64_t q = 1; q < ly; ++q) {
+            const double c = CELL(p, q);
+            K[p * ly + q] = (K[p * ly + q - 1] + K[(p - 1) * ly + q]) * coef_a(c) - K[(p - 1) * ly + q - 1] * coef_b(c);
+        }
+    }
+    memset(G, 0, sizeof(double) * (size_t)(ncx * ncy));
+    for (int64_t p = lx - 1; p >= 1; --p)
+        for (int64_t q = ly - 1; q >= 1; --q) {
+            double lam = (p == lx - 1 && q == ly - 1) ? w : 0.0;
+            if (q + 1 < ly) lam += coef_a(CELL(p, q + 1)) * Lm[p * ly + q + 1];
+            if (p + 1 < lx) lam += coef_a(CELL(p + 1, q)) * Lm[(p + 1) * ly + q];
+            if (p + 1 < lx && q + 1 < ly) lam -= coef_b(CELL(p + 1, q + 1)) * Lm[(p + 1) * ly + q + 1];
+            Lm[p * ly + q] = lam;
+            const double c = CELL(p, q);
+            const double dk = (K[p * ly + q - 1] + K[(p - 1) * ly + q]) * (0.5 + c / 6.) - K[(p - 1) * ly + q - 1] * (-c / 6.);
+            G[((p - 1) >> order) * ncy + ((q - 1) >> order)] += lam * dk;
+        }
+#undef CELL
+    const double r = K[lx * ly - 1];
+    free(K);
+    free(Lm);
+    return r;
+}
+
+/* sko_grad_solve over a batch of increment blocks (npairs, ncx, ncy) with per-pair scale and weight. */
+void sko_grad_solve_batch(const double *incs, int64_t npairs, int64_t ncx, int64_t ncy, int order,
+                          const double *scale, const double *w, double *G, double *out)
+{
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t b = 0; b < npairs; ++b)
+        out[b] = sko_grad_solve(incs + b * ncx * ncy, ncx, ncy, order, scale ? scale[b] : 1.0, w ? w[b] : 1.0,
+                                G + b * ncx * ncy);
 }
 
 int sko_num_threads(void)

@@ -65,6 +65,9 @@ SIGNATURES = {
     "sigk_static_workspace_size": (_sz, [_int, _int, _i64, _i64, _i64, _i64, _i64, _int, _int, _int]),
     "sigk_gram_static": (_int, [_int, _int, _dbl, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _int, _int, _vp, _vp, _vp,
                                 _int, _vp, _sz, _vp]),
+    "sigk_backward_workspace_size": (_sz, [_int, _i64, _i64, _i64, _i64, _i64, _int, _int]),
+    "sigk_backward": (_int, [_int, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _int, _int, _dbl, _vp, _vp, _vp, _vp, _vp,
+                             _vp, _sz, _vp]),
     "sigk_self_norms": (_int, [_vp, _i64, _i64, _i64, _int, _int, _dbl, _vp, _vp, _sz, _vp]),
     "sigk_normalize": (_int, [_vp, _i64, _i64, _i64, _int, _int, _dbl, _vp, _vp, _dbl, _int, _vp, _vp, _vp, _sz,
                               _vp]),

@@ -17,6 +17,8 @@ struct TcGemmParams;
 struct TcRaggedImageParams;
 struct DgemmIncParams;
 struct StaticIncParams;
+struct GradParams;
+struct GradContractParams;
 }
 struct CUtensorMap_st; // cuda.h
 namespace sigk {
@@ -65,6 +67,21 @@ DgemmIncFn get_dgemm_inc_kernel();
 // float64 increment matrix of the RBF / L1-RBF static kernel from the path points (static_inc.cuh);
 // null for dim > 32
 StaticIncFn get_static_inc_kernel(int kind, int64_t dim);
+// backward pass (grad.cuh): forward-with-derivatives and adjoint wavefronts for R rows a lane,
+// order O (R >= 2^O); null members where the combination is not built
+struct GradFns {
+    void (*fwd)(GradParams);
+    void (*bwd)(GradParams);
+};
+GradFns get_grad_kernels(int R, int O);
+struct GradAuxFns {
+    void (*pair_inc)(const double *, const double *, int64_t, int64_t, int64_t, int64_t, int64_t, int64_t, double *);
+    void (*gx)(GradContractParams);
+    void (*gy)(GradContractParams);
+    void (*reduce)(const double *, int64_t, int64_t, int64_t, int64_t, int64_t, int64_t, double *);
+    void (*points)(const double *, int64_t, int64_t, int64_t, double, const void *, int, void *);
+};
+GradAuxFns get_grad_aux_kernels();
 // mat64: the increment matrix holds float64 (dgemm_inc_kernel) instead of float32 (tensor cores)
 StreamIncFn get_stream_inc_kernel(bool f64cells, int R, int O, bool mat64);
 

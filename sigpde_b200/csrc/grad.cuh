@@ -1,0 +1,414 @@
+// Backward pass: gradients of sum_pairs w * k(x, y) with respect to the path
+// points, for the linear static kernel with float64 cells.  The reference has
+// no backward pass (its Numba kernels end autograd); this is the adjoint of
+// the same scheme (sigpde/cuda_device_functions.py:3-5).
+//
+// With c the scaled coarse increment of a cell, A(c) = 1 + c/2 + c^2/12 and
+// B(c) = 1 - c^2/12, the forward scheme is
+//   K(p,q) = (K(p,q-1) + K(p-1,q)) A - K(p-1,q-1) B.
+// Its adjoint Lambda = w dk/dK(p,q) satisfies, in reverse order,
+//   Lambda(p,q) = P(p,q+1) + P(p+1,q) - Q(p+1,q+1),   Lambda(n,m) = w,
+// where each node carries P = A Lambda and Q = B Lambda with the coefficients
+// of the cell that produced it (absent nodes carry 0), and
+//   dk/dc of a coarse cell = sum over its fine cells of Lambda(p,q) D(p,q),
+//   D(p,q) = (K(p,q-1) + K(p-1,q)) A'(c) - K(p-1,q-1) B'(c),
+//   A'(c) = 1/2 + c/6,  B'(c) = -c/6.
+//
+// Kernels
+//   grad_fwd_kernel  one warp per pair: the forward wavefront (R rows a lane,
+//                    one fine column a step, bands of 32R rows) storing D of
+//                    every fine cell;
+//   grad_bwd_kernel  one warp per pair: the same schedule in reverse for
+//                    Lambda, summing Lambda D per coarse cell; each coarse
+//                    cell's rows belong to one lane (R >= 2^order), so the
+//                    sum is written once, over the cell's increment in the
+//                    increment matrix (which then holds dk/dc);
+//   grad_gx_kernel / grad_gy_kernel   contractions of dk/dc with the scaled
+//                    differences of the other side: the gradients with
+//                    respect to the coarse differences;
+//   grad_points_kernel   differences of those: gradients at the points.
+#pragma once
+
+#include "dgemm_inc.cuh"
+
+namespace sigk {
+
+struct GradParams {
+    int op;               // kOpPairwise / kOpGram
+    double *mat;          // increments in, dk/dc out; Gram: [n * ld + m], pairwise: per-pair blocks
+    int64_t ld;           // Gram: npaths_x(chunk) * rows_x; pairwise: rows_x
+    int64_t rows_x;
+    int64_t ncx, ncy;
+    int order;
+    int64_t nitems;       // pairs in this chunk
+    int64_t ny;           // Gram: y paths
+    const void *w;        // weights (grad_out): pairwise (n,), Gram (n_x, n_y) row-major; input dtype
+    int in64;
+    int64_t x0;           // first x path of the chunk
+    double *dbuf;         // D of every fine cell, per pair nbands * m * 32 * R doubles
+    double *bnd;          // per pair 2 * (m + 2) doubles: band boundary rows
+};
+
+// pair `it` of the chunk: its x path (global), y path, and its increment block
+__device__ __forceinline__ void grad_item(const GradParams &p, int64_t it, int64_t &xi, int64_t &yj, double *&base,
+                                          int64_t &row_ld)
+{
+    if (p.op == kOpPairwise) {
+        xi = p.x0 + it;
+        yj = xi;
+        base = p.mat + it * p.ncy * p.rows_x;
+        row_ld = p.rows_x;
+    } else {
+        const int64_t il = it / p.ny;
+        xi = p.x0 + il;
+        yj = it - il * p.ny;
+        base = p.mat + yj * p.ncy * p.ld + il * p.rows_x;
+        row_ld = p.ld;
+    }
+}
+
+template <int R, int O>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) grad_fwd_kernel(GradParams p)
+{
+    static_assert(R >= (1 << O), "a lane's rows hold whole coarse rows");
+    constexpr int RC = R >> O;
+    const int lane = threadIdx.x & 31;
+    const int64_t gwarp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int n = (int)(p.ncx << p.order), m = (int)(p.ncy << p.order);
+    const int nb = (n + 32 * R - 1) / (32 * R);
+    for (int64_t it = gwarp; it < p.nitems; it += nwarps) {
+        int64_t xi, yj, row_ld;
+        double *base;
+        grad_item(p, it, xi, yj, base, row_ld);
+        double *D = p.dbuf + it * (int64_t)nb * m * 32 * R;
+        double *bnd = p.bnd + it * 2 * (int64_t)(m + 2); // K of the row above the band, columns 0..m
+        for (int b = 0; b < nb; ++b) {
+            const int p0 = b * 32 * R + lane * R + 1; // this lane's first fine row (1-based)
+            const int ci0 = (p0 - 1) >> O;            // its first coarse row
+            double left[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) left[r] = 1.0; // K(p, 0)
+            double bot = 1.0, corner = 1.0;            // lane l-1's last row at q-1 (as received), at q-2
+            double c[RC], A[RC], B[RC], Ad[RC], Bd[RC];
+            __syncwarp();
+            for (int s = 0; s < m + 31; ++s) {
+                const double from_above = __shfl_up_sync(0xffffffffu, bot, 1);
+                const int q = s - lane + 1;
+                if (q >= 1 && q <= m) {
+                    double top, diag;
+                    if (lane == 0) {
+                        top = b == 0 ? 1.0 : bnd[q];
+                        diag = b == 0 ? 1.0 : bnd[q - 1];
+                    } else {
+                        top = from_above;
+                        diag = q == 1 ? 1.0 : corner;
+                    }
+                    if (q == 1 || ((q - 1) & ((1 << O) - 1)) == 0) { // a new coarse column
+                        const int cj = (q - 1) >> O;
+#pragma unroll
+                        for (int rc = 0; rc < RC; ++rc) {
+                            const int ci = ci0 + rc;
+                            c[rc] = ci < p.ncx ? base[(int64_t)cj * row_ld + ci] : 0.0;
+                            stencil_coefs(c[rc], A[rc], B[rc]);
+                            Ad[rc] = fma(c[rc], 1.0 / 6.0, 0.5);
+                            Bd[rc] = c[rc] * (-1.0 / 6.0);
+                        }
+                    }
+                    double *dq = D + (((int64_t)b * m + (q - 1)) * 32 + lane) * R;
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        const int rc = r >> O;
+                        const double sum = left[r] + top;
+                        const double k = sum * A[rc] - diag * B[rc];
+                        const bool valid = p0 + r <= n;
+                        dq[r] = valid ? sum * Ad[rc] - diag * Bd[rc] : 0.0;
+                        diag = left[r];
+                        left[r] = valid ? k : 0.0;
+                        top = left[r];
+                    }
+                    if (lane == 31 && b + 1 < nb) bnd[q] = left[R - 1];
+                    corner = from_above;
+                    bot = left[R - 1];
+                }
+            }
+            __syncwarp();
+            if (lane == 31 && b + 1 < nb) bnd[0] = 1.0;
+            __syncwarp();
+        }
+    }
+}
+
+template <int R, int O>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) grad_bwd_kernel(GradParams p)
+{
+    static_assert(R >= (1 << O), "a lane's rows hold whole coarse rows");
+    constexpr int RC = R >> O;
+    const int lane = threadIdx.x & 31;
+    const int64_t gwarp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int n = (int)(p.ncx << p.order), m = (int)(p.ncy << p.order);
+    const int nb = (n + 32 * R - 1) / (32 * R);
+    for (int64_t it = gwarp; it < p.nitems; it += nwarps) {
+        int64_t xi, yj, row_ld;
+        double *base;
+        grad_item(p, it, xi, yj, base, row_ld);
+        const int64_t widx = p.op == kOpPairwise ? xi : xi * p.ny + yj;
+        const double w = p.in64 ? reinterpret_cast<const double *>(p.w)[widx]
+                                : (double)reinterpret_cast<const float *>(p.w)[widx];
+        const double *D = p.dbuf + it * (int64_t)nb * m * 32 * R;
+        double *bP = p.bnd + it * 2 * (int64_t)(m + 2); // P and Q of the row below the band, columns 0..m+1
+        double *bQ = bP + (m + 2);
+        for (int b = nb - 1; b >= 0; --b) {
+            const int p0 = b * 32 * R + lane * R + 1;
+            const int ci0 = (p0 - 1) >> O;
+            double Pr[R], Qr[R]; // P, Q of the lane's rows at column q + 1
+#pragma unroll
+            for (int r = 0; r < R; ++r) Pr[r] = Qr[r] = 0.0;
+            double g[RC];
+#pragma unroll
+            for (int rc = 0; rc < RC; ++rc) g[rc] = 0.0;
+            double topP = 0.0, topQ = 0.0; // this lane's row 0 P, Q at its last column (published)
+            double belowQ_prev = 0.0;      // lane l+1's row 0 Q at column q + 1
+            double c[RC], A[RC], B[RC];
+            __syncwarp();
+            for (int s = m + 30; s >= 0; --s) {
+                const double belowP = __shfl_down_sync(0xffffffffu, topP, 1);
+                const double belowQ = __shfl_down_sync(0xffffffffu, topQ, 1);
+                const int q = s - lane + 1;
+                if (q >= 1 && q <= m) {
+                    double dP, dQ; // P(p+1, q) and Q(p+1, q+1) for the lane's last row
+                    if (lane == 31) {
+                        const bool last = b + 1 >= nb;
+                        dP = last ? 0.0 : bP[q];
+                        dQ = last ? 0.0 : bQ[q + 1];
+                    } else {
+                        dP = belowP;
+                        dQ = q == m ? 0.0 : belowQ_prev;
+                    }
+                    const int cj = (q - 1) >> O;
+                    if (q == m || (q & ((1 << O) - 1)) == 0) { // entering a coarse column (in reverse)
+#pragma unroll
+                        for (int rc = 0; rc < RC; ++rc) {
+                            const int ci = ci0 + rc;
+                            c[rc] = ci < p.ncx ? base[(int64_t)cj * row_ld + ci] : 0.0;
+                            stencil_coefs(c[rc], A[rc], B[rc]);
+                        }
+                    }
+                    const double *dq = D + (((int64_t)b * m + (q - 1)) * 32 + lane) * R;
+#pragma unroll
+                    for (int r = R - 1; r >= 0; --r) {
+                        const int rc = r >> O;
+                        const int pr = p0 + r;
+                        double lam = Pr[r] + dP - dQ;
+                        if (pr == n && q == m) lam += w;
+                        if (pr > n) lam = 0.0;
+                        g[rc] = fma(lam, dq[r], g[rc]);
+                        const double P = A[rc] * lam, Q = B[rc] * lam;
+                        dQ = Qr[r]; // Q(p, q+1) is the diagonal of the row above
+                        dP = P;
+                        Pr[r] = P;
+                        Qr[r] = Q;
+                    }
+                    topP = Pr[0];
+                    topQ = Qr[0];
+                    if (lane == 0 && b > 0) {
+                        bP[q] = Pr[0];
+                        bQ[q] = Qr[0];
+                    }
+                    if (((q - 1) & ((1 << O) - 1)) == 0) { // leaving the coarse column: dk/dc is complete
+#pragma unroll
+                        for (int rc = 0; rc < RC; ++rc) {
+                            const int ci = ci0 + rc;
+                            if (ci < p.ncx) base[(int64_t)cj * row_ld + ci] = g[rc];
+                            g[rc] = 0.0;
+                        }
+                    }
+                }
+                belowQ_prev = belowQ;
+            }
+            __syncwarp();
+            if (lane == 0 && b > 0) {
+                bP[m + 1] = 0.0;
+                bQ[m + 1] = 0.0;
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// Increments of pairwise pairs (x path = y path = x0 + item) in per-pair
+// blocks [item][cj][ci] (ci < rows_x; rows ci >= ncx are 0), summed as
+// fma(dx_k, dy_k, acc) for k = 0 .. d-1 from zero like the other producers.
+template <int V = 0> // instantiated once, in kernels_grad.cu
+__global__ void grad_pair_inc_kernel(const double *dx, const double *dy, int64_t nitems, int64_t x0, int64_t ncx,
+                                     int64_t ncy, int64_t rows_x, int64_t d, double *out)
+{
+    const int64_t total = nitems * ncy * rows_x;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t item = e / (ncy * rows_x), r = e - item * ncy * rows_x;
+        const int64_t cj = r / rows_x, ci = r - cj * rows_x;
+        double acc = 0.0;
+        if (ci < ncx) {
+            const double *a = dx + (x0 + item) * d * ncx + ci;
+            const double *b = dy + (x0 + item) * d * ncy + cj;
+            for (int64_t k = 0; k < d; ++k) acc = fma(a[k * ncx], b[k * ncy], acc);
+        }
+        out[e] = acc;
+    }
+}
+
+// Gradients with respect to the x side's scaled-difference rows: for each
+// matrix row m (x path il, cell ci), gdx[m][k] += fx * sum_n G[n][m] dy[n][k]
+// over the y cells n paired with it (Gram: all of them; pairwise: its own
+// pair's), where dy are the y side's scaled differences (dimension-major).
+// Each CTA-y slice sums a range of n into its own partial row; grad_reduce
+// adds the slices in order.
+struct GradContractParams {
+    int op;
+    const double *mat;     // dk/dc
+    int64_t ld, rows_x, ncx, ncy;
+    int64_t nrows_m;       // Gram: ld; pairwise: nitems * rows_x
+    int64_t ncols_n;       // Gram: ny * ncy; pairwise: ncy (per pair)
+    const double *dx;      // x differences (npaths, d, ncx), chunk-relative, scaled
+    const double *dy;      // y differences (npaths, d, ncy), scaled
+    int64_t d;
+    double *part;          // gx: [slice][nrows_m][d] partial sums
+    int64_t slice;         // columns per slice
+    double *gdy;           // gy: (ny, ncy, d) accumulated (+=) over chunks
+    int64_t x0;
+};
+
+template <int V = 0> // instantiated once, in kernels_grad.cu
+__global__ void grad_gx_kernel(GradContractParams p)
+{
+    const int64_t mm = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (mm >= p.nrows_m) return;
+    const int64_t n0 = (int64_t)blockIdx.y * p.slice;
+    const int64_t n1 = n0 + p.slice < p.ncols_n ? n0 + p.slice : p.ncols_n;
+    int64_t ci, item = 0;
+    const double *col;     // G[n][mm] = col[n * stride]
+    int64_t stride;
+    const double *dy;      // dy of column n: dy[(n / ncy) * d * ncy + k * ncy + n % ncy] (Gram)
+    if (p.op == kOpPairwise) {
+        item = mm / p.rows_x;
+        ci = mm - item * p.rows_x;
+        col = p.mat + item * p.ncy * p.rows_x + ci;
+        stride = p.rows_x;
+        dy = p.dy + item * p.d * p.ncy; // the pair's own y path (chunk-relative pairs start at x0)
+        dy += p.x0 * p.d * p.ncy;
+    } else {
+        ci = mm % p.rows_x;
+        col = p.mat + mm;
+        stride = p.ld;
+        dy = p.dy;
+    }
+    double *out = p.part + ((int64_t)blockIdx.y * p.nrows_m + mm) * p.d;
+    if (ci >= p.ncx) {
+        for (int64_t k = 0; k < p.d; ++k) out[k] = 0.0;
+        return;
+    }
+    for (int64_t k0 = 0; k0 < p.d; k0 += 8) {
+        double acc[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] = 0.0;
+        for (int64_t n = n0; n < n1; ++n) {
+            const double gv = col[n * stride];
+            const int64_t yp = n / p.ncy, cj = n - yp * p.ncy;
+            const double *dyn = dy + yp * p.d * p.ncy + cj;
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                if (k0 + k < p.d) acc[k] = fma(gv, dyn[(k0 + k) * p.ncy], acc[k]);
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (k0 + k < p.d) out[k0 + k] = acc[k];
+    }
+}
+
+// gy: one warp per y cell n (Gram: n = y path * ncy + cj over all y paths;
+// pairwise: n = pair * ncy + cj), lanes over the x cells paired with it.
+template <int V = 0> // instantiated once, in kernels_grad.cu
+__global__ void grad_gy_kernel(GradContractParams p)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t n = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nrows = p.op == kOpPairwise ? (p.nrows_m / p.rows_x) * p.ncy : p.ncols_n;
+    if (n >= nrows) return;
+    const double *row;
+    int64_t mlen, yrow;
+    const double *dx;
+    if (p.op == kOpPairwise) {
+        const int64_t item = n / p.ncy, cj = n - item * p.ncy;
+        row = p.mat + item * p.ncy * p.rows_x + cj * p.rows_x;
+        mlen = p.rows_x;
+        dx = p.dx + item * p.d * p.ncx;
+        yrow = (p.x0 + item) * p.ncy + cj;
+    } else {
+        row = p.mat + n * p.ld;
+        mlen = p.ld;
+        dx = p.dx;
+        yrow = n;
+    }
+    for (int64_t k0 = 0; k0 < p.d; k0 += 8) {
+        double acc[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] = 0.0;
+        for (int64_t mm = lane; mm < mlen; mm += 32) {
+            const int64_t il = mm / p.rows_x, ci = mm - il * p.rows_x;
+            if (ci >= p.ncx) continue;
+            const double gv = row[mm];
+            const double *dxm = dx + il * p.d * p.ncx + ci;
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                if (k0 + k < p.d) acc[k] = fma(gv, dxm[(k0 + k) * p.ncx], acc[k]);
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            double v = acc[k];
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+            if (lane == 0 && k0 + k < p.d) p.gdy[yrow * p.d + k0 + k] += v;
+        }
+    }
+}
+
+// gdx[(x0 + il) * ncx + ci][k] = sum over slices of part (rows ci < ncx).
+template <int V = 0> // instantiated once, in kernels_grad.cu
+__global__ void grad_reduce_kernel(const double *part, int64_t nslices, int64_t nrows_m, int64_t rows_x, int64_t ncx,
+                                   int64_t d, int64_t x0, double *gdx)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nrows_m * d) return;
+    const int64_t mm = e / d, k = e - mm * d;
+    const int64_t il = mm / rows_x, ci = mm - il * rows_x;
+    if (ci >= ncx) return;
+    double s = 0.0;
+    for (int64_t sl = 0; sl < nslices; ++sl) s += part[(sl * nrows_m + mm) * d + k];
+    gdx[((x0 + il) * ncx + ci) * d + k] = s;
+}
+
+// grad at the points: g[path][t][k] = scale(path) * (gd[t-1][k] - gd[t][k]),
+// gd of the path's coarse differences (ncells = len - 1), in the output dtype.
+template <int V = 0> // instantiated once, in kernels_grad.cu
+__global__ void grad_points_kernel(const double *gd, int64_t npaths, int64_t len, int64_t d, double f,
+                                   const void *sc, int in64, void *out)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= npaths * len * d) return;
+    const int64_t pth = e / (len * d), r = e - pth * len * d, t = r / d, k = r - t * d;
+    const int64_t nc = len - 1;
+    const double *g = gd + pth * nc * d;
+    const double a = t >= 1 ? g[(t - 1) * d + k] : 0.0;
+    const double b = t < nc ? g[t * d + k] : 0.0;
+    const double s = sc ? (in64 ? reinterpret_cast<const double *>(sc)[pth]
+                                : (double)reinterpret_cast<const float *>(sc)[pth]) : 1.0;
+    const double v = (a - b) * f * s;
+    if (in64)
+        reinterpret_cast<double *>(out)[e] = v;
+    else
+        reinterpret_cast<float *>(out)[e] = (float)v;
+}
+
+} // namespace sigk

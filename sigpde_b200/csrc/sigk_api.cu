@@ -25,6 +25,7 @@
 #include "norm_pipe.cuh"
 #include "dgemm_inc.cuh"
 #include "static_inc.cuh"
+#include "grad.cuh"
 
 namespace sigk {
 namespace {
@@ -802,6 +803,219 @@ int run_pairs_static(const TcPlan &t, int op, int kind, double param, const void
     return SIGK_OK;
 }
 
+// ------------------------------------------------------------------ backward pass
+// Gradients of sum w * k with respect to the points (grad.cuh).  Pairs are
+// processed in chunks of x paths so that the per-cell derivatives D (one
+// float64 per fine cell of every pair in the chunk) and the chunk's increment
+// matrix stay under kGradChunkBytes (SIGK_GRAD_CHUNK_MB overrides).
+// Workspace: zero word | x, y differences | dk/d(x diff), dk/d(y diff) |
+// partial sums of the x contraction | increment matrix | D | boundary rows.
+constexpr size_t kGradChunkBytes = 4ull << 30;
+constexpr int kGradMaxOrder = 4;
+constexpr int64_t kGradSlices = 64;
+
+struct GradPlan {
+    bool ok = false;
+    int R = 0, O = 0, nb = 0;
+    int64_t rows_x = 0, chunk = 0, nchunks = 0, slice = 0, nslices = 0;
+    size_t dx_off = 0, dy_off = 0, gdx_off = 0, gdy_off = 0, part_off = 0, mat_off = 0, d_off = 0, bnd_off = 0,
+           ws_bytes = 0;
+};
+
+GradPlan make_grad_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, int64_t d, int order)
+{
+    GradPlan g;
+    if (order > kGradMaxOrder) return g;
+    const int64_t n = ncx << order, m = ncy << order;
+    int R = 1;
+    while (R < 16 && (R < (1 << order) || 32 * R < n)) R *= 2;
+    g.R = R;
+    g.O = order;
+    g.nb = (int)((n + 32 * R - 1) / (32 * R));
+    g.rows_x = (ncx + 3) / 4 * 4;
+    const size_t dbytes = (size_t)g.nb * m * 32 * R * sizeof(double);
+    const size_t bbytes = 2 * (size_t)(m + 2) * sizeof(double);
+    const size_t mbytes = (size_t)ncy * g.rows_x * sizeof(double);
+    const int64_t items_per_x = op == kOpPairwise ? 1 : ny;
+    const size_t per_x = (size_t)items_per_x * (dbytes + bbytes + mbytes);
+    size_t cap = kGradChunkBytes;
+    if (const char *v = getenv("SIGK_GRAD_CHUNK_MB")) {
+        const long long mb = atoll(v);
+        if (mb > 0) cap = (size_t)mb << 20;
+    }
+    int64_t chunk = (int64_t)(cap / per_x);
+    if (chunk < 1) chunk = 1;
+    if (chunk > nx) chunk = nx;
+    g.chunk = chunk;
+    g.nchunks = (nx + chunk - 1) / chunk;
+    const int64_t ncols = op == kOpPairwise ? ncy : ny * ncy;
+    g.slice = (ncols + kGradSlices - 1) / kGradSlices;
+    if (g.slice < 32) g.slice = ncols < 32 ? ncols : 32;
+    g.nslices = (ncols + g.slice - 1) / g.slice;
+    const int64_t ny_paths = op == kOpPairwise ? nx : ny;
+    size_t off = 256;
+    g.dx_off = off;
+    off += align256((size_t)nx * d * ncx * sizeof(double));
+    g.dy_off = off;
+    off += align256((size_t)ny_paths * d * ncy * sizeof(double));
+    g.gdx_off = off;
+    off += align256((size_t)nx * ncx * d * sizeof(double));
+    g.gdy_off = off;
+    off += align256((size_t)ny_paths * ncy * d * sizeof(double));
+    g.part_off = off;
+    off += align256((size_t)g.nslices * chunk * g.rows_x * d * sizeof(double));
+    g.mat_off = off;
+    off += align256((size_t)chunk * items_per_x * mbytes);
+    g.d_off = off;
+    off += align256((size_t)chunk * items_per_x * dbytes);
+    g.bnd_off = off;
+    off += align256((size_t)chunk * items_per_x * bbytes);
+    g.ws_bytes = off;
+    g.ok = true;
+    return g;
+}
+
+int run_backward(const GradPlan &g, int op, const void *x, const void *y, int64_t nx, int64_t ny, int64_t lx,
+                 int64_t ly, int64_t d, int dtype, int order, double static_scale, const void *sx, const void *sy,
+                 const void *w, void *gx, void *gy, void *ws, cudaStream_t stream)
+{
+    const bool in64 = dtype == SIGK_F64;
+    const int64_t ncx = lx - 1, ncy = ly - 1;
+    unsigned char *wsb = reinterpret_cast<unsigned char *>(ws);
+    double *dx = reinterpret_cast<double *>(wsb + g.dx_off);
+    double *dy = reinterpret_cast<double *>(wsb + g.dy_off);
+    double *gdx = reinterpret_cast<double *>(wsb + g.gdx_off);
+    double *gdy = reinterpret_cast<double *>(wsb + g.gdy_off);
+    double *part = reinterpret_cast<double *>(wsb + g.part_off);
+    double *mat = reinterpret_cast<double *>(wsb + g.mat_off);
+    const int64_t ny_paths = op == kOpPairwise ? nx : ny;
+    cudaError_t e = cudaMemsetAsync(gdy, 0, (size_t)ny_paths * ncy * d * sizeof(double), stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+    DeltaFn delta = get_delta_kernel(true, in64);
+    auto run_delta = [&](const void *src, int64_t npaths, int64_t len, double f, const void *sc, double *dst) -> int {
+        const int64_t total = npaths * (len - 1) * d;
+        int64_t blocks = (total + 255) / 256;
+        if (blocks > (int64_t)sm_count() * 8) blocks = (int64_t)sm_count() * 8;
+        delta<<<(unsigned)blocks, 256, 0, stream>>>(src, npaths, len, d, d, f, sc, dst);
+        count_launch();
+        cudaError_t e2 = cudaGetLastError();
+        return e2 == cudaSuccess ? SIGK_OK : cuda_fail(e2, "delta kernel launch");
+    };
+    const double fs = static_scale * std::ldexp(1.0, -2 * order);
+    int st;
+    if ((st = run_delta(x, nx, lx, fs, sx, dx))) return st;
+    if ((st = run_delta(op == kOpPairwise ? y : y, ny_paths, ly, 1.0, sy, dy))) return st;
+    GradFns kf = get_grad_kernels(g.R, g.O);
+    GradAuxFns aux = get_grad_aux_kernels();
+    if (!kf.fwd || !kf.bwd) return fail(SIGK_EUNSUPPORTED, "no backward kernels for R=%d order=%d", g.R, g.O);
+    int nbf = 0, nbb = 0;
+    if ((st = blocks_per_sm((const void *)kf.fwd, 0, &nbf)) || (st = blocks_per_sm((const void *)kf.bwd, 0, &nbb)))
+        return st;
+    auto launched = [&](const char *what) -> int {
+        count_launch();
+        cudaError_t e2 = cudaGetLastError();
+        return e2 == cudaSuccess ? SIGK_OK : cuda_fail(e2, what);
+    };
+    for (int64_t c = 0; c < g.nchunks; ++c) {
+        const int64_t i0 = c * g.chunk, i1 = (i0 + g.chunk < nx) ? i0 + g.chunk : nx, nxc = i1 - i0;
+        const int64_t items = op == kOpPairwise ? nxc : nxc * ny;
+        const int64_t ld = op == kOpPairwise ? g.rows_x : nxc * g.rows_x;
+        // increments of the chunk's pairs, in the layout the wavefronts read
+        if (op == kOpPairwise) {
+            const int64_t total = items * ncy * g.rows_x;
+            int64_t blocks = (total + 255) / 256;
+            if (blocks > (int64_t)sm_count() * 16) blocks = (int64_t)sm_count() * 16;
+            aux.pair_inc<<<(unsigned)blocks, 256, 0, stream>>>(dx, dy, items, i0, ncx, ncy, g.rows_x, d, mat);
+            if ((st = launched("pairwise increment launch"))) return st;
+        } else {
+            DgemmIncParams gp{};
+            gp.dx = dx + i0 * d * ncx;
+            gp.dy = dy;
+            gp.npaths_x = nxc;
+            gp.ncx = ncx;
+            gp.rows_x = g.rows_x;
+            gp.npaths_y = ny;
+            gp.ncy = ncy;
+            gp.d = d;
+            gp.mode = kTcAll;
+            gp.x0 = i0;
+            gp.out = mat;
+            gp.ld = ld;
+            const int64_t mt = (ld + kDgTile - 1) / kDgTile;
+            int64_t nt = (ny * ncy + kDgTile - 1) / kDgTile;
+            if (nt > 65535) nt = 65535;
+            get_dgemm_inc_kernel()<<<dim3((unsigned)mt, (unsigned)nt), 256, 0, stream>>>(gp);
+            if ((st = launched("increment GEMM launch"))) return st;
+        }
+        GradParams gp{};
+        gp.op = op;
+        gp.mat = mat;
+        gp.ld = ld;
+        gp.rows_x = g.rows_x;
+        gp.ncx = ncx;
+        gp.ncy = ncy;
+        gp.order = order;
+        gp.nitems = items;
+        gp.ny = ny;
+        gp.w = w;
+        gp.in64 = in64;
+        gp.x0 = i0;
+        gp.dbuf = reinterpret_cast<double *>(wsb + g.d_off);
+        gp.bnd = reinterpret_cast<double *>(wsb + g.bnd_off);
+        auto grid_for = [&](int nb) -> unsigned {
+            int64_t warps = (int64_t)sm_count() * nb * kWarpsPerBlock;
+            if (warps > items) warps = items;
+            return (unsigned)((warps + kWarpsPerBlock - 1) / kWarpsPerBlock);
+        };
+        kf.fwd<<<grid_for(nbf), kWarpsPerBlock * 32, 0, stream>>>(gp);
+        if ((st = launched("backward forward-pass launch"))) return st;
+        kf.bwd<<<grid_for(nbb), kWarpsPerBlock * 32, 0, stream>>>(gp);
+        if ((st = launched("adjoint launch"))) return st;
+        // contractions: x side (partial slices, then their ordered sum) and y side
+        GradContractParams cp{};
+        cp.op = op;
+        cp.mat = mat;
+        cp.ld = ld;
+        cp.rows_x = g.rows_x;
+        cp.ncx = ncx;
+        cp.ncy = ncy;
+        cp.nrows_m = op == kOpPairwise ? items * g.rows_x : ld;
+        cp.ncols_n = op == kOpPairwise ? ncy : ny * ncy;
+        cp.dx = dx + i0 * d * ncx;
+        cp.dy = dy;
+        cp.d = d;
+        cp.part = part;
+        cp.slice = g.slice;
+        cp.gdy = gdy;
+        cp.x0 = i0;
+        const int64_t nsl = (cp.ncols_n + g.slice - 1) / g.slice;
+        if (gx) {
+            aux.gx<<<dim3((unsigned)((cp.nrows_m + 127) / 128), (unsigned)nsl), 128, 0, stream>>>(cp);
+            if ((st = launched("x contraction launch"))) return st;
+            const int64_t tot = cp.nrows_m * d;
+            aux.reduce<<<(unsigned)((tot + 255) / 256), 256, 0, stream>>>(part, nsl, cp.nrows_m, g.rows_x, ncx, d, i0,
+                                                                        gdx);
+            if ((st = launched("x reduction launch"))) return st;
+        }
+        if (gy) {
+            const int64_t rows = op == kOpPairwise ? items * ncy : ny * ncy;
+            aux.gy<<<(unsigned)((rows * 32 + 255) / 256), 256, 0, stream>>>(cp);
+            if ((st = launched("y contraction launch"))) return st;
+        }
+    }
+    if (gx) {
+        const int64_t tot = nx * lx * d;
+        aux.points<<<(unsigned)((tot + 255) / 256), 256, 0, stream>>>(gdx, nx, lx, d, fs, sx, in64, gx);
+        if ((st = launched("x point-gradient launch"))) return st;
+    }
+    if (gy) {
+        const int64_t tot = ny_paths * ly * d;
+        aux.points<<<(unsigned)((tot + 255) / 256), 256, 0, stream>>>(gdy, ny_paths, ly, d, 1.0, sy, in64, gy);
+        if ((st = launched("y point-gradient launch"))) return st;
+    }
+    return SIGK_OK;
+}
+
 int run_pairs(int op, const void *x, const void *y, int64_t nx, int64_t ny, int64_t lx, int64_t ly, int64_t d,
               int dtype, int order, double static_scale, const void *sx, const void *sy, void *out, int64_t out_ld,
               int precision, void *ws, size_t ws_bytes, cudaStream_t stream)
@@ -1145,6 +1359,52 @@ int sigk_gram_static(int op, int kind, double param, const void *x, const void *
     if (((uintptr_t)workspace & 255) != 0) return fail(SIGK_EINVAL, "workspace must be 256-byte aligned");
     return run_pairs_static(t, kop, kind, param, x, y, n_x, n_y, len_x, len_y, dim, dtype, order, scale_x, scale_y,
                             out, n_y, workspace, (cudaStream_t)stream);
+}
+
+size_t sigk_backward_workspace_size(int op, int64_t n_x, int64_t n_y, int64_t len_x, int64_t len_y, int64_t dim,
+                                    int order, int dtype)
+{
+    (void)dtype;
+    if (op != SIGK_OP_PAIRWISE && op != SIGK_OP_GRAM) return 0;
+    if (len_x < 2 || len_y < 2 || order < 0 || order > 12 || dim < 1 || n_x < 1 || n_y < 1) return 0;
+    if (op == SIGK_OP_PAIRWISE) n_y = n_x;
+    GradPlan g = make_grad_plan(op == SIGK_OP_PAIRWISE ? kOpPairwise : kOpGram, n_x, n_y, len_x - 1, len_y - 1, dim,
+                                order);
+    return g.ok ? g.ws_bytes : 0;
+}
+
+int sigk_backward(int op, const void *x, const void *y, int64_t n_x, int64_t n_y, int64_t len_x, int64_t len_y,
+                  int64_t dim, int dtype, int order, double static_scale, const void *scale_x, const void *scale_y,
+                  const void *grad_out, void *grad_x, void *grad_y, void *workspace, size_t workspace_bytes,
+                  sigk_stream_t stream)
+{
+    if (op != SIGK_OP_PAIRWISE && op != SIGK_OP_GRAM)
+        return fail(SIGK_EINVAL, "op must be SIGK_OP_PAIRWISE or SIGK_OP_GRAM (got %d)", op);
+    int st = check_common(dtype, SIGK_PREC_FP64, order);
+    if (st) return st;
+    if (op == SIGK_OP_PAIRWISE) n_y = n_x;
+    if (n_x < 1 || n_y < 1) return fail(SIGK_EINVAL, "path counts must be >= 1 (got %lld, %lld)", (long long)n_x,
+                                        (long long)n_y);
+    if (len_x < 2 || len_y < 2) return fail(SIGK_EINVAL, "path lengths must be >= 2 (got %lld, %lld)",
+                                            (long long)len_x, (long long)len_y);
+    if (dim < 1) return fail(SIGK_EINVAL, "dim must be >= 1");
+    if (order > kGradMaxOrder)
+        return fail(SIGK_EUNSUPPORTED, "the backward pass takes dyadic order <= %d (got %d)", kGradMaxOrder, order);
+    if (!grad_x && !grad_y) return SIGK_OK;
+    if ((st = check_dev(x, "x", false)) || (st = check_dev(y, "y", false)) ||
+        (st = check_dev(grad_out, "grad_out", false)) || (st = check_dev(grad_x, "grad_x", true)) ||
+        (st = check_dev(grad_y, "grad_y", true)) || (st = check_dev(scale_x, "scale_x", true)) ||
+        (st = check_dev(scale_y, "scale_y", true)))
+        return st;
+    const int kop = op == SIGK_OP_PAIRWISE ? kOpPairwise : kOpGram;
+    GradPlan g = make_grad_plan(kop, n_x, n_y, len_x - 1, len_y - 1, dim, order);
+    if (!g.ok) return fail(SIGK_EUNSUPPORTED, "no backward plan");
+    if (!workspace || workspace_bytes < g.ws_bytes)
+        return fail(SIGK_ENOMEM, "workspace of %zu bytes needed (got %zu)", g.ws_bytes,
+                    workspace ? workspace_bytes : 0);
+    if (((uintptr_t)workspace & 255) != 0) return fail(SIGK_EINVAL, "workspace must be 256-byte aligned");
+    return run_backward(g, kop, x, y, n_x, n_y, len_x, len_y, dim, dtype, order, static_scale, scale_x, scale_y,
+                        grad_out, grad_x, grad_y, workspace, (cudaStream_t)stream);
 }
 
 // Shared body of sigk_normalize, sigk_normalize_inc and sigk_self_norms

@@ -124,6 +124,89 @@ def log_normalizer(x):
     return 2 - 1 / (1 + x.log())
 
 
+def _wants_grad(*ts) -> bool:
+    return torch.is_grad_enabled() and any(isinstance(t, torch.Tensor) and t.requires_grad for t in ts)
+
+
+class _LinearSigKernel(torch.autograd.Function):
+    """Differentiable LinearKernel values: pairwise, Gram and symmetric Gram.
+
+    The forward is the solver's own path (any precision); the backward runs
+    sigk_backward, the adjoint of the float64 scheme, for the gradients with
+    respect to the points of x and y.  Per-path scales are constants.  The
+    reference has no backward pass (its Numba kernels end autograd)."""
+
+    @staticmethod
+    def forward(ctx, x, y, sx, sy, solver, op):
+        if op == "pairwise":
+            out = solver.pairwise(x, y, sx, sy)
+        elif op == "gram":
+            out = solver._gram(x, y, sx, sy, 1000)
+        else:
+            out = solver._gram_sym(x, sx, 1000)
+        ctx.solver = solver
+        ctx.op = op
+        ctx.save_for_backward(x, y, sx, sy)
+        return out
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        x, y, sx, sy = ctx.saved_tensors
+        solver, op = ctx.solver, ctx.op
+        self_pairs = y is None  # k(x_i, x_j) / k(x_b, x_b): both sides are x
+        yy = x if self_pairs else y
+        if self_pairs:
+            sy = sx
+        kop = _lib.SIGK_OP_PAIRWISE if op == "pairwise" else _lib.SIGK_OP_GRAM
+        need_x = ctx.needs_input_grad[0]
+        need_y = (not self_pairs) and ctx.needs_input_grad[1]
+        if not (need_x or need_y):
+            return None, None, None, None, None, None
+        x = x.contiguous()
+        yy = yy.contiguous()
+        g = grad_out.detach().to(dtype=x.dtype).contiguous()
+        gx = torch.empty_like(x) if (need_x or self_pairs) else None
+        gy = torch.empty_like(yy) if (need_y or self_pairs) else None
+        Nx, Ny = x.shape[0], yy.shape[0]
+        dt = _dtype_code(x)
+        with torch.cuda.device(x.device):
+            n = _lib.lib().sigk_backward_workspace_size(kop, Nx, Ny, x.shape[1], yy.shape[1], x.shape[2],
+                                                        solver.dyadic_order, dt)
+            ws = torch.empty(n, dtype=torch.uint8, device=x.device)
+            _lib.call("sigk_backward", kop, _ptr(x), _ptr(yy), Nx, Ny, x.shape[1], yy.shape[1], x.shape[2], dt,
+                      solver.dyadic_order, float(solver.static_kernel.scale), _ptr(sx), _ptr(sy), _ptr(g), _ptr(gx),
+                      _ptr(gy), _ptr(ws), n, _stream())
+        if self_pairs:
+            return gx + gy, None, None, None, None, None
+        return gx, gy, None, None, None, None
+
+
+def _differentiable(solver, op, x, y, x_scale, y_scale, n_y):
+    """Route a call whose paths require grad through _LinearSigKernel."""
+    if not _is_fused_linear(solver.static_kernel):
+        raise NotImplementedError("gradients are implemented for LinearKernel")
+    if _wants_grad(x_scale, y_scale):
+        raise NotImplementedError("gradients with respect to the path scales are not implemented")
+    _check_paths(x, "x")
+    if y is not None:
+        _check_paths(y, "y")
+    n_x = x.shape[0]
+    if op == "pairwise":
+        yv = x if y is None else y
+        ys = x_scale if y is None else y_scale
+        scaled = x_scale is not None or ys is not None
+        sx = _broadcast_scale(x_scale, n_x, x) if scaled else None
+        sy = _broadcast_scale(ys, n_x, yv) if scaled else None
+        return _LinearSigKernel.apply(x, y, sx, sy, solver, op)
+    if op == "gram":
+        scaled = x_scale is not None or y_scale is not None
+        sx = _broadcast_scale(x_scale, n_x, x) if scaled else None
+        sy = _broadcast_scale(y_scale, n_y, y) if scaled else None
+        return _LinearSigKernel.apply(x, y, sx, sy, solver, op)
+    sx = _broadcast_scale(x_scale, n_x, x)
+    return _LinearSigKernel.apply(x, None, sx, None, solver, op)
+
+
 def _batches(n, size):
     size = max(1, int(size))
     for start in range(0, n, size):
@@ -144,6 +227,8 @@ class SigPDE:
 
     # ------------------------------------------------------------------ pairwise
     def pairwise(self, x, y=None, x_scale=None, y_scale=None, max_batch=1000, max_threads=1024):
+        if _wants_grad(x, y):
+            return _differentiable(self, "pairwise", x, y, x_scale, y_scale, None)
         y_scale = x_scale if y is None else y_scale
         y = x if y is None else y
         _check_paths(x, "x")
@@ -191,6 +276,10 @@ class SigPDE:
 
     # ------------------------------------------------------------------ gram
     def gram(self, x, y=None, x_scale=None, y_scale=None, max_batch=1000, max_threads=1024):
+        if _wants_grad(x, y):
+            if y is None:
+                return _differentiable(self, "gram_sym", x, None, x_scale, None, None)
+            return _differentiable(self, "gram", x, y, x_scale, y_scale, y.shape[0])
         if y is None:
             return self._gram_sym(x, x_scale, max_batch)
         return self._gram(x, y, x_scale, y_scale, max_batch)
@@ -361,6 +450,9 @@ class RobustSigPDE:
 
     def pairwise(self, x, y=None, normalizer=None, tol=1e-8, maxit=100, max_batch=1000, max_threads=1024):
         """Robust pairwise kernel (sigpde/torch/kernel.py:232-291)."""
+        if _wants_grad(x, y):
+            raise NotImplementedError("gradients through the robust normalisation are not implemented "
+                                      "(RobustSigPDE.gram with explicit scales is differentiable in the paths)")
         solver = SigPDE(self.static_kernel, self.dyadic_order, self.precision)
         lx = self.normalization(x, normalizer, tol, maxit, max_batch, max_threads)
         if y is None:
@@ -371,6 +463,9 @@ class RobustSigPDE:
     def gram(self, x, y=None, x_scale=None, y_scale=None, normalizer=None, tol=1e-8, maxit=100, max_batch=1000,
              max_threads=1024):
         """Robust Gram (sigpde/torch/kernel.py:293-301): given scales skip the normalisation."""
+        if (x_scale is None and _wants_grad(x)) or (y is not None and y_scale is None and _wants_grad(y)):
+            raise NotImplementedError("gradients through the robust normalisation are not implemented "
+                                      "(pass x_scale / y_scale to differentiate with the scales held fixed)")
         xs = self.normalization(x, normalizer, tol, maxit, max_batch, max_threads) if x_scale is None else x_scale
         if y is None:
             ys = None

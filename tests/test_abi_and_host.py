@@ -145,3 +145,35 @@ def test_static_gram_argument_checks(built_lib):
                                         _lib.SIGK_F32, _lib.SIGK_PREC_FP64) == 0
     assert L.sigk_static_workspace_size(_lib.SIGK_OP_GRAM, 9, 3, 3, 10, 10, 4, 1, _lib.SIGK_F32,
                                         _lib.SIGK_PREC_FP64) == 0
+
+
+def test_backward_argument_checks(built_lib):
+    """sigk_backward rejects bad arguments before any device call."""
+    from sigpde_b200 import _lib
+    L = _lib.lib()
+
+    def call(op=_lib.SIGK_OP_GRAM, order=1, dim=3, length=8):
+        return L.sigk_backward(op, None, None, 2, 3, length, length, dim, _lib.SIGK_F32, order, 1.0, None, None,
+                               None, None, None, None, 0, None)
+
+    assert call(op=_lib.SIGK_OP_GRAM_SYM) == _lib.SIGK_EINVAL
+    assert call(order=5) == _lib.SIGK_EUNSUPPORTED
+    assert "order <= 4" in _lib.last_error()
+    assert call(dim=0) == _lib.SIGK_EINVAL
+    assert call(length=1) == _lib.SIGK_EINVAL
+    assert call() == _lib.SIGK_OK  # no gradient requested: nothing to do
+    assert L.sigk_backward_workspace_size(_lib.SIGK_OP_GRAM_SYM, 2, 3, 8, 8, 3, 1, _lib.SIGK_F32) == 0
+    assert L.sigk_backward_workspace_size(_lib.SIGK_OP_GRAM, 2, 3, 8, 8, 3, 5, _lib.SIGK_F32) == 0
+
+
+def test_gradients_are_refused_where_not_implemented():
+    import sigpde_b200.torch as sig
+    from sigpde_b200.torch.kernel import _differentiable
+    x = torch.zeros((2, 5, 3), requires_grad=True)
+    with pytest.raises(NotImplementedError, match="LinearKernel"):
+        _differentiable(sig.SigPDE(sig.kernels.RBFKernel(), 1), "gram", x, x, None, None, 2)
+    with pytest.raises(NotImplementedError, match="scales"):
+        _differentiable(sig.SigPDE(sig.kernels.LinearKernel(), 1), "gram", x, x,
+                        torch.ones(2, requires_grad=True), None, 2)
+    with pytest.raises(NotImplementedError, match="robust"):
+        sig.RobustSigPDE(sig.kernels.LinearKernel()).gram(x)

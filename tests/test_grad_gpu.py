@@ -1,0 +1,152 @@
+"""Backward pass (sigk_backward, autograd through sigpde_b200.torch) against
+the oracle's gradients, which are pinned by central differences of the
+oracle's solve (tests/test_oracle_grad.py).
+
+Tolerance: float64 paths, max |got - want| <= 1e-9 * max |want| (the adjoint
+runs in float64 with the same increments as the forward; only summation
+order differs); float32 paths return float32 gradients: 2e-6 relative to
+max |want|.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-9
+TOL32 = 2e-6
+
+
+def cuda(a, dtype=torch.float64, grad=False):
+    t = torch.as_tensor(np.asarray(a), dtype=dtype, device="cuda")
+    return t.requires_grad_(grad)
+
+
+def host(t):
+    return t.detach().double().cpu().numpy()
+
+
+def close(got, want, tol, msg=""):
+    err = np.max(np.abs(got - want)) / max(np.max(np.abs(want)), 1e-300)
+    assert err <= tol, f"{msg}: error {err:.3e} relative to max |grad| > {tol:.1e}"
+
+
+@pytest.fixture(scope="module")
+def sig():
+    import sigpde_b200.torch as sig
+    return sig
+
+
+@pytest.mark.parametrize("shape", [
+    # (batch, L_x, L_y, d, order)
+    (5, 9, 11, 3, 0),
+    (4, 20, 17, 4, 1),
+    (3, 33, 40, 2, 2),
+    (3, 12, 9, 5, 3),
+    (2, 8, 10, 3, 4),
+    (2, 70, 30, 2, 3),   # 552 refined rows: two bands of 512
+    (6, 2, 3, 1, 0),     # one coarse row
+])
+def test_pairwise_gradients(sig, oracle, shape):
+    B, lx, ly, d, o = shape
+    x = oracle.brownian(B, lx, d, 1 + lx)
+    y = oracle.brownian(B, ly, d, 2 + ly)
+    w = np.linspace(-1.0, 1.5, B)
+    X, Y = cuda(x, grad=True), cuda(y, grad=True)
+    k = sig.SigPDE(sig.kernels.LinearKernel(0.8), o)
+    out = k.pairwise(X, Y)
+    np.testing.assert_allclose(host(out), oracle.pairwise(x, y, o, static_param=0.8), rtol=1e-9)
+    out.backward(cuda(w))
+    gx, gy = oracle.grad_pairwise(x, y, o, w, static_scale=0.8)
+    close(host(X.grad), gx, TOL64, "grad x")
+    close(host(Y.grad), gy, TOL64, "grad y")
+
+
+@pytest.mark.parametrize("shape", [(4, 3, 15, 13, 3, 1), (3, 5, 40, 33, 8, 2), (6, 2, 7, 70, 2, 0)])
+def test_gram_gradients_with_scales(sig, oracle, shape):
+    nx, ny, lx, ly, d, o = shape
+    x = oracle.brownian(nx, lx, d, 10 + lx)
+    y = oracle.brownian(ny, ly, d, 20 + ly)
+    sx = np.linspace(0.6, 1.4, nx)
+    sy = np.linspace(1.2, 0.7, ny)
+    w = np.random.default_rng(5).standard_normal((nx, ny))
+    X, Y = cuda(x, grad=True), cuda(y, grad=True)
+    k = sig.SigPDE(sig.kernels.LinearKernel(), o)
+    G = k.gram(X, Y, cuda(sx), cuda(sy))
+    (G * cuda(w)).sum().backward()
+    gx, gy = oracle.grad_gram(x, y, o, w, sx, sy)
+    close(host(X.grad), gx, TOL64, "grad x")
+    close(host(Y.grad), gy, TOL64, "grad y")
+
+
+def test_symmetric_gram_and_self_pairwise_gradients(sig, oracle):
+    x = oracle.brownian(5, 24, 3, 31)
+    w = np.random.default_rng(6).standard_normal((5, 5))
+    X = cuda(x, grad=True)
+    k = sig.SigPDE(sig.kernels.LinearKernel(), 2)
+    (k.gram(X) * cuda(w)).sum().backward()
+    close(host(X.grad), oracle.grad_gram(x, None, 2, w), TOL64, "symmetric gram")
+    X2 = cuda(x, grad=True)
+    wp = np.linspace(0.5, 2.0, 5)
+    (k.pairwise(X2) * cuda(wp)).sum().backward()
+    gx, gy = oracle.grad_pairwise(x, x, 2, wp)
+    close(host(X2.grad), gx + gy, TOL64, "pairwise(x)")
+
+
+def test_float32_paths_and_one_sided_gradients(sig, oracle):
+    x = oracle.brownian(4, 18, 3, 41)
+    y = oracle.brownian(3, 21, 3, 42)
+    X = cuda(x, torch.float32, grad=True)
+    Y = cuda(y, torch.float32)
+    k = sig.SigPDE(sig.kernels.LinearKernel(), 1)
+    G = k.gram(X, Y)
+    assert G.requires_grad and G.dtype == torch.float32
+    G.sum().backward()
+    assert X.grad.dtype == torch.float32 and Y.grad is None
+    gx, _ = oracle.grad_gram(host(X), host(Y), 1, np.ones((4, 3)))
+    close(host(X.grad), gx, TOL32, "float32 grad x")
+
+
+def test_chunked_backward_matches(sig, oracle, monkeypatch):
+    """Chunks of x paths (a 1 MB cap) give the same gradients up to summation order."""
+    x = oracle.brownian(9, 30, 3, 51)
+    y = oracle.brownian(7, 26, 3, 52)
+    k = sig.SigPDE(sig.kernels.LinearKernel(), 2)
+    w = cuda(np.random.default_rng(7).standard_normal((9, 7)))
+
+    def grads():
+        X, Y = cuda(x, grad=True), cuda(y, grad=True)
+        (k.gram(X, Y) * w).sum().backward()
+        return host(X.grad), host(Y.grad)
+
+    a = grads()
+    monkeypatch.setenv("SIGK_GRAD_CHUNK_MB", "1")
+    b = grads()
+    for u, v in zip(a, b):
+        close(v, u, 1e-13, "chunked")
+
+
+def test_gradcheck_small(sig):
+    """torch.autograd.gradcheck: the backward against finite differences of the forward."""
+    rng = np.random.default_rng(8)
+    x = cuda(rng.standard_normal((2, 5, 2)) * 0.4, grad=True)
+    y = cuda(rng.standard_normal((3, 4, 2)) * 0.4, grad=True)
+    k = sig.SigPDE(sig.kernels.LinearKernel(), 1)
+    assert torch.autograd.gradcheck(lambda a, b: k.gram(a, b), (x, y), eps=1e-6, atol=1e-7, rtol=1e-6)
+    assert torch.autograd.gradcheck(lambda a, b: k.pairwise(a, b[:2]), (x, y), eps=1e-6, atol=1e-7, rtol=1e-6)
+
+
+def test_backward_refusals(sig):
+    x = cuda(np.zeros((2, 5, 2)), grad=True)
+    with pytest.raises(NotImplementedError):
+        sig.SigPDE(sig.kernels.RBFKernel(), 1).gram(x)
+    with pytest.raises(NotImplementedError):
+        sig.RobustSigPDE(sig.kernels.LinearKernel(), 1).pairwise(x)
+    from sigpde_b200._lib import SigkError
+    with pytest.raises(SigkError, match="order <= 4"):
+        sig.SigPDE(sig.kernels.LinearKernel(), 5).gram(x, x).sum().backward()
+    # robust Gram with fixed scales is differentiable in the paths
+    g = sig.RobustSigPDE(sig.kernels.LinearKernel(), 1).gram(x, None, cuda([0.5, 0.9]))
+    g.sum().backward()
+    assert x.grad is not None
