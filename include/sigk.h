@@ -181,7 +181,7 @@ SIGK_API int sigk_gram_static(int op, int kind, double param, const void *x, con
  *   be NULL (not computed).  For a symmetric Gram pass y = x and add the two.
  * Dyadic order <= 4 (SIGK_EUNSUPPORTED above).  Workspace:
  * sigk_backward_workspace_size(...) bytes, 256-byte aligned (pairs are taken
- * in chunks of x paths so that it stays near 4 GiB plus the inputs' size).
+ * in chunks of x paths so that it stays near 8 GiB plus the inputs' size).
  */
 SIGK_API size_t sigk_backward_workspace_size(int op, int64_t n_x, int64_t n_y, int64_t len_x, int64_t len_y,
                                              int64_t dim, int order, int dtype);

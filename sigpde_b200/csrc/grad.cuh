@@ -45,7 +45,8 @@ struct GradParams {
     const void *w;        // weights (grad_out): pairwise (n,), Gram (n_x, n_y) row-major; input dtype
     int in64;
     int64_t x0;           // first x path of the chunk
-    double *dbuf;         // D of every fine cell, per pair nbands * m * 32 * R doubles
+    double *dbuf;         // D of every fine cell, per pair nbands * (m + 31) * R * 32 doubles, laid out
+                          // [band][step][row of the lane][lane] so that each store / load is coalesced
     double *bnd;          // per pair 2 * (m + 2) doubles: band boundary rows
 };
 
@@ -81,7 +82,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) grad_fwd_kernel(GradParam
         int64_t xi, yj, row_ld;
         double *base;
         grad_item(p, it, xi, yj, base, row_ld);
-        double *D = p.dbuf + it * (int64_t)nb * m * 32 * R;
+        double *D = p.dbuf + it * (int64_t)nb * (m + 31) * R * 32;
         double *bnd = p.bnd + it * 2 * (int64_t)(m + 2); // K of the row above the band, columns 0..m
         for (int b = 0; b < nb; ++b) {
             const int p0 = b * 32 * R + lane * R + 1; // this lane's first fine row (1-based)
@@ -90,7 +91,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) grad_fwd_kernel(GradParam
 #pragma unroll
             for (int r = 0; r < R; ++r) left[r] = 1.0; // K(p, 0)
             double bot = 1.0, corner = 1.0;            // lane l-1's last row at q-1 (as received), at q-2
-            double c[RC], A[RC], B[RC], Ad[RC], Bd[RC];
+            double c[RC], A[RC], B[RC], Ad[RC], Bd[RC], cn[RC];
+#pragma unroll
+            for (int rc = 0; rc < RC; ++rc) // increments of coarse column 0, then one column ahead
+                cn[rc] = ci0 + rc < p.ncx ? base[ci0 + rc] : 0.0;
             __syncwarp();
             for (int s = 0; s < m + 31; ++s) {
                 const double from_above = __shfl_up_sync(0xffffffffu, bot, 1);
@@ -104,25 +108,26 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) grad_fwd_kernel(GradParam
                         top = from_above;
                         diag = q == 1 ? 1.0 : corner;
                     }
-                    if (q == 1 || ((q - 1) & ((1 << O) - 1)) == 0) { // a new coarse column
+                    if (((q - 1) & ((1 << O) - 1)) == 0) { // a new coarse column
                         const int cj = (q - 1) >> O;
 #pragma unroll
                         for (int rc = 0; rc < RC; ++rc) {
                             const int ci = ci0 + rc;
-                            c[rc] = ci < p.ncx ? base[(int64_t)cj * row_ld + ci] : 0.0;
+                            c[rc] = cn[rc];
+                            cn[rc] = (ci < p.ncx && cj + 1 < p.ncy) ? base[(int64_t)(cj + 1) * row_ld + ci] : 0.0;
                             stencil_coefs(c[rc], A[rc], B[rc]);
                             Ad[rc] = fma(c[rc], 1.0 / 6.0, 0.5);
                             Bd[rc] = c[rc] * (-1.0 / 6.0);
                         }
                     }
-                    double *dq = D + (((int64_t)b * m + (q - 1)) * 32 + lane) * R;
+                    double *dq = D + ((int64_t)b * (m + 31) + s) * R * 32 + lane;
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
                         const int rc = r >> O;
                         const double sum = left[r] + top;
                         const double k = sum * A[rc] - diag * B[rc];
                         const bool valid = p0 + r <= n;
-                        dq[r] = valid ? sum * Ad[rc] - diag * Bd[rc] : 0.0;
+                        dq[r * 32] = valid ? sum * Ad[rc] - diag * Bd[rc] : 0.0;
                         diag = left[r];
                         left[r] = valid ? k : 0.0;
                         top = left[r];
@@ -139,10 +144,16 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) grad_fwd_kernel(GradParam
     }
 }
 
+// steps of D in flight per lane in the adjoint (the ring stays within 32 KB of static shared memory)
+template <int R>
+constexpr int grad_prefetch() { return R >= 16 ? 1 : (R >= 8 ? 3 : 4); }
+
 template <int R, int O>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) grad_bwd_kernel(GradParams p)
 {
     static_assert(R >= (1 << O), "a lane's rows hold whole coarse rows");
+    constexpr int kGradPrefetch = grad_prefetch<R>();
+    __shared__ double dring[kWarpsPerBlock][kGradPrefetch + 1][R][32];
     constexpr int RC = R >> O;
     const int lane = threadIdx.x & 31;
     const int64_t gwarp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -156,7 +167,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) grad_bwd_kernel(GradParam
         const int64_t widx = p.op == kOpPairwise ? xi : xi * p.ny + yj;
         const double w = p.in64 ? reinterpret_cast<const double *>(p.w)[widx]
                                 : (double)reinterpret_cast<const float *>(p.w)[widx];
-        const double *D = p.dbuf + it * (int64_t)nb * m * 32 * R;
+        const double *D = p.dbuf + it * (int64_t)nb * (m + 31) * R * 32;
         double *bP = p.bnd + it * 2 * (int64_t)(m + 2); // P and Q of the row below the band, columns 0..m+1
         double *bQ = bP + (m + 2);
         for (int b = nb - 1; b >= 0; --b) {
@@ -170,12 +181,39 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) grad_bwd_kernel(GradParam
             for (int rc = 0; rc < RC; ++rc) g[rc] = 0.0;
             double topP = 0.0, topQ = 0.0; // this lane's row 0 P, Q at its last column (published)
             double belowQ_prev = 0.0;      // lane l+1's row 0 Q at column q + 1
-            double c[RC], A[RC], B[RC];
+            double c[RC], A[RC], B[RC], cn[RC];
+#pragma unroll
+            for (int rc = 0; rc < RC; ++rc) // increments of the last coarse column, then one column ahead
+                cn[rc] = ci0 + rc < p.ncx ? base[(int64_t)(p.ncy - 1) * row_ld + ci0 + rc] : 0.0;
+            // each step's D arrives through this lane's cp.async ring, kGradPrefetch steps ahead (only the
+            // issuing lane reads a slot, after cp.async.wait_group)
+            const double *Db = D + (int64_t)b * (m + 31) * R * 32 + lane;
+            double *ring = &dring[threadIdx.x >> 5][0][0][lane];
+            int rd = 0, wr = 0, snext = m + 30;
+            auto fetch = [&]() {
+                if (snext >= 0) {
+#pragma unroll
+                    for (int r = 0; r < R; ++r)
+                        cp_async_zfill<8>((uint32_t)__cvta_generic_to_shared(ring + (wr * R + r) * 32),
+                                          Db + ((int64_t)snext * R + r) * 32, 8);
+                    --snext;
+                }
+                cp_async_commit(); // empty groups past the end keep the count uniform
+                if (++wr == kGradPrefetch + 1) wr = 0;
+            };
+#pragma unroll 1
+            for (int i = 0; i < kGradPrefetch; ++i) fetch();
             __syncwarp();
             for (int s = m + 30; s >= 0; --s) {
                 const double belowP = __shfl_down_sync(0xffffffffu, topP, 1);
                 const double belowQ = __shfl_down_sync(0xffffffffu, topQ, 1);
                 const int q = s - lane + 1;
+                cp_async_wait<kGradPrefetch - 1>(); // step s has landed
+                double dq[R];
+#pragma unroll
+                for (int r = 0; r < R; ++r) dq[r] = ring[(rd * R + r) * 32];
+                if (++rd == kGradPrefetch + 1) rd = 0;
+                fetch();
                 if (q >= 1 && q <= m) {
                     double dP, dQ; // P(p+1, q) and Q(p+1, q+1) for the lane's last row
                     if (lane == 31) {
@@ -191,11 +229,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) grad_bwd_kernel(GradParam
 #pragma unroll
                         for (int rc = 0; rc < RC; ++rc) {
                             const int ci = ci0 + rc;
-                            c[rc] = ci < p.ncx ? base[(int64_t)cj * row_ld + ci] : 0.0;
+                            c[rc] = cn[rc];
+                            cn[rc] = (ci < p.ncx && cj > 0) ? base[(int64_t)(cj - 1) * row_ld + ci] : 0.0;
                             stencil_coefs(c[rc], A[rc], B[rc]);
                         }
                     }
-                    const double *dq = D + (((int64_t)b * m + (q - 1)) * 32 + lane) * R;
 #pragma unroll
                     for (int r = R - 1; r >= 0; --r) {
                         const int rc = r >> O;
@@ -227,6 +265,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) grad_bwd_kernel(GradParam
                 }
                 belowQ_prev = belowQ;
             }
+            cp_async_wait<0>();
             __syncwarp();
             if (lane == 0 && b > 0) {
                 bP[m + 1] = 0.0;

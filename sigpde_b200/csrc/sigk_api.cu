@@ -810,7 +810,7 @@ int run_pairs_static(const TcPlan &t, int op, int kind, double param, const void
 // matrix stay under kGradChunkBytes (SIGK_GRAD_CHUNK_MB overrides).
 // Workspace: zero word | x, y differences | dk/d(x diff), dk/d(y diff) |
 // partial sums of the x contraction | increment matrix | D | boundary rows.
-constexpr size_t kGradChunkBytes = 4ull << 30;
+constexpr size_t kGradChunkBytes = 8ull << 30;
 constexpr int kGradMaxOrder = 4;
 constexpr int64_t kGradSlices = 64;
 
@@ -827,13 +827,16 @@ GradPlan make_grad_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy
     GradPlan g;
     if (order > kGradMaxOrder) return g;
     const int64_t n = ncx << order, m = ncy << order;
+    // rows per lane: the smallest power of two with 32R >= n, at most 8 (bands of 256 rows keep the
+    // adjoint's registers near 128), and at least 2^order (a lane holds whole coarse rows)
     int R = 1;
-    while (R < 16 && (R < (1 << order) || 32 * R < n)) R *= 2;
+    while (R < 8 && 32 * R < n) R *= 2;
+    while (R < (1 << order)) R *= 2;
     g.R = R;
     g.O = order;
     g.nb = (int)((n + 32 * R - 1) / (32 * R));
     g.rows_x = (ncx + 3) / 4 * 4;
-    const size_t dbytes = (size_t)g.nb * m * 32 * R * sizeof(double);
+    const size_t dbytes = (size_t)g.nb * (m + 31) * R * 32 * sizeof(double);
     const size_t bbytes = 2 * (size_t)(m + 2) * sizeof(double);
     const size_t mbytes = (size_t)ncy * g.rows_x * sizeof(double);
     const int64_t items_per_x = op == kOpPairwise ? 1 : ny;
