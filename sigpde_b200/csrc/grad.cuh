@@ -16,9 +16,13 @@
 //
 // Kernels
 //   grad_fwd_kernel  one warp per pair: the forward wavefront (R rows a lane,
-//                    one fine column a step, bands of 32R rows) storing D of
-//                    every fine cell;
-//   grad_bwd_kernel  one warp per pair: the same schedule in reverse for
+//                    one fine column a step, bands of 32R rows) storing the
+//                    top input of every lane step and each lane's rows at the
+//                    start of every segment of T = 32/R steps;
+//   grad_bwd_kernel  one warp per pair: per segment (last first), each lane
+//                    recomputes its rows' K and D over the segment on its own
+//                    (no cross-lane dependency: its inputs were stored), then
+//                    the adjoint runs the same schedule in reverse for
 //                    Lambda, summing Lambda D per coarse cell; each coarse
 //                    cell's rows belong to one lane (R >= 2^order), so the
 //                    sum is written once, over the cell's increment in the
@@ -45,8 +49,7 @@ struct GradParams {
     const void *w;        // weights (grad_out): pairwise (n,), Gram (n_x, n_y) row-major; input dtype
     int in64;
     int64_t x0;           // first x path of the chunk
-    double *dbuf;         // D of every fine cell, per pair nbands * (m + 31) * R * 32 doubles, laid out
-                          // [band][step][row of the lane][lane] so that each store / load is coalesced
+    double *dbuf;         // per pair and band grad_band_doubles(m, R): top inputs and segment checkpoints
     double *bnd;          // per pair 2 * (m + 2) doubles: band boundary rows
 };
 
@@ -68,39 +71,94 @@ __device__ __forceinline__ void grad_item(const GradParams &p, int64_t it, int64
     }
 }
 
+// Steps per recompute segment: T * R = 32 doubles of D per lane in shared memory.
+template <int R>
+constexpr int grad_seg() { return 32 / R; }
+
+// Per pair and band, the forward pass stores what the adjoint needs to
+// recompute any segment of T steps lane by lane: the top input K(p0-1, q)
+// each lane used at every step ([step][lane]) and each lane's K(rows, q-1)
+// at the start of every segment ([segment][row][lane]).
+__host__ __device__ __forceinline__ int64_t grad_band_doubles(int m, int R)
+{
+    const int64_t S = m + 31, T = 32 / R, NS = (S + T - 1) / T;
+    return S * 32 + NS * R * 32;
+}
+
+// Coefficients of the lane's coarse rows for coarse column cj.
+template <int RC>
+__device__ __forceinline__ void grad_coefs(const double *base, int64_t row_ld, int ci0, int64_t ncx, int cj,
+                                           double (&A)[RC], double (&B)[RC], double (&Ad)[RC], double (&Bd)[RC])
+{
+#pragma unroll
+    for (int rc = 0; rc < RC; ++rc) {
+        const int ci = ci0 + rc;
+        const double c = ci < ncx ? base[(int64_t)cj * row_ld + ci] : 0.0;
+        stencil_coefs(c, A[rc], B[rc]);
+        Ad[rc] = fma(c, 1.0 / 6.0, 0.5);
+        Bd[rc] = c * (-1.0 / 6.0);
+    }
+}
+
+// One forward step of the lane's R rows at a column: left holds K(rows, q-1)
+// and becomes K(rows, q); rows beyond n hold 0.  D of each row goes to d[r * 32].
+template <int R, int O, bool WANT_D>
+__device__ __forceinline__ void grad_lane_step(double (&left)[R], double top, double diag, const double *A,
+                                               const double *B, const double *Ad, const double *Bd, int p0, int n,
+                                               double *d)
+{
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int rc = r >> O;
+        const double sum = left[r] + top;
+        const double k = sum * A[rc] - diag * B[rc];
+        const bool valid = p0 + r <= n;
+        if constexpr (WANT_D) d[r * 32] = valid ? sum * Ad[rc] - diag * Bd[rc] : 0.0;
+        diag = left[r];
+        left[r] = valid ? k : 0.0;
+        top = left[r];
+    }
+}
+
 template <int R, int O>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) grad_fwd_kernel(GradParams p)
 {
     static_assert(R >= (1 << O), "a lane's rows hold whole coarse rows");
     constexpr int RC = R >> O;
+    constexpr int T = grad_seg<R>();
     const int lane = threadIdx.x & 31;
     const int64_t gwarp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int n = (int)(p.ncx << p.order), m = (int)(p.ncy << p.order);
     const int nb = (n + 32 * R - 1) / (32 * R);
+    const int S = m + 31;
+    const int64_t band_doubles = grad_band_doubles(m, R);
     for (int64_t it = gwarp; it < p.nitems; it += nwarps) {
         int64_t xi, yj, row_ld;
         double *base;
         grad_item(p, it, xi, yj, base, row_ld);
-        double *D = p.dbuf + it * (int64_t)nb * (m + 31) * R * 32;
         double *bnd = p.bnd + it * 2 * (int64_t)(m + 2); // K of the row above the band, columns 0..m
         for (int b = 0; b < nb; ++b) {
+            double *tops = p.dbuf + (it * nb + b) * band_doubles + lane;
+            double *ck = tops + (int64_t)S * 32;
             const int p0 = b * 32 * R + lane * R + 1; // this lane's first fine row (1-based)
             const int ci0 = (p0 - 1) >> O;            // its first coarse row
             double left[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) left[r] = 1.0; // K(p, 0)
             double bot = 1.0, corner = 1.0;            // lane l-1's last row at q-1 (as received), at q-2
-            double c[RC], A[RC], B[RC], Ad[RC], Bd[RC], cn[RC];
-#pragma unroll
-            for (int rc = 0; rc < RC; ++rc) // increments of coarse column 0, then one column ahead
-                cn[rc] = ci0 + rc < p.ncx ? base[ci0 + rc] : 0.0;
+            double A[RC], B[RC], Ad[RC], Bd[RC];
             __syncwarp();
-            for (int s = 0; s < m + 31; ++s) {
+            for (int s = 0; s < S; ++s) {
                 const double from_above = __shfl_up_sync(0xffffffffu, bot, 1);
+                if (s % T == 0) {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) ck[((int64_t)(s / T) * R + r) * 32] = left[r];
+                }
                 const int q = s - lane + 1;
+                double top = 1.0;
                 if (q >= 1 && q <= m) {
-                    double top, diag;
+                    double diag;
                     if (lane == 0) {
                         top = b == 0 ? 1.0 : bnd[q];
                         diag = b == 0 ? 1.0 : bnd[q - 1];
@@ -108,34 +166,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) grad_fwd_kernel(GradParam
                         top = from_above;
                         diag = q == 1 ? 1.0 : corner;
                     }
-                    if (((q - 1) & ((1 << O) - 1)) == 0) { // a new coarse column
-                        const int cj = (q - 1) >> O;
-#pragma unroll
-                        for (int rc = 0; rc < RC; ++rc) {
-                            const int ci = ci0 + rc;
-                            c[rc] = cn[rc];
-                            cn[rc] = (ci < p.ncx && cj + 1 < p.ncy) ? base[(int64_t)(cj + 1) * row_ld + ci] : 0.0;
-                            stencil_coefs(c[rc], A[rc], B[rc]);
-                            Ad[rc] = fma(c[rc], 1.0 / 6.0, 0.5);
-                            Bd[rc] = c[rc] * (-1.0 / 6.0);
-                        }
-                    }
-                    double *dq = D + ((int64_t)b * (m + 31) + s) * R * 32 + lane;
-#pragma unroll
-                    for (int r = 0; r < R; ++r) {
-                        const int rc = r >> O;
-                        const double sum = left[r] + top;
-                        const double k = sum * A[rc] - diag * B[rc];
-                        const bool valid = p0 + r <= n;
-                        dq[r * 32] = valid ? sum * Ad[rc] - diag * Bd[rc] : 0.0;
-                        diag = left[r];
-                        left[r] = valid ? k : 0.0;
-                        top = left[r];
-                    }
+                    if (((q - 1) & ((1 << O) - 1)) == 0) // a new coarse column
+                        grad_coefs<RC>(base, row_ld, ci0, p.ncx, (q - 1) >> O, A, B, Ad, Bd);
+                    grad_lane_step<R, O, false>(left, top, diag, A, B, Ad, Bd, p0, n, nullptr);
                     if (lane == 31 && b + 1 < nb) bnd[q] = left[R - 1];
                     corner = from_above;
                     bot = left[R - 1];
                 }
+                tops[(int64_t)s * 32] = top;
             }
             __syncwarp();
             if (lane == 31 && b + 1 < nb) bnd[0] = 1.0;
@@ -144,22 +182,21 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) grad_fwd_kernel(GradParam
     }
 }
 
-// steps of D in flight per lane in the adjoint (the ring stays within 32 KB of static shared memory)
-template <int R>
-constexpr int grad_prefetch() { return R >= 16 ? 1 : (R >= 8 ? 3 : 4); }
-
 template <int R, int O>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) grad_bwd_kernel(GradParams p)
 {
     static_assert(R >= (1 << O), "a lane's rows hold whole coarse rows");
-    constexpr int kGradPrefetch = grad_prefetch<R>();
-    __shared__ double dring[kWarpsPerBlock][kGradPrefetch + 1][R][32];
     constexpr int RC = R >> O;
+    constexpr int T = grad_seg<R>();
+    __shared__ double dsm[kWarpsPerBlock][T][R][32]; // D of the current segment, per lane
     const int lane = threadIdx.x & 31;
     const int64_t gwarp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int n = (int)(p.ncx << p.order), m = (int)(p.ncy << p.order);
     const int nb = (n + 32 * R - 1) / (32 * R);
+    const int S = m + 31, NS = (S + T - 1) / T;
+    const int64_t band_doubles = grad_band_doubles(m, R);
+    double *dl = &dsm[threadIdx.x >> 5][0][0][lane];
     for (int64_t it = gwarp; it < p.nitems; it += nwarps) {
         int64_t xi, yj, row_ld;
         double *base;
@@ -167,10 +204,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) grad_bwd_kernel(GradParam
         const int64_t widx = p.op == kOpPairwise ? xi : xi * p.ny + yj;
         const double w = p.in64 ? reinterpret_cast<const double *>(p.w)[widx]
                                 : (double)reinterpret_cast<const float *>(p.w)[widx];
-        const double *D = p.dbuf + it * (int64_t)nb * (m + 31) * R * 32;
         double *bP = p.bnd + it * 2 * (int64_t)(m + 2); // P and Q of the row below the band, columns 0..m+1
         double *bQ = bP + (m + 2);
         for (int b = nb - 1; b >= 0; --b) {
+            const double *tops = p.dbuf + (it * nb + b) * band_doubles + lane;
+            const double *ck = tops + (int64_t)S * 32;
             const int p0 = b * 32 * R + lane * R + 1;
             const int ci0 = (p0 - 1) >> O;
             double Pr[R], Qr[R]; // P, Q of the lane's rows at column q + 1
@@ -181,91 +219,90 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) grad_bwd_kernel(GradParam
             for (int rc = 0; rc < RC; ++rc) g[rc] = 0.0;
             double topP = 0.0, topQ = 0.0; // this lane's row 0 P, Q at its last column (published)
             double belowQ_prev = 0.0;      // lane l+1's row 0 Q at column q + 1
-            double c[RC], A[RC], B[RC], cn[RC];
-#pragma unroll
-            for (int rc = 0; rc < RC; ++rc) // increments of the last coarse column, then one column ahead
-                cn[rc] = ci0 + rc < p.ncx ? base[(int64_t)(p.ncy - 1) * row_ld + ci0 + rc] : 0.0;
-            // each step's D arrives through this lane's cp.async ring, kGradPrefetch steps ahead (only the
-            // issuing lane reads a slot, after cp.async.wait_group)
-            const double *Db = D + (int64_t)b * (m + 31) * R * 32 + lane;
-            double *ring = &dring[threadIdx.x >> 5][0][0][lane];
-            int rd = 0, wr = 0, snext = m + 30;
-            auto fetch = [&]() {
-                if (snext >= 0) {
-#pragma unroll
-                    for (int r = 0; r < R; ++r)
-                        cp_async_zfill<8>((uint32_t)__cvta_generic_to_shared(ring + (wr * R + r) * 32),
-                                          Db + ((int64_t)snext * R + r) * 32, 8);
-                    --snext;
-                }
-                cp_async_commit(); // empty groups past the end keep the count uniform
-                if (++wr == kGradPrefetch + 1) wr = 0;
-            };
-#pragma unroll 1
-            for (int i = 0; i < kGradPrefetch; ++i) fetch();
+            double A[RC], B[RC], Ad[RC], Bd[RC];
             __syncwarp();
-            for (int s = m + 30; s >= 0; --s) {
-                const double belowP = __shfl_down_sync(0xffffffffu, topP, 1);
-                const double belowQ = __shfl_down_sync(0xffffffffu, topQ, 1);
-                const int q = s - lane + 1;
-                cp_async_wait<kGradPrefetch - 1>(); // step s has landed
-                double dq[R];
+            for (int k = NS - 1; k >= 0; --k) {
+                const int s0 = k * T;
+                // phase A: recompute this segment's steps lane by lane from the checkpoint and the
+                // stored top inputs, keeping D in shared memory
+                {
+                    double left[R], tp[T + 1];
 #pragma unroll
-                for (int r = 0; r < R; ++r) dq[r] = ring[(rd * R + r) * 32];
-                if (++rd == kGradPrefetch + 1) rd = 0;
-                fetch();
-                if (q >= 1 && q <= m) {
-                    double dP, dQ; // P(p+1, q) and Q(p+1, q+1) for the lane's last row
-                    if (lane == 31) {
-                        const bool last = b + 1 >= nb;
-                        dP = last ? 0.0 : bP[q];
-                        dQ = last ? 0.0 : bQ[q + 1];
-                    } else {
-                        dP = belowP;
-                        dQ = q == m ? 0.0 : belowQ_prev;
-                    }
-                    const int cj = (q - 1) >> O;
-                    if (q == m || (q & ((1 << O) - 1)) == 0) { // entering a coarse column (in reverse)
+                    for (int r = 0; r < R; ++r) left[r] = ck[((int64_t)k * R + r) * 32];
 #pragma unroll
-                        for (int rc = 0; rc < RC; ++rc) {
-                            const int ci = ci0 + rc;
-                            c[rc] = cn[rc];
-                            cn[rc] = (ci < p.ncx && cj > 0) ? base[(int64_t)(cj - 1) * row_ld + ci] : 0.0;
-                            stencil_coefs(c[rc], A[rc], B[rc]);
-                        }
+                    for (int t = 0; t <= T; ++t) {
+                        const int st = s0 - 1 + t;
+                        tp[t] = (st >= 0 && st < S) ? tops[(int64_t)st * 32] : 1.0;
                     }
+                    bool have = false;
 #pragma unroll
-                    for (int r = R - 1; r >= 0; --r) {
-                        const int rc = r >> O;
-                        const int pr = p0 + r;
-                        double lam = Pr[r] + dP - dQ;
-                        if (pr == n && q == m) lam += w;
-                        if (pr > n) lam = 0.0;
-                        g[rc] = fma(lam, dq[r], g[rc]);
-                        const double P = A[rc] * lam, Q = B[rc] * lam;
-                        dQ = Qr[r]; // Q(p, q+1) is the diagonal of the row above
-                        dP = P;
-                        Pr[r] = P;
-                        Qr[r] = Q;
-                    }
-                    topP = Pr[0];
-                    topQ = Qr[0];
-                    if (lane == 0 && b > 0) {
-                        bP[q] = Pr[0];
-                        bQ[q] = Qr[0];
-                    }
-                    if (((q - 1) & ((1 << O) - 1)) == 0) { // leaving the coarse column: dk/dc is complete
-#pragma unroll
-                        for (int rc = 0; rc < RC; ++rc) {
-                            const int ci = ci0 + rc;
-                            if (ci < p.ncx) base[(int64_t)cj * row_ld + ci] = g[rc];
-                            g[rc] = 0.0;
+                    for (int t = 0; t < T; ++t) {
+                        const int q = s0 + t - lane + 1;
+                        if (q >= 1 && q <= m) {
+                            if (!have || ((q - 1) & ((1 << O) - 1)) == 0)
+                                grad_coefs<RC>(base, row_ld, ci0, p.ncx, (q - 1) >> O, A, B, Ad, Bd);
+                            have = true;
+                            grad_lane_step<R, O, true>(left, tp[t + 1], q == 1 ? 1.0 : tp[t], A, B, Ad, Bd, p0, n,
+                                                       dl + t * R * 32);
                         }
                     }
                 }
-                belowQ_prev = belowQ;
+                // phase B: the adjoint over the same steps in reverse
+                bool have = false;
+#pragma unroll 1
+                for (int t = T - 1; t >= 0; --t) {
+                    const int s = s0 + t;
+                    if (s >= S) continue; // uniform: the last segment may be short
+                    const double belowP = __shfl_down_sync(0xffffffffu, topP, 1);
+                    const double belowQ = __shfl_down_sync(0xffffffffu, topQ, 1);
+                    const int q = s - lane + 1;
+                    if (q >= 1 && q <= m) {
+                        double dP, dQ; // P(p+1, q) and Q(p+1, q+1) for the lane's last row
+                        if (lane == 31) {
+                            const bool last = b + 1 >= nb;
+                            dP = last ? 0.0 : bP[q];
+                            dQ = last ? 0.0 : bQ[q + 1];
+                        } else {
+                            dP = belowP;
+                            dQ = q == m ? 0.0 : belowQ_prev;
+                        }
+                        const int cj = (q - 1) >> O;
+                        if (!have || q == m || (q & ((1 << O) - 1)) == 0)
+                            grad_coefs<RC>(base, row_ld, ci0, p.ncx, cj, A, B, Ad, Bd);
+                        have = true;
+                        const double *dq = dl + t * R * 32;
+#pragma unroll
+                        for (int r = R - 1; r >= 0; --r) {
+                            const int rc = r >> O;
+                            const int pr = p0 + r;
+                            double lam = Pr[r] + dP - dQ;
+                            if (pr == n && q == m) lam += w;
+                            if (pr > n) lam = 0.0;
+                            g[rc] = fma(lam, dq[r * 32], g[rc]);
+                            const double P = A[rc] * lam, Q = B[rc] * lam;
+                            dQ = Qr[r]; // Q(p, q+1) is the diagonal of the row above
+                            dP = P;
+                            Pr[r] = P;
+                            Qr[r] = Q;
+                        }
+                        topP = Pr[0];
+                        topQ = Qr[0];
+                        if (lane == 0 && b > 0) {
+                            bP[q] = Pr[0];
+                            bQ[q] = Qr[0];
+                        }
+                        if (((q - 1) & ((1 << O) - 1)) == 0) { // leaving the coarse column: dk/dc is complete
+#pragma unroll
+                            for (int rc = 0; rc < RC; ++rc) {
+                                const int ci = ci0 + rc;
+                                if (ci < p.ncx) base[(int64_t)cj * row_ld + ci] = g[rc];
+                                g[rc] = 0.0;
+                            }
+                        }
+                    }
+                    belowQ_prev = belowQ;
+                }
             }
-            cp_async_wait<0>();
             __syncwarp();
             if (lane == 0 && b > 0) {
                 bP[m + 1] = 0.0;

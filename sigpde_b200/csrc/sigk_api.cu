@@ -836,7 +836,7 @@ GradPlan make_grad_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy
     g.O = order;
     g.nb = (int)((n + 32 * R - 1) / (32 * R));
     g.rows_x = (ncx + 3) / 4 * 4;
-    const size_t dbytes = (size_t)g.nb * (m + 31) * R * 32 * sizeof(double);
+    const size_t dbytes = (size_t)g.nb * grad_band_doubles((int)m, R) * sizeof(double);
     const size_t bbytes = 2 * (size_t)(m + 2) * sizeof(double);
     const size_t mbytes = (size_t)ncy * g.rows_x * sizeof(double);
     const int64_t items_per_x = op == kOpPairwise ? 1 : ny;
