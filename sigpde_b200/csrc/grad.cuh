@@ -336,25 +336,39 @@ __global__ void grad_pair_inc_kernel(const double *dx, const double *dy, int64_t
 }
 
 // Gradients with respect to the x side's scaled-difference rows: for each
-// matrix row m (x path il, cell ci), gdx[m][k] += fx * sum_n G[n][m] dy[n][k]
-// over the y cells n paired with it (Gram: all of them; pairwise: its own
-// pair's), where dy are the y side's scaled differences (dimension-major).
-// Each CTA-y slice sums a range of n into its own partial row; grad_reduce
-// adds the slices in order.
+// matrix row m (x path il, cell ci), part[slice][m][k] = sum over the slice's
+// y cells n paired with it (Gram: all of them; pairwise: its own pair's) of
+// G[n][m] * dyt[n][k].  grad_reduce_kernel adds the slices in order.
+// dxt / dyt are the scaled differences in row layout (one row of d values per
+// cell; x rows padded to rows_x per path with zeros), so that the inner loops
+// index them directly.
 struct GradContractParams {
     int op;
     const double *mat;     // dk/dc
     int64_t ld, rows_x, ncx, ncy;
     int64_t nrows_m;       // Gram: ld; pairwise: nitems * rows_x
     int64_t ncols_n;       // Gram: ny * ncy; pairwise: ncy (per pair)
-    const double *dx;      // x differences (npaths, d, ncx), chunk-relative, scaled
-    const double *dy;      // y differences (npaths, d, ncy), scaled
+    const double *dxt;     // x differences, rows m of the chunk: [m][k]
+    const double *dyt;     // y differences, all y cells: [y path * ncy + cj][k]
     int64_t d;
     double *part;          // gx: [slice][nrows_m][d] partial sums
     int64_t slice;         // columns per slice
     double *gdy;           // gy: (ny, ncy, d) accumulated (+=) over chunks
     int64_t x0;
 };
+
+// Row layout of scaled differences: dst[(path * rows + r) * d + k] =
+// src[(path * d + k) * nc + r] for r < nc, 0 for nc <= r < rows.
+template <int V = 0> // instantiated once, in kernels_grad.cu
+__global__ void grad_rows_kernel(const double *src, int64_t npaths, int64_t nc, int64_t rows, int64_t d, double *dst)
+{
+    const int64_t total = npaths * rows * d;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t path = e / (rows * d), rem = e - path * rows * d, r = rem / d, k = rem - r * d;
+        dst[e] = r < nc ? src[(path * d + k) * nc + r] : 0.0;
+    }
+}
 
 template <int V = 0> // instantiated once, in kernels_grad.cu
 __global__ void grad_gx_kernel(GradContractParams p)
@@ -363,39 +377,31 @@ __global__ void grad_gx_kernel(GradContractParams p)
     if (mm >= p.nrows_m) return;
     const int64_t n0 = (int64_t)blockIdx.y * p.slice;
     const int64_t n1 = n0 + p.slice < p.ncols_n ? n0 + p.slice : p.ncols_n;
-    int64_t ci, item = 0;
     const double *col;     // G[n][mm] = col[n * stride]
     int64_t stride;
-    const double *dy;      // dy of column n: dy[(n / ncy) * d * ncy + k * ncy + n % ncy] (Gram)
+    const double *dyt;     // dyt[n * d + k] for the n of this row
     if (p.op == kOpPairwise) {
-        item = mm / p.rows_x;
-        ci = mm - item * p.rows_x;
+        const int64_t item = mm / p.rows_x, ci = mm - item * p.rows_x;
         col = p.mat + item * p.ncy * p.rows_x + ci;
         stride = p.rows_x;
-        dy = p.dy + item * p.d * p.ncy; // the pair's own y path (chunk-relative pairs start at x0)
-        dy += p.x0 * p.d * p.ncy;
+        dyt = p.dyt + (p.x0 + item) * p.ncy * p.d; // the pair's own y path
     } else {
-        ci = mm % p.rows_x;
         col = p.mat + mm;
         stride = p.ld;
-        dy = p.dy;
+        dyt = p.dyt;
     }
     double *out = p.part + ((int64_t)blockIdx.y * p.nrows_m + mm) * p.d;
-    if (ci >= p.ncx) {
-        for (int64_t k = 0; k < p.d; ++k) out[k] = 0.0;
-        return;
-    }
     for (int64_t k0 = 0; k0 < p.d; k0 += 8) {
         double acc[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) acc[k] = 0.0;
+        const double *yk = dyt + k0;
         for (int64_t n = n0; n < n1; ++n) {
             const double gv = col[n * stride];
-            const int64_t yp = n / p.ncy, cj = n - yp * p.ncy;
-            const double *dyn = dy + yp * p.d * p.ncy + cj;
+            const double *yn = yk + n * p.d;
 #pragma unroll
             for (int k = 0; k < 8; ++k)
-                if (k0 + k < p.d) acc[k] = fma(gv, dyn[(k0 + k) * p.ncy], acc[k]);
+                if (k0 + k < p.d) acc[k] = fma(gv, yn[k], acc[k]);
         }
 #pragma unroll
         for (int k = 0; k < 8; ++k)
@@ -413,18 +419,18 @@ __global__ void grad_gy_kernel(GradContractParams p)
     const int64_t nrows = p.op == kOpPairwise ? (p.nrows_m / p.rows_x) * p.ncy : p.ncols_n;
     if (n >= nrows) return;
     const double *row;
+    const double *xt;
     int64_t mlen, yrow;
-    const double *dx;
     if (p.op == kOpPairwise) {
         const int64_t item = n / p.ncy, cj = n - item * p.ncy;
         row = p.mat + item * p.ncy * p.rows_x + cj * p.rows_x;
         mlen = p.rows_x;
-        dx = p.dx + item * p.d * p.ncx;
+        xt = p.dxt + item * p.rows_x * p.d;
         yrow = (p.x0 + item) * p.ncy + cj;
     } else {
         row = p.mat + n * p.ld;
         mlen = p.ld;
-        dx = p.dx;
+        xt = p.dxt;
         yrow = n;
     }
     for (int64_t k0 = 0; k0 < p.d; k0 += 8) {
@@ -432,13 +438,11 @@ __global__ void grad_gy_kernel(GradContractParams p)
 #pragma unroll
         for (int k = 0; k < 8; ++k) acc[k] = 0.0;
         for (int64_t mm = lane; mm < mlen; mm += 32) {
-            const int64_t il = mm / p.rows_x, ci = mm - il * p.rows_x;
-            if (ci >= p.ncx) continue;
-            const double gv = row[mm];
-            const double *dxm = dx + il * p.d * p.ncx + ci;
+            const double gv = row[mm]; // padding rows hold 0, as do their differences
+            const double *xm = xt + mm * p.d + k0;
 #pragma unroll
             for (int k = 0; k < 8; ++k)
-                if (k0 + k < p.d) acc[k] = fma(gv, dxm[(k0 + k) * p.ncx], acc[k]);
+                if (k0 + k < p.d) acc[k] = fma(gv, xm[k], acc[k]);
         }
 #pragma unroll
         for (int k = 0; k < 8; ++k) {

@@ -819,7 +819,7 @@ struct GradPlan {
     int R = 0, O = 0, nb = 0;
     int64_t rows_x = 0, chunk = 0, nchunks = 0, slice = 0, nslices = 0;
     size_t dx_off = 0, dy_off = 0, gdx_off = 0, gdy_off = 0, part_off = 0, mat_off = 0, d_off = 0, bnd_off = 0,
-           ws_bytes = 0;
+           xt_off = 0, yt_off = 0, ws_bytes = 0;
 };
 
 GradPlan make_grad_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, int64_t d, int order)
@@ -867,6 +867,10 @@ GradPlan make_grad_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy
     off += align256((size_t)ny_paths * ncy * d * sizeof(double));
     g.part_off = off;
     off += align256((size_t)g.nslices * chunk * g.rows_x * d * sizeof(double));
+    g.xt_off = off; // the chunk's x differences in row layout
+    off += align256((size_t)chunk * g.rows_x * d * sizeof(double));
+    g.yt_off = off; // all y differences in row layout
+    off += align256((size_t)ny_paths * ncy * d * sizeof(double));
     g.mat_off = off;
     off += align256((size_t)chunk * items_per_x * mbytes);
     g.d_off = off;
@@ -907,7 +911,19 @@ int run_backward(const GradPlan &g, int op, const void *x, const void *y, int64_
     const double fs = static_scale * std::ldexp(1.0, -2 * order);
     int st;
     if ((st = run_delta(x, nx, lx, fs, sx, dx))) return st;
-    if ((st = run_delta(op == kOpPairwise ? y : y, ny_paths, ly, 1.0, sy, dy))) return st;
+    if ((st = run_delta(y, ny_paths, ly, 1.0, sy, dy))) return st;
+    double *dxt = reinterpret_cast<double *>(wsb + g.xt_off);
+    double *dyt = reinterpret_cast<double *>(wsb + g.yt_off);
+    auto run_rows = [&](const double *src, int64_t npaths, int64_t nc, int64_t rows, double *dst) -> int {
+        const int64_t total = npaths * rows * d;
+        int64_t blocks = (total + 255) / 256;
+        if (blocks > (int64_t)sm_count() * 8) blocks = (int64_t)sm_count() * 8;
+        get_grad_aux_kernels().rows<<<(unsigned)blocks, 256, 0, stream>>>(src, npaths, nc, rows, d, dst);
+        count_launch();
+        cudaError_t e2 = cudaGetLastError();
+        return e2 == cudaSuccess ? SIGK_OK : cuda_fail(e2, "row-layout launch");
+    };
+    if ((st = run_rows(dy, ny_paths, ncy, ncy, dyt))) return st;
     GradFns kf = get_grad_kernels(g.R, g.O);
     GradAuxFns aux = get_grad_aux_kernels();
     if (!kf.fwd || !kf.bwd) return fail(SIGK_EUNSUPPORTED, "no backward kernels for R=%d order=%d", g.R, g.O);
@@ -950,6 +966,7 @@ int run_backward(const GradPlan &g, int op, const void *x, const void *y, int64_
             get_dgemm_inc_kernel()<<<dim3((unsigned)mt, (unsigned)nt), 256, 0, stream>>>(gp);
             if ((st = launched("increment GEMM launch"))) return st;
         }
+        if ((st = run_rows(dx + i0 * d * ncx, nxc, ncx, g.rows_x, dxt))) return st;
         GradParams gp{};
         gp.op = op;
         gp.mat = mat;
@@ -984,8 +1001,8 @@ int run_backward(const GradPlan &g, int op, const void *x, const void *y, int64_
         cp.ncy = ncy;
         cp.nrows_m = op == kOpPairwise ? items * g.rows_x : ld;
         cp.ncols_n = op == kOpPairwise ? ncy : ny * ncy;
-        cp.dx = dx + i0 * d * ncx;
-        cp.dy = dy;
+        cp.dxt = dxt;
+        cp.dyt = dyt;
         cp.d = d;
         cp.part = part;
         cp.slice = g.slice;
