@@ -52,6 +52,9 @@ WORKLOADS = {
     # the device from the points
     "rbf256": dict(kind="static", nx=256, ny=256, L=128, d=8, order=2, seed_x=2001, seed_y=2002, static="rbf",
                    sigma=1.0),
+    # forward + backward of sum(SigPDE.gram(x, y)) with LinearKernel: X, Y 128 Brownian paths, L=128, d=8,
+    # dyadic order 2 (gradients with respect to both sides' points)
+    "grad128": dict(kind="grad", nx=128, ny=128, L=128, d=8, order=2, seed_x=2001, seed_y=2002),
     "uneven4096": dict(kind="ragged", npairs=4096, lmin=16, lmax=512, d=32, orders=(0, 1, 2, 3), seed=4096),
 }
 
@@ -538,6 +541,93 @@ def run_ours_static(args, w):
         "e2e": {"value": entries / (statistics.mean(e2e_times) * 1e-3), "unit": "entries/s",
                 "h2d_bytes_per_step": 2 * Xh.numel() * Xh.element_size(),
                 "d2h_bytes_per_step": Rh.numel() * Rh.element_size(), "ms_per_step": statistics.mean(e2e_times)},
+        "gpu_launches": launches, "clocks": clk, "lib": _lib.version(),
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+
+
+def run_ours_grad(args, w):
+    """Forward + backward of sum(k.gram(X, Y)) (LinearKernel, float64 paths): the
+    gradients with respect to every point of X and Y through sigk_backward."""
+    import numpy as np
+    import torch
+    import sigpde_b200.torch as sig
+    from sigpde_b200 import _lib
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    entries, cells, _ = workload_units(w)
+    X0, Y0 = make_inputs(w, device=dev, dtype=torch.float64)
+    X = X0.clone().requires_grad_()
+    Y = Y0.clone().requires_grad_()
+    k = sig.SigPDE(sig.kernels.LinearKernel(), w["order"])
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+
+    def step():
+        X.grad = None
+        Y.grad = None
+        k.gram(X, Y).sum().backward()
+
+    step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    times = timed_steps(torch, step, args.steps, args.warmup, flush, lambda: None)
+    launches = LAUNCHES["last"]
+    clk = clocks.stop()
+    t_fwd = timed_steps(torch, lambda: k.gram(X0, Y0), args.steps, args.warmup, flush, lambda: None)
+    Xh, Yh = X0.cpu().pin_memory(), Y0.cpu().pin_memory()
+    GXh, GYh = torch.empty_like(Xh).pin_memory(), torch.empty_like(Yh).pin_memory()
+
+    def e2e_step():
+        Xd = Xh.to(dev, non_blocking=True).requires_grad_()
+        Yd = Yh.to(dev, non_blocking=True).requires_grad_()
+        k.gram(Xd, Yd).sum().backward()
+        GXh.copy_(Xd.grad, non_blocking=True)
+        GYh.copy_(Yd.grad, non_blocking=True)
+
+    e2e_times = timed_steps(torch, e2e_step, args.steps, args.warmup, flush, lambda: None)
+    ms = statistics.mean(times)
+    acc = cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle
+        # the gradient of the sum over an 8 x 8 corner of the Gram, ours against the oracle's adjoint
+        Xs = X0[:8].clone().requires_grad_()
+        Ys = Y0[:8].clone().requires_grad_()
+        k.gram(Xs, Ys).sum().backward()
+        xs, ys = X0[:8].cpu().numpy(), Y0[:8].cpu().numpy()
+        t0 = time.perf_counter()
+        gx, gy = oracle.grad_gram(xs, ys, w["order"], np.ones((8, 8)))
+        t_cpu = time.perf_counter() - t0
+        scale = max(np.abs(gx).max(), np.abs(gy).max())
+        acc = {"max_abs_err_rel_to_max_grad": float(max(np.abs(Xs.grad.cpu().numpy() - gx).max(),
+                                                        np.abs(Ys.grad.cpu().numpy() - gy).max()) / scale),
+               "sample": "gradients of the sum over the 8 x 8 corner of the Gram vs the float64 oracle's adjoint"}
+        cpu = {"value": 64 / t_cpu, "unit": "entries/s", "cores": oracle.num_threads(), "kind": "port",
+               "sample": f"forward + adjoint of the 64 pairs of the 8 x 8 corner in {t_cpu:.1f} s "
+                         "(float64 C restatement, OpenMP over pairs)"}
+    # algorithmic FLOPs: the forward stencil (4 per cell) three times (forward, recompute, adjoint)
+    flops = 3 * 4 * cells
+    peak = device_peak_tflops(torch, torch.float64)
+    achieved = flops / (ms * 1e-3) / 1e12
+    line = {
+        "metric": "gram_gradient_entries_per_s", "value": entries / (ms * 1e-3), "unit": "entries/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "p50_ms": percentile(times, 0.5),
+        "p99_ms": percentile(times, 0.99), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic Brownian paths (seeded PCG64), float64",
+        "config": {"workload": "forward + backward of sum(SigPDE.gram(x, y)) 128x128, L=128, d=8, dyadic_order=2, "
+                               "LinearKernel", "global_batch": entries, "seq_len": w["L"],
+                   "parallelism": "single GPU", "l2": "flushed between timed steps (256 MB write)"},
+        "forward_ms_per_step": statistics.mean(t_fwd),
+        "accuracy": acc,
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "traffic": None, "scope": "whole step: 4 FLOPs per refined cell for each of the forward, "
+                     "the recompute and the adjoint, over the step time",
+                     "peak_source": "measured cuBLAS DGEMM 4096^3 on this device"},
+        "e2e": {"value": entries / (statistics.mean(e2e_times) * 1e-3), "unit": "entries/s",
+                "h2d_bytes_per_step": 2 * Xh.numel() * Xh.element_size(),
+                "d2h_bytes_per_step": 2 * GXh.numel() * GXh.element_size(), "ms_per_step": statistics.mean(e2e_times)},
         "gpu_launches": launches, "clocks": clk, "lib": _lib.version(),
     }
     if cpu is not None:
@@ -1063,6 +1153,12 @@ def main():
             print(json.dumps({"impl": "reference", "unavailable": "robust512 CPU arm: use the cpu_baseline of the "
                               "default run"}), flush=True)
         return
+    if w.get("kind") == "grad" and args.impl != "ours":
+        if int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps({"impl": args.impl, "unavailable": "the reference has no backward pass (its Numba "
+                              "kernels end autograd); the oracle's adjoint is the cpu_baseline of the default run"}),
+                  flush=True)
+        return
     if args.impl == "reference":
         if ragged:
             if int(os.environ.get("RANK", "0")) == 0:
@@ -1088,6 +1184,10 @@ def main():
     if w.get("kind") == "static":
         if int(os.environ.get("RANK", "0")) == 0:
             run_ours_static(args, w)
+        return
+    if w.get("kind") == "grad":
+        if int(os.environ.get("RANK", "0")) == 0:
+            run_ours_grad(args, w)
         return
     run_ours(args, w)
 
