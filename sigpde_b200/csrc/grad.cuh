@@ -101,22 +101,22 @@ __device__ __forceinline__ void grad_coefs(const double *base, int64_t row_ld, i
 }
 
 // One forward step of the lane's R rows at a column: left holds K(rows, q-1)
-// and becomes K(rows, q); rows beyond n hold 0.  D of each row goes to d[r * 32].
+// and becomes K(rows, q); D of each row goes to d[r * 32].  Rows beyond n
+// (coarse rows >= ncx, c = 0) copy row n and carry Lambda = 0 in the adjoint:
+// they need no masking.
 template <int R, int O, bool WANT_D>
 __device__ __forceinline__ void grad_lane_step(double (&left)[R], double top, double diag, const double *A,
-                                               const double *B, const double *Ad, const double *Bd, int p0, int n,
-                                               double *d)
+                                               const double *B, const double *Ad, const double *Bd, double *d)
 {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int rc = r >> O;
         const double sum = left[r] + top;
         const double k = sum * A[rc] - diag * B[rc];
-        const bool valid = p0 + r <= n;
-        if constexpr (WANT_D) d[r * 32] = valid ? sum * Ad[rc] - diag * Bd[rc] : 0.0;
+        if constexpr (WANT_D) d[r * 32] = sum * Ad[rc] - diag * Bd[rc];
         diag = left[r];
-        left[r] = valid ? k : 0.0;
-        top = left[r];
+        left[r] = k;
+        top = k;
     }
 }
 
@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) grad_fwd_kernel(GradParam
                     }
                     if (((q - 1) & ((1 << O) - 1)) == 0) // a new coarse column
                         grad_coefs<RC>(base, row_ld, ci0, p.ncx, (q - 1) >> O, A, B, Ad, Bd);
-                    grad_lane_step<R, O, false>(left, top, diag, A, B, Ad, Bd, p0, n, nullptr);
+                    grad_lane_step<R, O, false>(left, top, diag, A, B, Ad, Bd, nullptr);
                     if (lane == 31 && b + 1 < nb) bnd[q] = left[R - 1];
                     corner = from_above;
                     bot = left[R - 1];
@@ -212,8 +212,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) grad_bwd_kernel(GradParam
             const int p0 = b * 32 * R + lane * R + 1;
             const int ci0 = (p0 - 1) >> O;
             double Pr[R], Qr[R]; // P, Q of the lane's rows at column q + 1
+            // the seed Lambda(n, m) = w enters as the right neighbour of row n at column m
+            const int rseed = n - p0;
 #pragma unroll
-            for (int r = 0; r < R; ++r) Pr[r] = Qr[r] = 0.0;
+            for (int r = 0; r < R; ++r) {
+                Pr[r] = r == rseed ? w : 0.0;
+                Qr[r] = 0.0;
+            }
             double g[RC];
 #pragma unroll
             for (int rc = 0; rc < RC; ++rc) g[rc] = 0.0;
@@ -242,7 +247,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) grad_bwd_kernel(GradParam
                             if (!have || ((q - 1) & ((1 << O) - 1)) == 0)
                                 grad_coefs<RC>(base, row_ld, ci0, p.ncx, (q - 1) >> O, A, B, Ad, Bd);
                             have = true;
-                            grad_lane_step<R, O, true>(left, tp[t + 1], q == 1 ? 1.0 : tp[t], A, B, Ad, Bd, p0, n,
+                            grad_lane_step<R, O, true>(left, tp[t + 1], q == 1 ? 1.0 : tp[t], A, B, Ad, Bd,
                                                        dl + t * R * 32);
                         }
                     }
@@ -274,10 +279,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) grad_bwd_kernel(GradParam
 #pragma unroll
                         for (int r = R - 1; r >= 0; --r) {
                             const int rc = r >> O;
-                            const int pr = p0 + r;
-                            double lam = Pr[r] + dP - dQ;
-                            if (pr == n && q == m) lam += w;
-                            if (pr > n) lam = 0.0;
+                            const double lam = Pr[r] + dP - dQ;
                             g[rc] = fma(lam, dq[r * 32], g[rc]);
                             const double P = A[rc] * lam, Q = B[rc] * lam;
                             dQ = Qr[r]; // Q(p, q+1) is the diagonal of the row above
