@@ -81,6 +81,7 @@ struct GradAuxFns {
     void (*reduce)(const double *, int64_t, int64_t, int64_t, int64_t, int64_t, int64_t, double *);
     void (*points)(const double *, int64_t, int64_t, int64_t, double, const void *, int, void *);
     void (*rows)(const double *, int64_t, int64_t, int64_t, int64_t, double *);
+    void (*gy_gram)(GradContractParams);
 };
 GradAuxFns get_grad_aux_kernels();
 // mat64: the increment matrix holds float64 (dgemm_inc_kernel) instead of float32 (tensor cores)

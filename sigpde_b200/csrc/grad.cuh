@@ -456,6 +456,58 @@ __global__ void grad_gy_kernel(GradContractParams p)
     }
 }
 
+// gy for the Gram: gdy[n][k] += sum_m G[n][m] dxt[m][k], a tall-skinny GEMM
+// (rows n: all y cells, m: the chunk's x cells, k < d).  A CTA owns 32 rows
+// and k-chunks of up to 32; m goes in tiles of 64 staged in shared memory
+// (G rows coalesced along m; dxt transposed to [k][m] with a padded stride so
+// that the 8 k-groups of a warp hit different banks).  Each (n, k) has one
+// owner thread, so the sum over chunks stays in order.
+constexpr int kGyRows = 32, kGyTile = 64, kGyK = 32;
+
+template <int V = 0> // instantiated once, in kernels_grad.cu
+__global__ void __launch_bounds__(256) grad_gy_gram_kernel(GradContractParams p)
+{
+    __shared__ double gs[kGyRows][kGyTile + 1];
+    __shared__ double xs[kGyK][kGyTile + 1];
+    const int tid = threadIdx.x;
+    const int row = tid >> 3, kg = tid & 7; // 32 rows x 8 k-groups; k = kg + 8 j
+    const int64_t n0 = (int64_t)blockIdx.x * kGyRows;
+    const int64_t nrows = p.ncols_n;
+    for (int64_t k0 = 0; k0 < p.d; k0 += kGyK) {
+        const int kn = (int)((p.d - k0) < kGyK ? (p.d - k0) : kGyK);
+        double acc[kGyK / 8];
+#pragma unroll
+        for (int j = 0; j < kGyK / 8; ++j) acc[j] = 0.0;
+        for (int64_t m0 = 0; m0 < p.ld; m0 += kGyTile) {
+            __syncthreads();
+            for (int e = tid; e < kGyRows * kGyTile; e += 256) {
+                const int r = e / kGyTile, mm = e - r * kGyTile;
+                const int64_t n = n0 + r, m = m0 + mm;
+                gs[r][mm] = (n < nrows && m < p.ld) ? p.mat[n * p.ld + m] : 0.0;
+            }
+            for (int e = tid; e < kGyTile * kn; e += 256) {
+                const int mm = e / kn, k = e - mm * kn;
+                const int64_t m = m0 + mm;
+                xs[k][mm] = m < p.ld ? p.dxt[m * p.d + k0 + k] : 0.0;
+            }
+            __syncthreads();
+#pragma unroll 4
+            for (int mm = 0; mm < kGyTile; ++mm) {
+                const double gv = gs[row][mm];
+#pragma unroll
+                for (int j = 0; j < kGyK / 8; ++j)
+                    if (kg + 8 * j < kn) acc[j] = fma(gv, xs[kg + 8 * j][mm], acc[j]);
+            }
+        }
+        const int64_t n = n0 + row;
+        if (n < nrows) {
+#pragma unroll
+            for (int j = 0; j < kGyK / 8; ++j)
+                if (kg + 8 * j < kn) p.gdy[n * p.d + k0 + kg + 8 * j] += acc[j];
+        }
+    }
+}
+
 // gdx[(x0 + il) * ncx + ci][k] = sum over slices of part (rows ci < ncx).
 template <int V = 0> // instantiated once, in kernels_grad.cu
 __global__ void grad_reduce_kernel(const double *part, int64_t nslices, int64_t nrows_m, int64_t rows_x, int64_t ncx,

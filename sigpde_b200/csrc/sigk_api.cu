@@ -1018,8 +1018,12 @@ int run_backward(const GradPlan &g, int op, const void *x, const void *y, int64_
             if ((st = launched("x reduction launch"))) return st;
         }
         if (gy) {
-            const int64_t rows = op == kOpPairwise ? items * ncy : ny * ncy;
-            aux.gy<<<(unsigned)((rows * 32 + 255) / 256), 256, 0, stream>>>(cp);
+            if (op == kOpPairwise) {
+                const int64_t rows = items * ncy;
+                aux.gy<<<(unsigned)((rows * 32 + 255) / 256), 256, 0, stream>>>(cp);
+            } else {
+                aux.gy_gram<<<(unsigned)((ny * ncy + kGyRows - 1) / kGyRows), 256, 0, stream>>>(cp);
+            }
             if ((st = launched("y contraction launch"))) return st;
         }
     }
