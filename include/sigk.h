@@ -191,6 +191,23 @@ SIGK_API int sigk_backward(int op, const void *x, const void *y, int64_t n_x, in
                            void *grad_y, void *workspace, size_t workspace_bytes, sigk_stream_t stream);
 
 /*
+ * Backward pass over caller's increments (any static kernel): for
+ * L = sum_b grad_out[b] k_b, where k_b solves the PDE on increments
+ * inc[b] * scale_x[b] * scale_y[b] as sigk_pairwise_inc does, writes
+ * grad_inc = dL/dinc (npairs, nc_x, nc_y) with element strides (g0, g1, g2)
+ * in dtype.  A Gram tile passes its pairs flattened (strides of the 4-D
+ * tensor's last two axes, s0 = the stride between consecutive pairs when they
+ * are evenly spaced, else one call per row).  Float64 adjoint; dyadic order
+ * <= 4.  Workspace: sigk_backward_inc_workspace_size(...) bytes, 256-byte
+ * aligned.  No counterpart in the reference.
+ */
+SIGK_API size_t sigk_backward_inc_workspace_size(int64_t npairs, int64_t nc_x, int64_t nc_y, int order);
+SIGK_API int sigk_backward_inc(const void *inc, int64_t npairs, int64_t nc_x, int64_t nc_y, int64_t s0, int64_t s1,
+                               int64_t s2, int dtype, int order, const void *scale_x, const void *scale_y,
+                               const void *grad_out, void *grad_inc, int64_t g0, int64_t g1, int64_t g2,
+                               void *workspace, size_t workspace_bytes, sigk_stream_t stream);
+
+/*
  * Self norms k(x_b, x_b) in float64, NaN mapped to +inf.
  * First half of RobustSigPDE._norm_factors (sigpde/torch/kernel.py:181-183);
  * used when the normaliser is a user callable that the host applies.

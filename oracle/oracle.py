@@ -344,6 +344,77 @@ def grad_gram(x, y, order: int, grad_out, x_scale=None, y_scale=None, static_sca
     return gx, gy
 
 
+def _chain_static(kind, H, x, y, param):
+    """Gradients of sum_pq H[p, q] k(x_p, y_q) for the RBF / L1-RBF static kernels
+    (sigpde/torch/static_kernels.py:13-53) with respect to the points."""
+    S = static_gram(kind, x[None], y[None], param)[0, 0]
+    diff = x[:, None, :] - y[None, :, :]                 # (Lx, Ly, d)
+    if kind == "rbf":
+        W = H * S * (-2.0 / param)
+        gx = np.einsum("pq,pqk->pk", W, diff)
+        gy = -np.einsum("pq,pqk->qk", W, diff)
+    elif kind == "l1rbf":
+        W = H * S * (-1.0 / param)
+        sg = np.sign(diff)
+        gx = np.einsum("pq,pqk->pk", W, sg)
+        gy = -np.einsum("pq,pqk->qk", W, sg)
+    else:
+        raise ValueError(kind)
+    return gx, gy
+
+
+def _second_difference_adjoint(Ginc, f):
+    """dL/dS for inc = f * (S[1:,1:] + S[:-1,:-1] - S[1:,:-1] - S[:-1,1:])."""
+    ncx, ncy = Ginc.shape
+    H = np.zeros((ncx + 1, ncy + 1))
+    H[1:, 1:] += Ginc
+    H[:-1, :-1] += Ginc
+    H[1:, :-1] -= Ginc
+    H[:-1, 1:] -= Ginc
+    return H * f
+
+
+def grad_static_pairs(kind, x, y, order, w, param, sx=None, sy=None):
+    """Per-pair gradients of sum_b w[b] k(x_b, y_b) for a static kernel of the
+    generic route (increments from the static Gram), float64.  Returns (gx, gy)."""
+    x = _f64(x)
+    y = _f64(y)
+    B = x.shape[0]
+    s = np.ones(B) * (1.0 if sx is None else _f64(sx).reshape(B)) * (1.0 if sy is None else _f64(sy).reshape(B))
+    incs = np.stack([second_difference(static_gram(kind, x[b:b + 1], y[b:b + 1], param)[0, 0], order)
+                     for b in range(B)])
+    G, _ = grad_increments(incs, order, s, _f64(w).reshape(B))
+    f = 1.0 / float(4 ** order)
+    gx = np.zeros_like(x)
+    gy = np.zeros_like(y)
+    for b in range(B):
+        H = _second_difference_adjoint(G[b] * s[b], f)
+        gx[b], gy[b] = _chain_static(kind, H, x[b], y[b], param)
+    return gx, gy
+
+
+def grad_static_gram(kind, x, y, order, w, param, sx=None, sy=None):
+    """Gradients of sum_ij w[i, j] k(x_i, y_j) for RBF / L1-RBF (y=None: the
+    symmetric Gram, both sides' contributions to x)."""
+    sym = y is None
+    x = _f64(x)
+    y = x if sym else _f64(y)
+    Nx, Ny = x.shape[0], y.shape[0]
+    w = _f64(w).reshape(Nx, Ny)
+    sxv = np.ones(Nx) if sx is None else _scale_vec(sx, Nx)
+    syv = sxv if sym else (np.ones(Ny) if sy is None else _scale_vec(sy, Ny))
+    ii, jj = np.meshgrid(np.arange(Nx), np.arange(Ny), indexing="ij")
+    ii, jj = ii.reshape(-1), jj.reshape(-1)
+    gxp, gyp = grad_static_pairs(kind, x[ii], y[jj], order, w.reshape(-1), param, sxv[ii], syv[jj])
+    gx = np.zeros_like(x)
+    gy = np.zeros_like(y)
+    np.add.at(gx, ii, gxp)
+    np.add.at(gy, jj, gyp)
+    if sym:
+        return gx + gy
+    return gx, gy
+
+
 # --------------------------------------------------------------------------- robust
 def log_normalizer(k):
     """Default normalizer f(s) = 2 - 1/(1 + log s) (sigpde/torch/kernel.py:23-24)."""

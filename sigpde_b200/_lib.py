@@ -68,6 +68,9 @@ SIGNATURES = {
     "sigk_backward_workspace_size": (_sz, [_int, _i64, _i64, _i64, _i64, _i64, _int, _int]),
     "sigk_backward": (_int, [_int, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _int, _int, _dbl, _vp, _vp, _vp, _vp, _vp,
                              _vp, _sz, _vp]),
+    "sigk_backward_inc_workspace_size": (_sz, [_i64, _i64, _i64, _int]),
+    "sigk_backward_inc": (_int, [_vp, _i64, _i64, _i64, _i64, _i64, _i64, _int, _int, _vp, _vp, _vp, _vp, _i64, _i64,
+                                 _i64, _vp, _sz, _vp]),
     "sigk_self_norms": (_int, [_vp, _i64, _i64, _i64, _int, _int, _dbl, _vp, _vp, _sz, _vp]),
     "sigk_normalize": (_int, [_vp, _i64, _i64, _i64, _int, _int, _dbl, _vp, _vp, _dbl, _int, _vp, _vp, _vp, _sz,
                               _vp]),

@@ -82,6 +82,8 @@ struct GradAuxFns {
     void (*points)(const double *, int64_t, int64_t, int64_t, double, const void *, int, void *);
     void (*rows)(const double *, int64_t, int64_t, int64_t, int64_t, double *);
     void (*gy_gram)(GradContractParams);
+    void (*inc_blocks)(const void *, int, int64_t, int64_t, int64_t, int64_t, int64_t, int64_t, int64_t, int64_t,
+                       const void *, const void *, double *, void *, int);
 };
 GradAuxFns get_grad_aux_kernels();
 // mat64: the increment matrix holds float64 (dgemm_inc_kernel) instead of float32 (tensor cores)

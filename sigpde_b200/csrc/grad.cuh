@@ -337,6 +337,39 @@ __global__ void grad_pair_inc_kernel(const double *dx, const double *dy, int64_t
     }
 }
 
+// Caller's increments (npairs, ncx, ncy) with element strides, times the
+// pair's scales, into per-pair blocks [item][cj][ci] (rows ci >= ncx are 0);
+// with `back`, the reverse: out = block * scales written with the strides.
+template <int V = 0> // instantiated once, in kernels_grad.cu
+__global__ void grad_inc_blocks_kernel(const void *inc, int in64, int64_t s0, int64_t s1, int64_t s2, int64_t nitems,
+                                       int64_t b0, int64_t ncx, int64_t ncy, int64_t rows_x, const void *sx,
+                                       const void *sy, double *blocks, void *out, int back)
+{
+    const int64_t total = nitems * ncy * rows_x;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t item = e / (ncy * rows_x), r = e - item * ncy * rows_x;
+        const int64_t cj = r / rows_x, ci = r - cj * rows_x;
+        const int64_t b = b0 + item;
+        double sc = 1.0;
+        if (sx) sc *= in64 ? reinterpret_cast<const double *>(sx)[b] : (double)reinterpret_cast<const float *>(sx)[b];
+        if (sy) sc *= in64 ? reinterpret_cast<const double *>(sy)[b] : (double)reinterpret_cast<const float *>(sy)[b];
+        const int64_t off = b * s0 + ci * s1 + cj * s2;
+        if (!back) {
+            double v = 0.0;
+            if (ci < ncx)
+                v = in64 ? reinterpret_cast<const double *>(inc)[off] : (double)reinterpret_cast<const float *>(inc)[off];
+            blocks[e] = v * sc;
+        } else if (ci < ncx) {
+            const double v = blocks[e] * sc;
+            if (in64)
+                reinterpret_cast<double *>(out)[off] = v;
+            else
+                reinterpret_cast<float *>(out)[off] = (float)v;
+        }
+    }
+}
+
 // Gradients with respect to the x side's scaled-difference rows: for each
 // matrix row m (x path il, cell ci), part[slice][m][k] = sum over the slice's
 // y cells n paired with it (Gram: all of them; pairwise: its own pair's) of

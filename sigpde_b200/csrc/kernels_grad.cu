@@ -35,7 +35,7 @@ GradFns get_grad_kernels(int R, int O)
 GradAuxFns get_grad_aux_kernels()
 {
     return {grad_pair_inc_kernel<>, grad_gx_kernel<>, grad_gy_kernel<>, grad_reduce_kernel<>, grad_points_kernel<>,
-            grad_rows_kernel<>, grad_gy_gram_kernel<>};
+            grad_rows_kernel<>, grad_gy_gram_kernel<>, grad_inc_blocks_kernel<>};
 }
 
 } // namespace sigk

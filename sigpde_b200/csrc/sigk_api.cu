@@ -1040,6 +1040,86 @@ int run_backward(const GradPlan &g, int op, const void *x, const void *y, int64_
     return SIGK_OK;
 }
 
+// Backward over caller's increments: per chunk of pairs, the scaled increments
+// in per-pair blocks, then the same forward / adjoint kernels (pairwise
+// layout, weight of pair b = grad_out[b]), then dk/dc * scales back out.
+GradPlan make_grad_inc_plan(int64_t npairs, int64_t ncx, int64_t ncy, int order)
+{
+    GradPlan g = make_grad_plan(kOpPairwise, npairs, npairs, ncx, ncy, 1, order);
+    if (!g.ok) return g;
+    // only the matrix, the per-step records and the boundary rows are used
+    const int64_t m = ncy << order;
+    const size_t dbytes = (size_t)g.nb * grad_band_doubles((int)m, g.R) * sizeof(double);
+    const size_t bbytes = 2 * (size_t)(m + 2) * sizeof(double);
+    const size_t mbytes = (size_t)ncy * g.rows_x * sizeof(double);
+    size_t off = 256;
+    g.mat_off = off;
+    off += align256((size_t)g.chunk * mbytes);
+    g.d_off = off;
+    off += align256((size_t)g.chunk * dbytes);
+    g.bnd_off = off;
+    off += align256((size_t)g.chunk * bbytes);
+    g.ws_bytes = off;
+    return g;
+}
+
+int run_backward_inc(const GradPlan &g, const void *inc, int64_t npairs, int64_t ncx, int64_t ncy, int64_t s0,
+                     int64_t s1, int64_t s2, int dtype, int order, const void *sx, const void *sy, const void *w,
+                     void *ginc, int64_t g0, int64_t g1, int64_t g2, void *ws, cudaStream_t stream)
+{
+    const bool in64 = dtype == SIGK_F64;
+    unsigned char *wsb = reinterpret_cast<unsigned char *>(ws);
+    double *mat = reinterpret_cast<double *>(wsb + g.mat_off);
+    GradFns kf = get_grad_kernels(g.R, g.O);
+    GradAuxFns aux = get_grad_aux_kernels();
+    if (!kf.fwd || !kf.bwd) return fail(SIGK_EUNSUPPORTED, "no backward kernels for R=%d order=%d", g.R, g.O);
+    int st, nbf = 0, nbb = 0;
+    if ((st = blocks_per_sm((const void *)kf.fwd, 0, &nbf)) || (st = blocks_per_sm((const void *)kf.bwd, 0, &nbb)))
+        return st;
+    auto launched = [&](const char *what) -> int {
+        count_launch();
+        cudaError_t e2 = cudaGetLastError();
+        return e2 == cudaSuccess ? SIGK_OK : cuda_fail(e2, what);
+    };
+    for (int64_t c = 0; c < g.nchunks; ++c) {
+        const int64_t b0 = c * g.chunk, b1 = (b0 + g.chunk < npairs) ? b0 + g.chunk : npairs, items = b1 - b0;
+        const int64_t total = items * ncy * g.rows_x;
+        int64_t blocks = (total + 255) / 256;
+        if (blocks > (int64_t)sm_count() * 16) blocks = (int64_t)sm_count() * 16;
+        aux.inc_blocks<<<(unsigned)blocks, 256, 0, stream>>>(inc, in64, s0, s1, s2, items, b0, ncx, ncy, g.rows_x,
+                                                             sx, sy, mat, nullptr, 0);
+        if ((st = launched("increment blocks launch"))) return st;
+        GradParams gp{};
+        gp.op = kOpPairwise;
+        gp.mat = mat;
+        gp.ld = g.rows_x;
+        gp.rows_x = g.rows_x;
+        gp.ncx = ncx;
+        gp.ncy = ncy;
+        gp.order = order;
+        gp.nitems = items;
+        gp.ny = npairs;
+        gp.w = w;
+        gp.in64 = in64;
+        gp.x0 = b0;
+        gp.dbuf = reinterpret_cast<double *>(wsb + g.d_off);
+        gp.bnd = reinterpret_cast<double *>(wsb + g.bnd_off);
+        auto grid_for = [&](int nb) -> unsigned {
+            int64_t warps = (int64_t)sm_count() * nb * kWarpsPerBlock;
+            if (warps > items) warps = items;
+            return (unsigned)((warps + kWarpsPerBlock - 1) / kWarpsPerBlock);
+        };
+        kf.fwd<<<grid_for(nbf), kWarpsPerBlock * 32, 0, stream>>>(gp);
+        if ((st = launched("backward forward-pass launch"))) return st;
+        kf.bwd<<<grid_for(nbb), kWarpsPerBlock * 32, 0, stream>>>(gp);
+        if ((st = launched("adjoint launch"))) return st;
+        aux.inc_blocks<<<(unsigned)blocks, 256, 0, stream>>>(nullptr, in64, g0, g1, g2, items, b0, ncx, ncy, g.rows_x,
+                                                             sx, sy, mat, ginc, 1);
+        if ((st = launched("increment gradient launch"))) return st;
+    }
+    return SIGK_OK;
+}
+
 int run_pairs(int op, const void *x, const void *y, int64_t nx, int64_t ny, int64_t lx, int64_t ly, int64_t d,
               int dtype, int order, double static_scale, const void *sx, const void *sy, void *out, int64_t out_ld,
               int precision, void *ws, size_t ws_bytes, cudaStream_t stream)
@@ -1429,6 +1509,39 @@ int sigk_backward(int op, const void *x, const void *y, int64_t n_x, int64_t n_y
     if (((uintptr_t)workspace & 255) != 0) return fail(SIGK_EINVAL, "workspace must be 256-byte aligned");
     return run_backward(g, kop, x, y, n_x, n_y, len_x, len_y, dim, dtype, order, static_scale, scale_x, scale_y,
                         grad_out, grad_x, grad_y, workspace, (cudaStream_t)stream);
+}
+
+size_t sigk_backward_inc_workspace_size(int64_t npairs, int64_t nc_x, int64_t nc_y, int order)
+{
+    if (npairs < 1 || nc_x < 1 || nc_y < 1 || order < 0 || order > kGradMaxOrder) return 0;
+    GradPlan g = make_grad_inc_plan(npairs, nc_x, nc_y, order);
+    return g.ok ? g.ws_bytes : 0;
+}
+
+int sigk_backward_inc(const void *inc, int64_t npairs, int64_t nc_x, int64_t nc_y, int64_t s0, int64_t s1, int64_t s2,
+                      int dtype, int order, const void *scale_x, const void *scale_y, const void *grad_out,
+                      void *grad_inc, int64_t g0, int64_t g1, int64_t g2, void *workspace, size_t workspace_bytes,
+                      sigk_stream_t stream)
+{
+    int st = check_common(dtype, SIGK_PREC_FP64, order);
+    if (st) return st;
+    if (npairs < 1 || nc_x < 1 || nc_y < 1)
+        return fail(SIGK_EINVAL, "need npairs, nc_x, nc_y >= 1 (got %lld, %lld, %lld)", (long long)npairs,
+                    (long long)nc_x, (long long)nc_y);
+    if (order > kGradMaxOrder)
+        return fail(SIGK_EUNSUPPORTED, "the backward pass takes dyadic order <= %d (got %d)", kGradMaxOrder, order);
+    if ((st = check_dev(inc, "inc", false)) || (st = check_dev(grad_out, "grad_out", false)) ||
+        (st = check_dev(grad_inc, "grad_inc", false)) || (st = check_dev(scale_x, "scale_x", true)) ||
+        (st = check_dev(scale_y, "scale_y", true)))
+        return st;
+    GradPlan g = make_grad_inc_plan(npairs, nc_x, nc_y, order);
+    if (!g.ok) return fail(SIGK_EUNSUPPORTED, "no backward plan");
+    if (!workspace || workspace_bytes < g.ws_bytes)
+        return fail(SIGK_ENOMEM, "workspace of %zu bytes needed (got %zu)", g.ws_bytes,
+                    workspace ? workspace_bytes : 0);
+    if (((uintptr_t)workspace & 255) != 0) return fail(SIGK_EINVAL, "workspace must be 256-byte aligned");
+    return run_backward_inc(g, inc, npairs, nc_x, nc_y, s0, s1, s2, dtype, order, scale_x, scale_y, grad_out,
+                            grad_inc, g0, g1, g2, workspace, (cudaStream_t)stream);
 }
 
 // Shared body of sigk_normalize, sigk_normalize_inc and sigk_self_norms

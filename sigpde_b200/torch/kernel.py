@@ -181,12 +181,102 @@ class _LinearSigKernel(torch.autograd.Function):
         return gx, gy, None, None, None, None
 
 
-def _differentiable(solver, op, x, y, x_scale, y_scale, n_y):
-    """Route a call whose paths require grad through _LinearSigKernel."""
-    if not _is_fused_linear(solver.static_kernel):
-        raise NotImplementedError("gradients are implemented for LinearKernel")
+class _IncSolve(torch.autograd.Function):
+    """k of each pair from caller's increments (sigk_pairwise_inc), differentiable
+    with respect to the increments (sigk_backward_inc, the float64 adjoint), so
+    that autograd continues through whatever torch code built them: any static
+    kernel of the duck-typed protocol.  Scales are constants."""
+
+    @staticmethod
+    def forward(ctx, inc, sx, sy, solver):
+        B, ncx, ncy = inc.shape
+        out = torch.empty(B, device=inc.device, dtype=inc.dtype)
+        solver._solve_pairwise_inc(inc, sx, sy, out)
+        ctx.solver = solver
+        ctx.save_for_backward(inc, sx, sy)
+        return out
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        inc, sx, sy = ctx.saved_tensors
+        if not ctx.needs_input_grad[0]:
+            return None, None, None, None
+        B, ncx, ncy = inc.shape
+        g = grad_out.detach().to(dtype=inc.dtype).contiguous()
+        ginc = torch.empty(inc.shape, dtype=inc.dtype, device=inc.device)
+        dt = _dtype_code(inc)
+        order = ctx.solver.dyadic_order
+        with torch.cuda.device(inc.device):
+            n = _lib.lib().sigk_backward_inc_workspace_size(B, ncx, ncy, order)
+            ws = torch.empty(n, dtype=torch.uint8, device=inc.device)
+            _lib.call("sigk_backward_inc", _ptr(inc), B, ncx, ncy, inc.stride(0), inc.stride(1), inc.stride(2), dt,
+                      order, _ptr(sx), _ptr(sy), _ptr(g), _ptr(ginc), ginc.stride(0), ginc.stride(1),
+                      ginc.stride(2), _ptr(ws), n, _stream())
+        return ginc, None, None, None
+
+
+def _generic_differentiable(solver, op, x, y, x_scale, y_scale, max_batch):
+    """Differentiable values for a static kernel other than the linear one: the
+    reference's route (torch builds the increments of each tile, so autograd
+    sees the static kernel) with _IncSolve for the solves."""
+    _check_paths(x, "x")
+    if op == "pairwise":
+        yv = x if y is None else y
+        _check_paths(yv, "y")
+        B = x.shape[0]
+        ys = x_scale if y is None else y_scale
+        scaled = x_scale is not None or ys is not None
+        sx = _broadcast_scale(x_scale, B, x) if scaled else None
+        sy = _broadcast_scale(ys, B, yv) if scaled else None
+        parts = []
+        for s0, s1 in _batches(B, max_batch):
+            inc = pairwise_inner_product(x[s0:s1], yv[s0:s1], solver.static_kernel, solver.dyadic_order)
+            parts.append(_IncSolve.apply(inc.to(x.dtype), None if sx is None else sx[s0:s1],
+                                         None if sy is None else sy[s0:s1], solver))
+        return torch.cat(parts)
+    sym = y is None
+    yv = x if sym else y
+    _check_paths(yv, "y")
+    Nx, Ny = x.shape[0], yv.shape[0]
+    ys = x_scale if sym else y_scale
+    scaled = x_scale is not None or ys is not None
+    sx = _broadcast_scale(x_scale, Nx, x) if scaled else None
+    sy = _broadcast_scale(ys, Ny, yv) if scaled else None
+    tile = math.ceil(math.sqrt(max_batch))  # sigpde/torch/kernel.py:68
+    blocks = {}
+    rows = []
+    for x0, x1 in _batches(Nx, tile):
+        row = []
+        for y0, y1 in _batches(Ny, tile):
+            if sym and y0 > x0:  # upper tiles are the transposed lower ones
+                row.append(None)
+                continue
+            inc = gram_inner_product(x[x0:x1], yv[y0:y1], solver.static_kernel, solver.dyadic_order)
+            tx, ty, ncx, ncy = inc.shape
+            flat = inc.to(x.dtype).reshape(tx * ty, ncx, ncy)
+            vx = None if sx is None else sx[x0:x1].repeat_interleave(ty)
+            vy = None if sy is None else sy[y0:y1].repeat(tx)
+            blk = _IncSolve.apply(flat, vx, vy, solver).reshape(tx, ty)
+            blocks[(x0, y0)] = blk
+            row.append(blk)
+        rows.append(row)
+    xs = list(_batches(Nx, tile))
+    ysb = list(_batches(Ny, tile))
+    out_rows = []
+    for a, (x0, _) in enumerate(xs):
+        out_rows.append(torch.cat([rows[a][b] if rows[a][b] is not None else blocks[(y0, x0)].t()
+                                   for b, (y0, _) in enumerate(ysb)], dim=1))
+    return torch.cat(out_rows, dim=0)
+
+
+def _differentiable(solver, op, x, y, x_scale, y_scale, n_y, max_batch=1000):
+    """Route a call whose paths require grad through _LinearSigKernel (linear
+    kernel) or the increment route with _IncSolve (any other static kernel)."""
     if _wants_grad(x_scale, y_scale):
         raise NotImplementedError("gradients with respect to the path scales are not implemented")
+    if not _is_fused_linear(solver.static_kernel):
+        return _generic_differentiable(solver, "pairwise" if op == "pairwise" else "gram", x, y, x_scale,
+                                       y_scale, max_batch)
     _check_paths(x, "x")
     if y is not None:
         _check_paths(y, "y")
@@ -228,7 +318,7 @@ class SigPDE:
     # ------------------------------------------------------------------ pairwise
     def pairwise(self, x, y=None, x_scale=None, y_scale=None, max_batch=1000, max_threads=1024):
         if _wants_grad(x, y):
-            return _differentiable(self, "pairwise", x, y, x_scale, y_scale, None)
+            return _differentiable(self, "pairwise", x, y, x_scale, y_scale, None, max_batch)
         y_scale = x_scale if y is None else y_scale
         y = x if y is None else y
         _check_paths(x, "x")
@@ -278,8 +368,8 @@ class SigPDE:
     def gram(self, x, y=None, x_scale=None, y_scale=None, max_batch=1000, max_threads=1024):
         if _wants_grad(x, y):
             if y is None:
-                return _differentiable(self, "gram_sym", x, None, x_scale, None, None)
-            return _differentiable(self, "gram", x, y, x_scale, y_scale, y.shape[0])
+                return _differentiable(self, "gram_sym", x, None, x_scale, None, None, max_batch)
+            return _differentiable(self, "gram", x, y, x_scale, y_scale, y.shape[0], max_batch)
         if y is None:
             return self._gram_sym(x, x_scale, max_batch)
         return self._gram(x, y, x_scale, y_scale, max_batch)

@@ -137,10 +137,57 @@ def test_gradcheck_small(sig):
     assert torch.autograd.gradcheck(lambda a, b: k.pairwise(a, b[:2]), (x, y), eps=1e-6, atol=1e-7, rtol=1e-6)
 
 
+@pytest.mark.parametrize("kind", ["rbf", "l1rbf"])
+def test_static_kernel_gradients(sig, oracle, kind):
+    """RBF / L1-RBF: autograd through the torch static Gram of the increment route and
+    sigk_backward_inc, against the oracle's adjoint and chain rule."""
+    x = oracle.brownian(5, 14, 3, 61)
+    y = oracle.brownian(4, 17, 3, 62) + 0.05
+    sk = sig.kernels.RBFKernel(0.9) if kind == "rbf" else sig.kernels.L1RBFKernel(0.9)
+    k = sig.SigPDE(sk, 2)
+    w = np.random.default_rng(9).standard_normal((5, 4))
+    X, Y = cuda(x, grad=True), cuda(y, grad=True)
+    G = k.gram(X, Y, max_batch=9)  # 3 x 3 path tiles, as the reference tiles
+    np.testing.assert_allclose(host(G), oracle.gram(x, y, 2, static=kind, static_param=0.9), rtol=1e-9)
+    (G * cuda(w)).sum().backward()
+    gx, gy = oracle.grad_static_gram(kind, x, y, 2, w, 0.9)
+    close(host(X.grad), gx, TOL64, "grad x")
+    close(host(Y.grad), gy, TOL64, "grad y")
+    # pairwise with scales, and the symmetric Gram
+    X2, Y2 = cuda(x[:4], grad=True), cuda(y, grad=True)
+    sx, sy = np.linspace(0.7, 1.2, 4), np.linspace(1.1, 0.8, 4)
+    wp = np.array([1.0, -2.0, 0.5, 0.25])
+    (k.pairwise(X2, Y2, cuda(sx), cuda(sy)) * cuda(wp)).sum().backward()
+    gx, gy = oracle.grad_static_pairs(kind, x[:4], y, 2, wp, 0.9, sx, sy)
+    close(host(X2.grad), gx, TOL64, "pairwise grad x")
+    close(host(Y2.grad), gy, TOL64, "pairwise grad y")
+    xs = x + np.linspace(0, 0.2, 5)[:, None, None]
+    X3 = cuda(xs, grad=True)
+    ws = np.random.default_rng(10).standard_normal((5, 5))
+    (k.gram(X3, max_batch=4) * cuda(ws)).sum().backward()
+    close(host(X3.grad), oracle.grad_static_gram(kind, xs, None, 2, ws, 0.9), TOL64, "symmetric")
+
+
+def test_duck_typed_kernel_gradcheck(sig):
+    """Any object with the static-kernel protocol is differentiable through the
+    increment route: gradcheck on a polynomial kernel (1 + <x, y>)^2."""
+    class PolyKernel:
+        def pairwise(self, X, Y):
+            return (1 + torch.bmm(X, Y.transpose(1, 2))) ** 2
+
+        def gram(self, X, Y):
+            return (1 + torch.einsum("ipk,jqk->ijpq", X, Y)) ** 2
+
+    rng = np.random.default_rng(11)
+    x = cuda(rng.standard_normal((2, 4, 2)) * 0.3, grad=True)
+    y = cuda(rng.standard_normal((3, 5, 2)) * 0.3, grad=True)
+    k = sig.SigPDE(PolyKernel(), 1)
+    assert torch.autograd.gradcheck(lambda a, b: k.gram(a, b), (x, y), eps=1e-6, atol=1e-7, rtol=1e-6)
+    assert torch.autograd.gradcheck(lambda a, b: k.pairwise(a, b[:2, :4]), (x, y), eps=1e-6, atol=1e-7, rtol=1e-6)
+
+
 def test_backward_refusals(sig):
     x = cuda(np.zeros((2, 5, 2)), grad=True)
-    with pytest.raises(NotImplementedError):
-        sig.SigPDE(sig.kernels.RBFKernel(), 1).gram(x)
     with pytest.raises(NotImplementedError):
         sig.RobustSigPDE(sig.kernels.LinearKernel(), 1).pairwise(x)
     from sigpde_b200._lib import SigkError

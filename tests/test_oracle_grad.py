@@ -57,3 +57,25 @@ def test_grad_of_increments_is_linear_in_the_weight(oracle):
     g2, k2 = oracle.grad_increments(inc, 2, None, np.array([-2.5]))
     np.testing.assert_allclose(g2, -2.5 * g1, rtol=1e-14)
     assert k1[0] == k2[0] == oracle.solve_increments(inc, 2)[0]
+
+
+@pytest.mark.parametrize("kind", ["rbf", "l1rbf"])
+def test_static_kernel_gradients(oracle, kind):
+    """RBF / L1-RBF: the adjoint plus the chain rule through the static Gram and its
+    second difference, against central differences."""
+    x = oracle.brownian(2, 5, 2, 31)
+    y = oracle.brownian(2, 6, 2, 32) + 0.05  # no coincident coordinates: |.| has a kink at 0
+    w = np.array([1.2, -0.4])
+    gx, gy = oracle.grad_static_pairs(kind, x, y, 1, w, 0.9, np.array([0.8, 1.1]), np.array([1.3, 0.7]))
+
+    def f(xx, yy):
+        return float(np.dot(w, oracle.pairwise(xx, yy, 1, np.array([0.8, 1.1]), np.array([1.3, 0.7]),
+                                               static=kind, static_param=0.9)))
+
+    np.testing.assert_allclose(gx, _fd(lambda a: f(a, y), x), atol=1e-7)
+    np.testing.assert_allclose(gy, _fd(lambda a: f(x, a), y), atol=1e-7)
+    x = x + np.array([0.0, 0.03])[:, None, None]  # the two paths start apart
+    g = oracle.grad_static_gram(kind, x, None, 2, np.array([[1.0, 0.5], [-0.3, 2.0]]), 1.1)
+    fd = _fd(lambda a: float(np.sum(np.array([[1.0, 0.5], [-0.3, 2.0]]) *
+                                    oracle.gram(a, None, 2, static=kind, static_param=1.1))), x)
+    np.testing.assert_allclose(g, fd, atol=1e-7)
