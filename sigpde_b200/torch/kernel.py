@@ -230,9 +230,10 @@ def _generic_differentiable(solver, op, x, y, x_scale, y_scale, max_batch):
         sy = _broadcast_scale(ys, B, yv) if scaled else None
         parts = []
         for s0, s1 in _batches(B, max_batch):
-            inc = pairwise_inner_product(x[s0:s1], yv[s0:s1], solver.static_kernel, solver.dyadic_order)
-            parts.append(_IncSolve.apply(inc.to(x.dtype), None if sx is None else sx[s0:s1],
-                                         None if sy is None else sy[s0:s1], solver))
+            inc = pairwise_inner_product(x[s0:s1], yv[s0:s1], solver.static_kernel, solver.dyadic_order).to(x.dtype)
+            if scaled:  # in torch, so that autograd reaches the scales (sigpde/cuda_pairwise_kernels.py:73,81)
+                inc = inc * (sx[s0:s1] * sy[s0:s1])[:, None, None]
+            parts.append(_IncSolve.apply(inc, None, None, solver))
         return torch.cat(parts)
     sym = y is None
     yv = x if sym else y
@@ -251,12 +252,11 @@ def _generic_differentiable(solver, op, x, y, x_scale, y_scale, max_batch):
             if sym and y0 > x0:  # upper tiles are the transposed lower ones
                 row.append(None)
                 continue
-            inc = gram_inner_product(x[x0:x1], yv[y0:y1], solver.static_kernel, solver.dyadic_order)
+            inc = gram_inner_product(x[x0:x1], yv[y0:y1], solver.static_kernel, solver.dyadic_order).to(x.dtype)
+            if scaled:  # in torch, so that autograd reaches the scales (sigpde/cuda_gram_kernels.py:52,60)
+                inc = inc * (sx[x0:x1][:, None] * sy[y0:y1][None, :])[:, :, None, None]
             tx, ty, ncx, ncy = inc.shape
-            flat = inc.to(x.dtype).reshape(tx * ty, ncx, ncy)
-            vx = None if sx is None else sx[x0:x1].repeat_interleave(ty)
-            vy = None if sy is None else sy[y0:y1].repeat(tx)
-            blk = _IncSolve.apply(flat, vx, vy, solver).reshape(tx, ty)
+            blk = _IncSolve.apply(inc.reshape(tx * ty, ncx, ncy), None, None, solver).reshape(tx, ty)
             blocks[(x0, y0)] = blk
             row.append(blk)
         rows.append(row)
@@ -270,13 +270,25 @@ def _generic_differentiable(solver, op, x, y, x_scale, y_scale, max_batch):
 
 
 def _differentiable(solver, op, x, y, x_scale, y_scale, n_y, max_batch=1000):
-    """Route a call whose paths require grad through _LinearSigKernel (linear
-    kernel) or the increment route with _IncSolve (any other static kernel)."""
-    if _wants_grad(x_scale, y_scale):
-        raise NotImplementedError("gradients with respect to the path scales are not implemented")
+    """Route a call whose paths or scales require grad through _LinearSigKernel
+    (linear kernel) or the increment route with _IncSolve (any other static
+    kernel)."""
     if not _is_fused_linear(solver.static_kernel):
         return _generic_differentiable(solver, "pairwise" if op == "pairwise" else "gram", x, y, x_scale,
                                        y_scale, max_batch)
+    if _wants_grad(x_scale, y_scale):
+        # the linear kernel's increments scaled by s_x s_y are those of the paths scaled by s_x and s_y,
+        # so autograd reaches the scales through the paths
+        _check_paths(x, "x")
+        n_x = x.shape[0]
+        sx = _broadcast_scale(x_scale, n_x, x) if x_scale is not None else None
+        xs = x if sx is None else x * sx[:, None, None]
+        if op == "gram_sym" or (op == "pairwise" and y is None):
+            return _differentiable(solver, op, xs, None, None, None, n_y, max_batch)
+        _check_paths(y, "y")
+        sy = _broadcast_scale(y_scale, y.shape[0], y) if y_scale is not None else None
+        ys = y if sy is None else y * sy[:, None, None]
+        return _differentiable(solver, op, xs, ys, None, None, n_y, max_batch)
     _check_paths(x, "x")
     if y is not None:
         _check_paths(y, "y")
@@ -317,7 +329,7 @@ class SigPDE:
 
     # ------------------------------------------------------------------ pairwise
     def pairwise(self, x, y=None, x_scale=None, y_scale=None, max_batch=1000, max_threads=1024):
-        if _wants_grad(x, y):
+        if _wants_grad(x, y, x_scale, y_scale):
             return _differentiable(self, "pairwise", x, y, x_scale, y_scale, None, max_batch)
         y_scale = x_scale if y is None else y_scale
         y = x if y is None else y
@@ -366,7 +378,7 @@ class SigPDE:
 
     # ------------------------------------------------------------------ gram
     def gram(self, x, y=None, x_scale=None, y_scale=None, max_batch=1000, max_threads=1024):
-        if _wants_grad(x, y):
+        if _wants_grad(x, y, x_scale, y_scale):
             if y is None:
                 return _differentiable(self, "gram_sym", x, None, x_scale, None, None, max_batch)
             return _differentiable(self, "gram", x, y, x_scale, y_scale, y.shape[0], max_batch)
@@ -476,6 +488,49 @@ class SigPDE:
                   result.stride(0), prec, _ptr(ws), nws, _stream())
 
 
+class _RobustLambda(torch.autograd.Function):
+    """The robust normalisation lambda(x) of each path, differentiable by the
+    implicit function theorem.  lambda solves phi = k(lambda^2 inc) - f(k(inc)) = 0
+    (inc: the path's self-increments, k: the PDE solution; lambda = 0 where
+    k(inc) < 1, sigpde/torch/kernel.py:180-195), so
+        dlambda/dx = -(d phi / dx) / (d phi / d lambda),
+    both from autograd through the increments and _IncSolve's adjoint, the
+    normaliser's derivative from autograd on the normaliser."""
+
+    @staticmethod
+    def forward(ctx, x, robust, normalizer, tol, maxit, max_batch):
+        lam = robust._normalization(x, normalizer, tol, maxit, max_batch)[0]
+        ctx.robust = robust
+        ctx.normalizer = robust.normalizer if normalizer is None else normalizer
+        ctx.max_batch = max_batch
+        ctx.save_for_backward(x, lam)
+        return lam
+
+    @staticmethod
+    def backward(ctx, g_lam):
+        x, lam = ctx.saved_tensors
+        if not ctx.needs_input_grad[0]:
+            return None, None, None, None, None, None
+        rk = ctx.robust
+        solver = SigPDE(rk.static_kernel, rk.dyadic_order, "fp64")
+        with torch.enable_grad():
+            xg = x.detach().requires_grad_()
+            inc = pairwise_inner_product(xg, xg, rk.static_kernel, rk.dyadic_order).to(torch.float64)
+            lv = lam.detach().to(torch.float64).requires_grad_()
+            k_lam = _IncSolve.apply(inc * (lv * lv)[:, None, None], None, None, solver)
+            k_0 = _IncSolve.apply(inc, None, None, solver)
+            kk = k_0.detach().clone().requires_grad_()
+            fk = torch.as_tensor(ctx.normalizer(kk))
+            (fprime,) = torch.autograd.grad(fk.sum(), kk)
+            (phi_lam,) = torch.autograd.grad(k_lam.sum(), lv, retain_graph=True)
+            valid = (lv.detach() > 0) & torch.isfinite(k_0.detach()) & torch.isfinite(fprime) & (phi_lam != 0)
+            v = torch.where(valid, -g_lam.to(torch.float64) / torch.where(valid, phi_lam, torch.ones_like(phi_lam)),
+                            torch.zeros_like(phi_lam))
+            total = (v * k_lam).sum() - (v * fprime.detach() * k_0).sum()
+            (gx,) = torch.autograd.grad(total, xg)
+        return gx.to(x.dtype), None, None, None, None, None
+
+
 class RobustSigPDE:
     """Robust (tensor-normalised) signature kernel (sigpde/torch/kernel.py:174-301)."""
 
@@ -540,10 +595,13 @@ class RobustSigPDE:
 
     def pairwise(self, x, y=None, normalizer=None, tol=1e-8, maxit=100, max_batch=1000, max_threads=1024):
         """Robust pairwise kernel (sigpde/torch/kernel.py:232-291)."""
-        if _wants_grad(x, y):
-            raise NotImplementedError("gradients through the robust normalisation are not implemented "
-                                      "(RobustSigPDE.gram with explicit scales is differentiable in the paths)")
         solver = SigPDE(self.static_kernel, self.dyadic_order, self.precision)
+        if _wants_grad(x, y):
+            lx = _RobustLambda.apply(x, self, normalizer, tol, maxit, max_batch)
+            if y is None:
+                return solver.pairwise(x, None, lx, None, max_batch, max_threads)
+            ly = _RobustLambda.apply(y, self, normalizer, tol, maxit, max_batch)
+            return solver.pairwise(x, y, lx, ly, max_batch, max_threads)
         lx = self.normalization(x, normalizer, tol, maxit, max_batch, max_threads)
         if y is None:
             return solver.pairwise(x, None, lx, None, max_batch, max_threads)
@@ -553,9 +611,13 @@ class RobustSigPDE:
     def gram(self, x, y=None, x_scale=None, y_scale=None, normalizer=None, tol=1e-8, maxit=100, max_batch=1000,
              max_threads=1024):
         """Robust Gram (sigpde/torch/kernel.py:293-301): given scales skip the normalisation."""
-        if (x_scale is None and _wants_grad(x)) or (y is not None and y_scale is None and _wants_grad(y)):
-            raise NotImplementedError("gradients through the robust normalisation are not implemented "
-                                      "(pass x_scale / y_scale to differentiate with the scales held fixed)")
+        if _wants_grad(x, y):
+            xs = _RobustLambda.apply(x, self, normalizer, tol, maxit, max_batch) if x_scale is None else x_scale
+            ys = None
+            if y is not None:
+                ys = _RobustLambda.apply(y, self, normalizer, tol, maxit, max_batch) if y_scale is None else y_scale
+            solver = SigPDE(self.static_kernel, self.dyadic_order, self.precision)
+            return solver.gram(x, y, xs, ys, max_batch, max_threads)
         xs = self.normalization(x, normalizer, tol, maxit, max_batch, max_threads) if x_scale is None else x_scale
         if y is None:
             ys = None

@@ -166,12 +166,18 @@ def test_backward_argument_checks(built_lib):
     assert L.sigk_backward_workspace_size(_lib.SIGK_OP_GRAM, 2, 3, 8, 8, 3, 5, _lib.SIGK_F32) == 0
 
 
-def test_gradients_are_refused_where_not_implemented():
+def test_gradient_routing():
+    """Calls are routed to the differentiable path only when a path or a scale
+    requires grad and grad mode is on; CPU tensors are still rejected there."""
     import sigpde_b200.torch as sig
-    from sigpde_b200.torch.kernel import _differentiable
+    from sigpde_b200.torch.kernel import _wants_grad
     x = torch.zeros((2, 5, 3), requires_grad=True)
-    with pytest.raises(NotImplementedError, match="scales"):
-        _differentiable(sig.SigPDE(sig.kernels.LinearKernel(), 1), "gram", x, x,
-                        torch.ones(2, requires_grad=True), None, 2)
-    with pytest.raises(NotImplementedError, match="robust"):
-        sig.RobustSigPDE(sig.kernels.LinearKernel()).gram(x)
+    s = torch.ones(2, requires_grad=True)
+    assert _wants_grad(x) and _wants_grad(None, s) and not _wants_grad(x.detach(), None, 1.0)
+    with torch.no_grad():
+        assert not _wants_grad(x, s)
+    for k in (sig.SigPDE(sig.kernels.LinearKernel(), 1), sig.SigPDE(sig.kernels.RBFKernel(), 1)):
+        with pytest.raises(ValueError, match="CUDA"):
+            k.gram(x, x)
+        with pytest.raises(ValueError, match="CUDA"):
+            k.pairwise(x)

@@ -186,10 +186,75 @@ def test_duck_typed_kernel_gradcheck(sig):
     assert torch.autograd.gradcheck(lambda a, b: k.pairwise(a, b[:2, :4]), (x, y), eps=1e-6, atol=1e-7, rtol=1e-6)
 
 
+def _fd(f, arr, h=1e-6):
+    g = np.zeros_like(arr)
+    for idx in np.ndindex(arr.shape):
+        a = arr.copy()
+        a[idx] += h
+        fp = f(a)
+        a[idx] -= 2 * h
+        g[idx] = (fp - f(a)) / (2 * h)
+    return g
+
+
+def test_scale_gradients(sig, oracle):
+    """Gradients with respect to the per-path scales (linear: through the scaled
+    paths; RBF: through the scaled increments), against central differences."""
+    x = oracle.brownian(3, 9, 2, 71)
+    y = oracle.brownian(2, 8, 2, 72) + 0.05
+    sx, sy = np.array([0.7, 1.1, 0.9]), np.array([1.3, 0.6])
+    w = np.array([[1.0, -0.5], [0.3, 2.0], [-1.2, 0.4]])
+    for kind, sk in (("linear", sig.kernels.LinearKernel()), ("rbf", sig.kernels.RBFKernel(1.3))):
+        k = sig.SigPDE(sk, 1)
+        X, Y = cuda(x, grad=True), cuda(y, grad=True)
+        SX, SY = cuda(sx, grad=True), cuda(sy, grad=True)
+        (k.gram(X, Y, SX, SY) * cuda(w)).sum().backward()
+        param = 1.0 if kind == "linear" else 1.3
+
+        def f(ax=sx, ay=sy, xx=x):
+            return float(np.sum(w * oracle.gram(xx, y, 1, ax, ay, static=kind, static_param=param)))
+
+        close(host(SX.grad), _fd(lambda a: f(ax=a), sx), 1e-6, f"{kind} d/d scale_x")
+        close(host(SY.grad), _fd(lambda a: f(ay=a), sy), 1e-6, f"{kind} d/d scale_y")
+        close(host(X.grad), _fd(lambda a: f(xx=a), x), 1e-6, f"{kind} d/dx with scales")
+
+
+@pytest.mark.parametrize("kind", ["linear", "rbf"])
+def test_robust_gradients(sig, oracle, kind):
+    """RobustSigPDE is differentiable through lambda(x) (implicit function theorem),
+    against central differences of the oracle's robust kernel (tight root tolerance)."""
+    x = oracle.brownian(3, 8, 2, 81) * 3.0
+    y = oracle.brownian(2, 9, 2, 82) * 2.5 + 0.05
+    sk = sig.kernels.LinearKernel() if kind == "linear" else sig.kernels.RBFKernel(0.5)
+    param = 1.0 if kind == "linear" else 0.5
+    rk = sig.RobustSigPDE(sk, 1)
+    tol, maxit = 1e-13, 200
+    lam = oracle.normalization(x, 1, None, tol, maxit, static=kind, static_param=param)
+    assert np.all(lam > 0) and np.all(lam < 1), lam  # the normalisation is active on every path
+    w = np.array([[1.0, -0.5], [0.3, 2.0], [-1.2, 0.4]])
+    X, Y = cuda(x, grad=True), cuda(y, grad=True)
+    (rk.gram(X, Y, tol=tol, maxit=maxit) * cuda(w)).sum().backward()
+
+    def f(xx, yy):
+        lx = oracle.normalization(xx, 1, None, tol, maxit, static=kind, static_param=param)
+        ly = oracle.normalization(yy, 1, None, tol, maxit, static=kind, static_param=param)
+        return float(np.sum(w * oracle.gram(xx, yy, 1, lx, ly, static=kind, static_param=param)))
+
+    close(host(X.grad), _fd(lambda a: f(a, y), x), 1e-5, "robust gram d/dx")
+    close(host(Y.grad), _fd(lambda a: f(x, a), y), 1e-5, "robust gram d/dy")
+    X2 = cuda(x, grad=True)
+    wp = np.array([0.5, -1.0, 2.0])
+    (rk.pairwise(X2, tol=tol, maxit=maxit) * cuda(wp)).sum().backward()
+
+    def fp(xx):
+        lx = oracle.normalization(xx, 1, None, tol, maxit, static=kind, static_param=param)
+        return float(np.dot(wp, oracle.pairwise(xx, None, 1, lx, lx, static=kind, static_param=param)))
+
+    close(host(X2.grad), _fd(fp, x), 1e-5, "robust pairwise(x) d/dx")
+
+
 def test_backward_refusals(sig):
     x = cuda(np.zeros((2, 5, 2)), grad=True)
-    with pytest.raises(NotImplementedError):
-        sig.RobustSigPDE(sig.kernels.LinearKernel(), 1).pairwise(x)
     from sigpde_b200._lib import SigkError
     with pytest.raises(SigkError, match="order <= 4"):
         sig.SigPDE(sig.kernels.LinearKernel(), 5).gram(x, x).sum().backward()
