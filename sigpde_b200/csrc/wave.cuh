@@ -211,7 +211,8 @@ struct DeltaIncs {
         for (int rc = 0; rc < RC; ++rc) c[rc] = T(0);
         const T *dy = dY + cj;
         if (dxs) {
-#pragma unroll 4
+            // no unroll here: unrolling by 4 made the uneven batch 30% slower (11.2 vs 8.6 ms) and the
+            // fused d = 32 Grams 25% slower
             for (int64_t k = 0; k < d; ++k) {
                 const T v = dy[k * ncy];
 #pragma unroll
