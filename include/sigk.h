@@ -309,8 +309,10 @@ SIGK_API int sigk_pairwise_ragged(const void *x_pack, const int64_t *x_off, cons
                                   void *workspace, size_t workspace_bytes, sigk_stream_t stream);
 
 /*
- * Tensor-core increments for an uneven batch (precision SIGK_PREC_TC32 or
- * SIGK_PREC_TC64, dim <= 32).  Pair b's coarse increments
+ * Precomputed increments for an uneven batch: tensor cores (precision
+ * SIGK_PREC_TC32 or SIGK_PREC_TC64, dim <= 32), or, with SIGK_PREC_FP64 (any
+ * dim), float64 increments from one FP64 GEMM on the CUDA cores over the same
+ * plan's tiles into float64 blocks (offsets and ld in doubles).  Pair b's coarse increments
  * <d row_ci, d col_cj> (row path = the shorter of its two paths, as the
  * wavefront puts it on the rows; rows_b = its coarse cells, cols_b the other
  * path's) come from one grouped split-TF32 tcgen05 GEMM into a float32 block

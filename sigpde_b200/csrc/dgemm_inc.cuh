@@ -101,4 +101,119 @@ __global__ void __launch_bounds__(256, 3) dgemm_inc_kernel(DgemmIncParams p)
     }
 }
 
+// ------------------------------------------------------------------ uneven batches
+// Float64 increments of an uneven batch from the tensor-core plan's tables
+// (fp64 cells with d >= 16): the pairs' scaled differences as float64 row
+// images, [image row][k], with the same rows and scalings as the tensor-core
+// operand images (row path on side 0 with the static scale and 4^-order),
+// then one FP64 GEMM over the plan's 128 x 256 tiles in 64 x 64 pieces.
+template <typename TIN>
+__global__ void ragged_image64_kernel(TcRaggedImageParams p, double *img)
+{
+    for (int64_t b = blockIdx.y; b < p.npairs; b += gridDim.y) {
+        const int64_t lx = p.x_len[b], ly = p.y_len[b];
+        const bool use_y = (p.side == 0) == (lx > ly);
+        const TIN *pack = reinterpret_cast<const TIN *>(use_y ? p.y_pack : p.x_pack);
+        const TIN *sc = reinterpret_cast<const TIN *>(use_y ? p.sy : p.sx);
+        const int64_t off = use_y ? p.y_off[b] : p.x_off[b];
+        const int64_t nc = (use_y ? ly : lx) - 1;
+        const int ord = p.order[b];
+        const int64_t r0 = p.row0[b];
+        const int64_t rows8 = (nc + 7) & ~7LL;
+        // a pair the plan cannot hold is skipped; the wavefront refuses it too
+        if (nc < 1 || ord < 0 || ord > 12 || r0 < 0 || (r0 & 7) != 0 || r0 + rows8 > p.rows_alloc) continue;
+        double g = sc ? (double)sc[b] : 1.0;
+        if (p.side == 0) g *= p.f * ldexp(1.0, -2 * ord);
+        const TIN *xp0 = pack + off * p.d;
+        double *out = img + r0 * p.d;
+        const int64_t total = rows8 * p.d;
+        for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+             e += (int64_t)gridDim.x * blockDim.x) {
+            const int64_t c = e / p.d, k = e - c * p.d;
+            double v = 0.0;
+            if (c < nc) {
+                const TIN *xp = xp0 + c * p.d + k;
+                v = ((double)xp[p.d] - (double)xp[0]) * g;
+            }
+            out[e] = v;
+        }
+    }
+}
+
+struct RaggedDgemmParams {
+    const double *a, *b;   // row images [row][d]
+    int64_t a_rows, b_rows, d;
+    const int64_t *tiles;  // ntiles x (a_row, b_row, m_valid, n_valid, out_off, ld), the tensor-core plan's
+    int64_t ntiles;
+    double *out;
+    int64_t out_elems;
+    unsigned *err;         // set when a tile lies outside the buffers (that tile is skipped)
+};
+
+template <int TILE = kDgTile>
+__global__ void __launch_bounds__(256, 3) ragged_dgemm_kernel(RaggedDgemmParams p)
+{
+    static_assert(TILE == 64, "4x4 outputs per thread of a 16x16 block");
+    __shared__ double As[kDgK][TILE + 1];
+    __shared__ double Bs[kDgK][TILE + 1];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int64_t nsub = p.ntiles * 8; // 2 x 4 pieces of 64 x 64 per 128 x 256 tile
+    for (int64_t w = blockIdx.x; w < nsub; w += gridDim.x) {
+        const int64_t t = w >> 3;
+        const int mi = (int)(w & 7) >> 2, nj = (int)(w & 3);
+        const int64_t *te = p.tiles + t * 6;
+        const int64_t a_row = te[0], b_row = te[1], m_valid = te[2], n_valid = te[3], out_off = te[4], ld = te[5];
+        const int64_t m0 = (int64_t)mi * TILE, n0 = (int64_t)nj * TILE;
+        // rows to store: the pair's rows rounded up to 4 (its own zero padding), within this piece
+        const int64_t m_store = ((m_valid + 3) & ~3LL);
+        if (m0 >= m_store || n0 >= n_valid) continue; // uniform across the CTA
+        const bool ok = a_row >= 0 && b_row >= 0 && a_row + m_store <= p.a_rows &&
+                        b_row + n_valid <= p.b_rows && out_off >= 0 && ld >= m_store &&
+                        out_off + (n_valid - 1) * ld + m_store <= p.out_elems;
+        if (!ok) {
+            if (threadIdx.x == 0) atomicExch(p.err, 1u);
+            continue;
+        }
+        double acc[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+        for (int64_t k0 = 0; k0 < p.d; k0 += kDgK) {
+            // stage A[k][m] and B[k][n]: consecutive threads read consecutive k of one image row
+            for (int e = threadIdx.x; e < kDgK * TILE; e += 256) {
+                const int mm = e / kDgK, kk = e - mm * kDgK;
+                const int64_t k = k0 + kk;
+                const int64_t m = m0 + mm, n = n0 + mm;
+                As[kk][mm] = (k < p.d && m < m_store) ? p.a[(a_row + m) * p.d + k] : 0.0;
+                Bs[kk][mm] = (k < p.d && n < n_valid) ? p.b[(b_row + n) * p.d + k] : 0.0;
+            }
+            __syncthreads();
+            const int kn = (int)((p.d - k0) < kDgK ? (p.d - k0) : kDgK);
+            for (int kk = 0; kk < kn; ++kk) {
+                double a[4], bb[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) a[i] = As[kk][tx + 16 * i];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) bb[j] = Bs[kk][ty + 16 * j];
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], bb[j], acc[i][j]);
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int64_t n = n0 + ty + 16 * j;
+            if (n >= n_valid) continue;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int64_t m = m0 + tx + 16 * i;
+                if (m < m_store) p.out[out_off + n * ld + m] = acc[i][j];
+            }
+        }
+    }
+}
+
 } // namespace sigk

@@ -18,6 +18,7 @@ struct TcRaggedImageParams;
 struct DgemmIncParams;
 struct StaticIncParams;
 struct GradParams;
+struct RaggedDgemmParams;
 struct GradContractParams;
 }
 struct CUtensorMap_st; // cuda.h
@@ -54,7 +55,13 @@ StreamFn get_stream_reg_kernel_f32(int R, int O, int D);
 StreamFn get_stream_smem_kernel(bool f64cells, int R, int O);
 DeltaFn get_delta_kernel(bool f64cells, bool in64);
 // mat: increments from a precomputed matrix (tensor-core modes) instead of differences
-RaggedFn get_ragged_kernel(bool f64cells, bool in64, bool mat);
+// mat64: the increment matrix holds float64 (fp64 cells with a plan) instead of float32
+RaggedFn get_ragged_kernel(bool f64cells, bool in64, bool mat, bool mat64 = false);
+// float64 increments of an uneven batch (dgemm_inc.cuh)
+using RaggedImage64Fn = void (*)(TcRaggedImageParams, double *);
+RaggedImage64Fn get_ragged_image64_kernel(bool in64);
+using RaggedDgemmFn = void (*)(RaggedDgemmParams);
+RaggedDgemmFn get_ragged_dgemm_kernel();
 RaggedDeltaFn get_ragged_delta_kernel(bool f64cells, bool in64);
 // Tensor-core increments (tc.cuh): operand images, the TF32x3 GEMM (N tile
 // kTcBN) and the streaming wavefront that reads its output.

@@ -3,8 +3,9 @@
 #include "ragged.cuh"
 
 namespace sigk {
-RaggedFn get_ragged_kernel(bool f64cells, bool in64, bool mat)
+RaggedFn get_ragged_kernel(bool f64cells, bool in64, bool mat, bool mat64)
 {
+    if (mat && mat64) return in64 ? ragged_kernel<double, double, true, double> : ragged_kernel<double, float, true, double>;
     if (mat) {
         if (f64cells) return in64 ? ragged_kernel<double, double, true> : ragged_kernel<double, float, true>;
         return in64 ? ragged_kernel<float, double, true> : ragged_kernel<float, float, true>;

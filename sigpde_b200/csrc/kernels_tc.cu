@@ -41,6 +41,13 @@ TcGemmFn get_tc_gemm_kernel() { return tc_gemm_kernel<kTcBN>; }
 
 DgemmIncFn get_dgemm_inc_kernel() { return dgemm_inc_kernel<kDgTile>; }
 
+RaggedImage64Fn get_ragged_image64_kernel(bool in64)
+{
+    return in64 ? ragged_image64_kernel<double> : ragged_image64_kernel<float>;
+}
+
+RaggedDgemmFn get_ragged_dgemm_kernel() { return ragged_dgemm_kernel<kDgTile>; }
+
 namespace {
 template <int KIND>
 StaticIncFn static_by_dim(int64_t d)

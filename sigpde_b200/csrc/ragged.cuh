@@ -79,9 +79,10 @@ struct RaggedParams {
     int *error;                 // set to 1 if a wait ran out or an item was invalid
     void *pool;                 // boundary rows
     int stage_elems_per_warp;   // dx staging capacity (elements of T) per warp
-    // precomputed increments (tensor-core modes): pair b's block starts at inc + inc_off[b], column-major
-    // over its coarse cells (row path on the rows) with round_up(rows, 4) floats per column
-    const float *inc;
+    // precomputed increments (tensor-core modes: float; fp64 with a plan: double): pair b's block starts
+    // at inc + inc_off[b], column-major over its coarse cells (row path on the rows) with round_up(rows, 4)
+    // elements per column
+    const void *inc;
     const int64_t *inc_off;
     int64_t inc_elems;
     const unsigned *tc_err;     // non-zero: the GEMM skipped a tile, the matrix is incomplete
@@ -221,19 +222,19 @@ __device__ T band_solve(const SolveGeom &g, Src &src, int band, bool last, const
 struct BandSource {
     const void *dX, *dY;  // differences (T), !MAT
     int64_t d;
-    const float *mat;     // increment block, MAT
+    const void *mat;      // increment block (TM), MAT
     int64_t ld;
 };
 
-template <typename T, int R, int O, bool MAT>
+template <typename T, int R, int O, bool MAT, typename TM>
 __device__ T ragged_band(const BandSource &bs, int64_t ncx, int64_t ncy, int order, T *stage, int stage_cap, int band,
                          bool last, const T *top_buf, const int *top_prog, T *bot_buf, int *bot_prog, int *error)
 {
     using BS = BlockShape<R, O>;
     const SolveGeom g = make_geom<R, O>(ncx, ncy, order);
     if constexpr (MAT) {
-        MatIncs<T, BS::RC> src;
-        src.base = bs.mat;
+        MatIncs<T, BS::RC, TM> src;
+        src.base = reinterpret_cast<const TM *>(bs.mat);
         src.ld = bs.ld;
         src.ncy = ncy;
         return band_solve<T, R, O>(g, src, band, last, top_buf, top_prog, bot_buf, bot_prog, error);
@@ -248,21 +249,21 @@ __device__ T ragged_band(const BandSource &bs, int64_t ncx, int64_t ncy, int ord
     }
 }
 
-template <typename T, int R, bool MAT>
+template <typename T, int R, bool MAT, typename TM>
 __device__ T ragged_band_by_o(const BandSource &bs, int64_t ncx, int64_t ncy, int order, T *stage, int stage_cap,
                               int band, bool last, const T *tb, const int *tp, T *bb, int *bp, int *error)
 {
     switch (order) {
-    case 0: return ragged_band<T, R, 0, MAT>(bs, ncx, ncy, order, stage, stage_cap, band, last, tb, tp, bb, bp, error);
-    case 1: return ragged_band<T, R, 1, MAT>(bs, ncx, ncy, order, stage, stage_cap, band, last, tb, tp, bb, bp, error);
-    case 2: return ragged_band<T, R, 2, MAT>(bs, ncx, ncy, order, stage, stage_cap, band, last, tb, tp, bb, bp, error);
-    case 3: return ragged_band<T, R, 3, MAT>(bs, ncx, ncy, order, stage, stage_cap, band, last, tb, tp, bb, bp, error);
+    case 0: return ragged_band<T, R, 0, MAT, TM>(bs, ncx, ncy, order, stage, stage_cap, band, last, tb, tp, bb, bp, error);
+    case 1: return ragged_band<T, R, 1, MAT, TM>(bs, ncx, ncy, order, stage, stage_cap, band, last, tb, tp, bb, bp, error);
+    case 2: return ragged_band<T, R, 2, MAT, TM>(bs, ncx, ncy, order, stage, stage_cap, band, last, tb, tp, bb, bp, error);
+    case 3: return ragged_band<T, R, 3, MAT, TM>(bs, ncx, ncy, order, stage, stage_cap, band, last, tb, tp, bb, bp, error);
     default:
-        return ragged_band<T, R, 4, MAT>(bs, ncx, ncy, order, stage, stage_cap, band, last, tb, tp, bb, bp, error);
+        return ragged_band<T, R, 4, MAT, TM>(bs, ncx, ncy, order, stage, stage_cap, band, last, tb, tp, bb, bp, error);
     }
 }
 
-template <typename T, typename TIN, bool MAT>
+template <typename T, typename TIN, bool MAT, typename TM = float>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) ragged_kernel(RaggedParams p)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -340,15 +341,15 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) ragged_kernel(RaggedParam
         bs.dX = X;
         bs.dY = Y;
         bs.d = d;
-        bs.mat = MAT ? p.inc + p.inc_off[b] : nullptr;
+        bs.mat = MAT ? reinterpret_cast<const TM *>(p.inc) + p.inc_off[b] : nullptr;
         bs.ld = (ncx + 3) & ~3LL;
         const int cap = p.stage_elems_per_warp;
         T v;
         switch (R) {
-        case 2: v = ragged_band_by_o<T, 2, MAT>(bs, ncx, ncy, order, stage, cap, band, last, tb, tp, bb, bp, p.error); break;
-        case 4: v = ragged_band_by_o<T, 4, MAT>(bs, ncx, ncy, order, stage, cap, band, last, tb, tp, bb, bp, p.error); break;
-        case 8: v = ragged_band_by_o<T, 8, MAT>(bs, ncx, ncy, order, stage, cap, band, last, tb, tp, bb, bp, p.error); break;
-        default: v = ragged_band_by_o<T, 16, MAT>(bs, ncx, ncy, order, stage, cap, band, last, tb, tp, bb, bp, p.error); break;
+        case 2: v = ragged_band_by_o<T, 2, MAT, TM>(bs, ncx, ncy, order, stage, cap, band, last, tb, tp, bb, bp, p.error); break;
+        case 4: v = ragged_band_by_o<T, 4, MAT, TM>(bs, ncx, ncy, order, stage, cap, band, last, tb, tp, bb, bp, p.error); break;
+        case 8: v = ragged_band_by_o<T, 8, MAT, TM>(bs, ncx, ncy, order, stage, cap, band, last, tb, tp, bb, bp, p.error); break;
+        default: v = ragged_band_by_o<T, 16, MAT, TM>(bs, ncx, ncy, order, stage, cap, band, last, tb, tp, bb, bp, p.error); break;
         }
         if (last && lane == 0) out[b] = TIN(v);
     }

@@ -1849,6 +1849,22 @@ struct RaggedTcLayout {
     size_t err_off, a_off, a_bytes, b_off, b_bytes, inc_off, ws_bytes;
 };
 
+// With fp64 cells the same plan holds float64 row images [row][dim] and a
+// float64 increment matrix (no hi / lo split).
+RaggedTcLayout ragged_mat64_layout(size_t base, int64_t dim, const sigk_ragged_tc_plan &pl)
+{
+    RaggedTcLayout t{};
+    t.kp = (int)dim;
+    t.err_off = align256(base);
+    t.a_off = t.err_off + 256;
+    t.a_bytes = align256((size_t)pl.a_rows * dim * sizeof(double));
+    t.b_off = t.a_off + t.a_bytes;
+    t.b_bytes = align256((size_t)pl.b_rows * dim * sizeof(double));
+    t.inc_off = t.b_off + t.b_bytes;
+    t.ws_bytes = t.inc_off + align256((size_t)pl.inc_elems * sizeof(double));
+    return t;
+}
+
 RaggedTcLayout ragged_tc_layout(size_t base, int64_t dim, const sigk_ragged_tc_plan &pl)
 {
     RaggedTcLayout t{};
@@ -1888,10 +1904,12 @@ int run_ragged(const void *x_pack, const int64_t *x_off, const int64_t *x_len, i
         (st = check_dev(out, "out", false)) || (st = check_dev(scale_x, "scale_x", true)) ||
         (st = check_dev(scale_y, "scale_y", true)))
         return st;
+    const bool mat64 = tc && precision == SIGK_PREC_FP64; // float64 increments on the CUDA cores from the plan
     if (tc) {
-        if (!is_tc(precision)) return fail(SIGK_EINVAL, "a tensor-core plan needs precision SIGK_PREC_TC32 or _TC64");
-        if (dim > 32) return fail(SIGK_EUNSUPPORTED, "tensor-core increments support dim <= 32 (got %lld)",
-                                  (long long)dim);
+        if (!is_tc(precision) && !mat64)
+            return fail(SIGK_EINVAL, "a plan needs precision SIGK_PREC_TC32, _TC64 or _FP64");
+        if (!mat64 && dim > 32)
+            return fail(SIGK_EUNSUPPORTED, "tensor-core increments support dim <= 32 (got %lld)", (long long)dim);
         if (tc->a_rows < kTcM || tc->b_rows < kTcBN || tc->inc_elems < 4 || tc->ntiles < 1 ||
             (tc->a_rows & 7) || (tc->b_rows & 7))
             return fail(SIGK_EINVAL, "tensor-core plan sizes are inconsistent");
@@ -1906,7 +1924,7 @@ int run_ragged(const void *x_pack, const int64_t *x_off, const int64_t *x_len, i
     RaggedTcLayout tl{};
     size_t need = pl.ws_bytes;
     if (tc) {
-        tl = ragged_tc_layout(pl.dx_off, dim, *tc);
+        tl = mat64 ? ragged_mat64_layout(pl.dx_off, dim, *tc) : ragged_tc_layout(pl.dx_off, dim, *tc);
         need = tl.ws_bytes;
     }
     if (!workspace || workspace_bytes < need)
@@ -1934,6 +1952,55 @@ int run_ragged(const void *x_pack, const int64_t *x_off, const int64_t *x_len, i
         if (e != cudaSuccess) return cuda_fail(e, "ragged delta launch");
         p.dx_pack = wsb + pl.dx_off;
         p.dy_pack = wsb + pl.dy_off;
+    } else if (mat64) {
+        double *a_img = reinterpret_cast<double *>(wsb + tl.a_off), *b_img = reinterpret_cast<double *>(wsb + tl.b_off);
+        double *inc = reinterpret_cast<double *>(wsb + tl.inc_off);
+        unsigned *gerr = reinterpret_cast<unsigned *>(wsb + tl.err_off);
+        RaggedImage64Fn image = get_ragged_image64_kernel(in64);
+        const dim3 igrid(8, (unsigned)(npairs < 65535 ? npairs : 65535));
+        for (int side = 0; side < 2; ++side) {
+            TcRaggedImageParams ip{};
+            ip.x_pack = x_pack;
+            ip.y_pack = y_pack;
+            ip.x_off = x_off;
+            ip.x_len = x_len;
+            ip.y_off = y_off;
+            ip.y_len = y_len;
+            ip.order = order;
+            ip.f = static_scale;
+            ip.sx = scale_x;
+            ip.sy = scale_y;
+            ip.row0 = side == 0 ? tc->a_row0 : tc->b_row0;
+            ip.rows_alloc = side == 0 ? tc->a_rows : tc->b_rows;
+            ip.npairs = npairs;
+            ip.d = dim;
+            ip.side = side;
+            image<<<igrid, 256, 0, stream>>>(ip, side == 0 ? a_img : b_img);
+            count_launch();
+        }
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(e, "ragged float64 image launch");
+        RaggedDgemmParams gp{};
+        gp.a = a_img;
+        gp.b = b_img;
+        gp.a_rows = tc->a_rows;
+        gp.b_rows = tc->b_rows;
+        gp.d = dim;
+        gp.tiles = tc->tiles;
+        gp.ntiles = tc->ntiles;
+        gp.out = inc;
+        gp.out_elems = tc->inc_elems;
+        gp.err = gerr;
+        int64_t blocks = tc->ntiles * 8;
+        if (blocks > (int64_t)nsm * 24) blocks = (int64_t)nsm * 24;
+        get_ragged_dgemm_kernel()<<<(unsigned)blocks, 256, 0, stream>>>(gp);
+        count_launch();
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(e, "ragged float64 increment GEMM launch");
+        p.inc = inc;
+        p.inc_off = tc->inc_off;
+        p.inc_elems = tc->inc_elems;
+        p.tc_err = gerr;
     } else {
         float *a_hi = reinterpret_cast<float *>(wsb + tl.a_off), *a_lo = reinterpret_cast<float *>(wsb + tl.a_off + tl.a_bytes);
         float *b_hi = reinterpret_cast<float *>(wsb + tl.b_off), *b_lo = reinterpret_cast<float *>(wsb + tl.b_off + tl.b_bytes);
@@ -2008,7 +2075,7 @@ int run_ragged(const void *x_pack, const int64_t *x_off, const int64_t *x_len, i
     p.progress = reinterpret_cast<int *>(wsb + pl.progress_off);
     p.pool = wsb + pl.pool_off;
     p.stage_elems_per_warp = tc ? 0 : (int)(kRaggedStageBytesPerWarp / ts);
-    RaggedFn fn = get_ragged_kernel(f64, in64, tc != nullptr);
+    RaggedFn fn = get_ragged_kernel(f64, in64, tc != nullptr, mat64);
     const size_t smem = tc ? 0 : kRaggedStageBytesPerWarp * kWarpsPerBlock;
     int nb = 0;
     if ((st = blocks_per_sm((const void *)fn, smem, &nb))) return st;
@@ -2041,10 +2108,12 @@ extern "C" int sigk_pairwise_ragged(const void *x_pack, const int64_t *x_off, co
 extern "C" size_t sigk_ragged_tc_workspace_size(int64_t npairs, int64_t dim, int64_t nitems, int64_t bnd_elems,
                                                 int precision, const sigk_ragged_tc_plan *plan)
 {
-    if (!plan || npairs < 1 || dim < 1 || dim > 32 || nitems < npairs || bnd_elems < 0 || plan->a_rows < 0 ||
+    if (!plan || npairs < 1 || dim < 1 || (dim > 32 && precision != SIGK_PREC_FP64) || nitems < npairs ||
+        bnd_elems < 0 || plan->a_rows < 0 ||
         plan->b_rows < 0 || plan->inc_elems < 0)
         return 0;
     RaggedPlan pl = ragged_plan(npairs, 2 * npairs, 2 * npairs, dim, nitems, bnd_elems, tsize_of(precision));
+    if (precision == SIGK_PREC_FP64) return ragged_mat64_layout(pl.dx_off, dim, *plan).ws_bytes;
     return ragged_tc_layout(pl.dx_off, dim, *plan).ws_bytes;
 }
 

@@ -78,7 +78,9 @@ class RaggedTuner:
             if R in ROWS:
                 return R
         tsize = 8 if self.precision in ("fp64", "tc64") else 4
-        staged = not (self.precision in ("tc32", "tc64") and self.dim <= 32)
+        from .ragged import MAT64_MIN_DIM
+        staged = not ((self.precision in ("tc32", "tc64") and self.dim <= 32) or
+                      (self.precision == "fp64" and self.dim >= MAT64_MIN_DIM))
         return rows_per_lane(n, self.dim, order, tsize, staged)
 
     def save(self, path):

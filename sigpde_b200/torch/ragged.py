@@ -46,6 +46,7 @@ def pack(paths, dtype=None, device=None):
 
 
 STAGE_BYTES_PER_WARP = 16 * 1024  # the kernel's dx staging budget per warp
+MAT64_MIN_DIM = 16                # fp64 batches of this dimension or more take the float64 increment matrix
 
 
 def rows_per_lane(n, d, order, tsize, staged=True):
@@ -173,6 +174,9 @@ class RaggedPairwise:
         self.order = od.to(self.device)
         tsize = 8 if precision in ("fp64", "tc64") else 4
         use_tc = precision in ("tc32", "tc64") and self.dim <= 32
+        # fp64 with d >= MAT64_MIN_DIM: float64 increments of all pairs from one FP64 GEMM over the same
+        # plan's tiles, read by the wavefront (the d FMAs per coarse cell dominate the fused form there)
+        use_tc = use_tc or (precision == "fp64" and self.dim >= MAT64_MIN_DIM)
         if rows_fn is None and tuner is not None:  # rows per lane from measurements (autotune.py)
             tuner.tune_for(x_lengths, y_lengths, orders)
             rows_fn = tuner.rows_for

@@ -109,6 +109,29 @@ def test_ragged_scales_and_dimension(sig, oracle):
     assert _rel(got, _want(oracle, X, Y, orders, sx, sy)) <= 1e-9
 
 
+@pytest.mark.parametrize("dim", [16, 40])
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_ragged_float64_increment_matrix(sig, oracle, monkeypatch, dim, dtype):
+    """fp64 batches with d >= 16 take float64 increments from one FP64 GEMM over the
+    plan's tiles: the oracle's values, and the fused path's up to the order of the
+    scalings (rows on the shorter path, scales on either side)."""
+    from sigpde_b200.torch import ragged as rg
+    specs = [(lx, ly, dim, o) for lx, ly, _, o in SPECS]
+    X, Y = _batch(oracle, specs, 7, dtype)
+    orders = [s[3] for s in specs]
+    sx = np.linspace(0.6, 1.3, len(specs))
+    sy = np.linspace(1.2, 0.7, len(specs))
+    got = sig.ragged.pairwise(X, Y, orders, x_scale=sx, y_scale=sy).double().cpu().numpy()
+    tol = 1e-9 if dtype is torch.float64 else 2.5e-7
+    # the scales are held in the paths' dtype, as the reference holds them
+    sxe = torch.tensor(sx, dtype=dtype).double().numpy()
+    sye = torch.tensor(sy, dtype=dtype).double().numpy()
+    assert _rel(got, _want(oracle, X, Y, orders, sxe, sye)) <= tol
+    monkeypatch.setattr(rg, "MAT64_MIN_DIM", 1 << 30)  # the fused form
+    fused = sig.ragged.pairwise(X, Y, orders, x_scale=sx, y_scale=sy).double().cpu().numpy()
+    assert _rel(got, fused) <= (1e-12 if dtype is torch.float64 else 2.5e-7)
+
+
 def test_ragged_graph_replay_with_new_values(sig, oracle):
     specs = [(30 + 11 * i, 25 + 5 * i, 8, (i % 3) + 1) for i in range(20)]
     orders = [s[3] for s in specs]
