@@ -94,6 +94,7 @@ struct GradAuxFns {
 };
 GradAuxFns get_grad_aux_kernels();
 // mat64: the increment matrix holds float64 (dgemm_inc_kernel) instead of float32 (tensor cores)
-StreamIncFn get_stream_inc_kernel(bool f64cells, int R, int O, bool mat64);
+// W: lanes a pair pipeline (32, or 16 for pairs of at most 16 R rows with R <= 8)
+StreamIncFn get_stream_inc_kernel(bool f64cells, int R, int O, bool mat64, int W = 32);
 
 } // namespace sigk

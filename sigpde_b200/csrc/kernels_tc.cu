@@ -6,33 +6,40 @@
 
 namespace sigk {
 namespace {
-template <typename T, int R, typename TM>
+template <typename T, int R, typename TM, int W>
 StreamIncFn inc_by_o(int O)
 {
     switch (O) {
-    case 0: return stream_inc_kernel<T, R, 0, TM>;
-    case 1: return stream_inc_kernel<T, R, 1, TM>;
-    case 2: return stream_inc_kernel<T, R, 2, TM>;
-    case 3: return stream_inc_kernel<T, R, 3, TM>;
-    default: return stream_inc_kernel<T, R, 4, TM>;
+    case 0: return stream_inc_kernel<T, R, 0, TM, W>;
+    case 1: return stream_inc_kernel<T, R, 1, TM, W>;
+    case 2: return stream_inc_kernel<T, R, 2, TM, W>;
+    case 3: return stream_inc_kernel<T, R, 3, TM, W>;
+    default: return stream_inc_kernel<T, R, 4, TM, W>;
     }
 }
 template <typename T, typename TM>
-StreamIncFn inc_by_r(int R, int O)
+StreamIncFn inc_by_r(int R, int O, int W)
 {
+    if (W == 16) { // half-warp pipelines: pairs of at most 16 R rows, R <= 8
+        switch (R) {
+        case 2: return inc_by_o<T, 2, TM, 16>(O);
+        case 4: return inc_by_o<T, 4, TM, 16>(O);
+        default: return inc_by_o<T, 8, TM, 16>(O);
+        }
+    }
     switch (R) {
-    case 2: return inc_by_o<T, 2, TM>(O);
-    case 4: return inc_by_o<T, 4, TM>(O);
-    case 8: return inc_by_o<T, 8, TM>(O);
-    default: return inc_by_o<T, 16, TM>(O);
+    case 2: return inc_by_o<T, 2, TM, 32>(O);
+    case 4: return inc_by_o<T, 4, TM, 32>(O);
+    case 8: return inc_by_o<T, 8, TM, 32>(O);
+    default: return inc_by_o<T, 16, TM, 32>(O);
     }
 }
 } // namespace
 
-StreamIncFn get_stream_inc_kernel(bool f64cells, int R, int O, bool mat64)
+StreamIncFn get_stream_inc_kernel(bool f64cells, int R, int O, bool mat64, int W)
 {
-    if (mat64) return inc_by_r<double, double>(R, O);
-    return f64cells ? inc_by_r<double, float>(R, O) : inc_by_r<float, float>(R, O);
+    if (mat64) return inc_by_r<double, double>(R, O, W);
+    return f64cells ? inc_by_r<double, float>(R, O, W) : inc_by_r<float, float>(R, O, W);
 }
 
 TcImageFn get_tc_image_kernel(bool in64) { return in64 ? tc_image_kernel<double> : tc_image_kernel<float>; }

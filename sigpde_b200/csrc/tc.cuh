@@ -679,22 +679,31 @@ struct StreamIncParams {
     const unsigned *err; // non-zero: the GEMM gave up a wait; results are NaN
 };
 
-template <typename T, int R, int O, typename TM>
+// W lanes a pair pipeline: 32, or 16 for short pairs (n <= 16 R), where each
+// half-warp streams its own run of pairs (per_warp counts pairs per pipeline):
+// twice the rows a lane for the same pairs and half the pipeline fill.
+template <typename T, int R, int O, typename TM, int W = 32>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_inc_kernel(StreamIncParams p)
 {
+    static_assert(W == 32 || W == 16, "a pipeline is a warp or a half-warp");
     using BS = BlockShape<R, O>;
     constexpr int C = BS::C;
     constexpr int RC = BS::RC;
     const int lane = threadIdx.x & 31;
+    const int sl = lane & (W - 1); // lane within the pipeline
     const int wib = threadIdx.x >> 5;
     const int64_t gwarp = (int64_t)blockIdx.x * kWarpsPerBlock + wib;
-    const int64_t first = gwarp * p.per_warp;
-    if (first >= p.nitems) return; // warp-uniform
-    const int cnt = (int)((p.nitems - first) < p.per_warp ? (p.nitems - first) : p.per_warp);
+    const int64_t wfirst = gwarp * (32 / W) * p.per_warp; // the warp's first item
+    if (wfirst >= p.nitems) return;                        // warp-uniform: no pipeline of this warp has work
+    const int64_t first = wfirst + (lane / W) * p.per_warp;
+    const int64_t left_items = p.nitems - first;
+    const int cnt = left_items <= 0 ? 0 : (int)(left_items < p.per_warp ? left_items : p.per_warp);
+    // the warp's first pipeline has the longest run; all lanes loop over its steps (shuffles are warp-wide)
+    const int cnt_max = (int)((p.nitems - wfirst) < p.per_warp ? (p.nitems - wfirst) : p.per_warp);
     const int ncx = (int)p.ncx, ncy = (int)p.ncy;
     const int n = ncx << p.order;
     const int nsteps = (ncy << p.order) / C;
-    const int ci0 = (lane * R) >> p.order;
+    const int ci0 = (sl * R) >> p.order;
     const int lstar = (n - 1) / R, rstar = (n - 1) % R;
     const int64_t row_ld = p.op == kOpPairwise ? p.rows_x : p.ld;
     StreamParams sp{}; // for stream_decode / stream_store
@@ -704,7 +713,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_inc_kernel(StreamI
     sp.out = p.out;
     sp.out_ld = p.out_ld;
     if (*p.err) { // the increments are incomplete: report NaN rather than wrong numbers
-        for (int k2 = lane; k2 < cnt; k2 += 32) {
+        for (int k2 = sl; k2 < cnt; k2 += W) {
             int64_t xi, yj;
             const int64_t item = p.item0 + first + k2;
             stream_decode(sp, item, xi, yj);
@@ -724,7 +733,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_inc_kernel(StreamI
     int64_t item = 0, xi = 0, yj = 0;
     const TM *inc = reinterpret_cast<const TM *>(p.inc);
     const TM *base = inc;
-    const int total = cnt * nsteps + 31;
+    const int total = cnt_max * nsteps + (W - 1);
 
     // prefetch ring: the copy for the lane's step t + PF is issued at step t
     using Ring = IncRing<TM, RC, R * C>;
@@ -765,12 +774,12 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_inc_kernel(StreamI
     for (int s = 0; s < total; ++s) {
         T top[C];
 #pragma unroll
-        for (int c = 0; c < C; ++c) top[c] = __shfl_up_sync(kFullMask, bot[c], 1);
-        if (lane == 0) {
+        for (int c = 0; c < C; ++c) top[c] = __shfl_up_sync(kFullMask, bot[c], 1, W);
+        if (sl == 0) {
 #pragma unroll
             for (int c = 0; c < C; ++c) top[c] = T(1);
         }
-        if (s >= lane && k < cnt) {
+        if (s >= sl && k < cnt) {
             if (q == 0) {
                 item = p.item0 + first + k;
                 stream_decode(sp, item, xi, yj);
@@ -796,7 +805,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_inc_kernel(StreamI
 #pragma unroll
             for (int rc = 0; rc < RC; ++rc) stencil_coefs(cur[rc], A[rc], B[rc]);
             stream_block<T, R, O>(left, top, corner, A, B, bot);
-            if (q == nsteps - 1 && lane == lstar) stream_store(sp, item, xi, yj, pick_row(left, rstar));
+            if (q == nsteps - 1 && sl == lstar) stream_store(sp, item, xi, yj, pick_row(left, rstar));
             if (++q == nsteps) {
                 q = 0;
                 ++k;
