@@ -52,6 +52,8 @@ NormFn get_norm_pipe_kernel(bool in64, int mode, int R, int O);
 StreamFn get_stream_reg_kernel(bool f64cells, int R, int O, int D);
 StreamFn get_stream_reg_kernel_f64(int R, int O, int D);
 StreamFn get_stream_reg_kernel_f32(int R, int O, int D);
+// float32 cells, two pairs per lane on paired float32 instructions (same shapes)
+StreamFn get_stream_reg_kernel_f32x2(int R, int O, int D);
 StreamFn get_stream_smem_kernel(bool f64cells, int R, int O);
 DeltaFn get_delta_kernel(bool f64cells, bool in64);
 // mat: increments from a precomputed matrix (tensor-core modes) instead of differences

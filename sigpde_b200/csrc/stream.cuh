@@ -236,6 +236,146 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_reg_kernel(StreamP
     }
 }
 
+// Paired float32 cells.  A float32 lane of stream_reg_kernel is issue-bound
+// (5 float32 instructions per cell plus the per-step shuffles and loads), so
+// here each lane advances two pairs at once and every cell operation is one
+// sm_100 paired instruction (add / mul / fma .f32x2) on a (pair a, pair b)
+// register pair.  The arithmetic of each half is exactly the float32
+// stencil_coefs / stencil_cell above (k01 - k00 is formed as
+// fma(k00, -1, k01), which rounds identically), so every value is
+// bit-identical to stream_reg_kernel<float>.
+__device__ __forceinline__ float2 splat2(float v) { return make_float2(v, v); }
+
+template <>
+__device__ __forceinline__ void stencil_coefs<float2>(float2 c, float2 &a, float2 &b)
+{
+    const float2 c2 = __fmul2_rn(c, c);
+    b = __fmul2_rn(c2, splat2(1.0f / 12.0f));
+    a = __ffma2_rn(c, splat2(0.5f), b);
+}
+
+template <>
+__device__ __forceinline__ float2 stencil_cell<float2>(float2 k00, float2 k01, float2 k10, float2 a, float2 b)
+{
+    const float2 s = __fadd2_rn(k10, k01);
+    const float2 t = __ffma2_rn(k00, splat2(-1.0f), k01);
+    return __fadd2_rn(k10, __ffma2_rn(s, a, __ffma2_rn(k00, b, t)));
+}
+
+// stream_reg_kernel with paired float32 cells: the warp's run of items is
+// walked two at a time (items first + 2k and first + 2k + 1 share every
+// pipeline step; an odd run leaves the last step's second half unused).
+// dx holds (x_a, x_b) for each coarse row and dimension; it is reloaded only
+// when either x path changes.
+template <int R, int O, int D>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_reg_paired_kernel(StreamParams p)
+{
+    using BS = BlockShape<R, O>;
+    constexpr int C = BS::C;
+    constexpr int RC = BS::RC;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int64_t gwarp = (int64_t)blockIdx.x * kWarpsPerBlock + wib;
+    const int64_t first = gwarp * p.per_warp;
+    if (first >= p.nitems) return; // warp-uniform
+    const int cnt = (int)((p.nitems - first) < p.per_warp ? (p.nitems - first) : p.per_warp);
+    const int cnt2 = (cnt + 1) >> 1;
+    const float *dX = reinterpret_cast<const float *>(p.dx);
+    const float *dY = reinterpret_cast<const float *>(p.dy);
+    const int ncx = (int)p.ncx, ncy = (int)p.ncy;
+    const int n = ncx << p.order;
+    const int nsteps = (ncy << p.order) / C;
+    const int ci0 = (lane * R) >> p.order;
+    const int lstar = (n - 1) / R, rstar = (n - 1) % R;
+    const float2 one = splat2(1.0f);
+
+    float2 dx[RC][D];
+    int64_t cur_xa = -1, cur_xb = -1;
+    float2 left[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) left[r] = one;
+    float2 bot[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) bot[c] = one;
+    float2 corner_next = one;
+    int q = 0, k = 0;
+    int64_t ia = first, xa = 0, ya = 0, xb = 0, yb = 0;
+    bool hasb = false;
+    const float *dypa = dY, *dypb = dY;
+
+    const int total = cnt2 * nsteps + 31;
+    for (int s = 0; s < total; ++s) {
+        float2 top[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            top[c].x = __shfl_up_sync(kFullMask, bot[c].x, 1);
+            top[c].y = __shfl_up_sync(kFullMask, bot[c].y, 1);
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int c = 0; c < C; ++c) top[c] = one;
+        }
+        if (s >= lane && k < cnt2) {
+            if (q == 0) { // this lane starts items first + 2k, first + 2k + 1
+                ia = first + 2 * k;
+                hasb = 2 * k + 1 < cnt;
+                stream_decode(p, ia, xa, ya);
+                if (hasb) {
+                    stream_decode(p, ia + 1, xb, yb);
+                } else {
+                    xb = xa;
+                    yb = ya;
+                }
+                dypa = dY + ya * (int64_t)D * ncy;
+                dypb = dY + yb * (int64_t)D * ncy;
+                if (xa != cur_xa || xb != cur_xb) {
+                    cur_xa = xa;
+                    cur_xb = xb;
+                    const float *srca = dX + xa * (int64_t)D * ncx;
+                    const float *srcb = dX + xb * (int64_t)D * ncx;
+#pragma unroll
+                    for (int rc = 0; rc < RC; ++rc) {
+                        const int ci = ci0 + (RC > 1 ? rc : 0);
+                        const bool ok = ci < ncx;
+#pragma unroll
+                        for (int kk = 0; kk < D; ++kk)
+                            dx[rc][kk] = ok ? make_float2(srca[kk * ncx + ci], srcb[kk * ncx + ci]) : splat2(0.0f);
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < R; ++r) left[r] = one;
+            }
+            const float2 corner = (q == 0) ? one : corner_next;
+            corner_next = top[C - 1];
+            const int cj = (O <= 3) ? q : ((q * C) >> p.order);
+            float2 cc[RC];
+#pragma unroll
+            for (int rc = 0; rc < RC; ++rc) cc[rc] = splat2(0.0f);
+            const float *dyra = dypa + cj;
+            const float *dyrb = dypb + cj;
+#pragma unroll
+            for (int kk = 0; kk < D; ++kk) {
+                const float2 dy = make_float2(dyra[kk * ncy], dyrb[kk * ncy]);
+#pragma unroll
+                for (int rc = 0; rc < RC; ++rc) cc[rc] = __ffma2_rn(dx[rc][kk], dy, cc[rc]);
+            }
+            float2 A[RC], B[RC];
+#pragma unroll
+            for (int rc = 0; rc < RC; ++rc) stencil_coefs(cc[rc], A[rc], B[rc]);
+            stream_block<float2, R, O>(left, top, corner, A, B, bot);
+            if (q == nsteps - 1 && lane == lstar) {
+                const float2 v = pick_row(left, rstar);
+                stream_store(p, ia, xa, ya, v.x);
+                if (hasb) stream_store(p, ia + 1, xb, yb, v.y);
+            }
+            if (++q == nsteps) {
+                q = 0;
+                ++k;
+            }
+        }
+    }
+}
+
 template <typename T, int R, int O>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_smem_kernel(StreamParams p)
 {

@@ -249,6 +249,29 @@ def test_stream_and_per_pair_kernels_agree(sig, oracle, monkeypatch):
     assert_rel(a, oracle.gram(x, y, 2), RTOL64, "stream vs oracle")
 
 
+@pytest.mark.parametrize("Nx,Ny,Lx,Ly,d,o", STREAM_SHAPES + [(7, 5, 128, 130, 8, 2), (1, 1, 60, 64, 5, 1)])
+def test_paired_fp32_stream_bit_identical(sig, oracle, monkeypatch, Nx, Ny, Lx, Ly, d, o):
+    """float32 cells: the two-pairs-per-lane kernel (paired f32x2 instructions)
+    returns exactly the one-pair kernel's values, for odd and even runs of
+    items (Gram, scaled Gram, symmetric Gram, pairwise)."""
+    X = cuda(oracle.brownian(Nx, Lx, d, 400 + o))
+    Y = cuda(oracle.brownian(Ny, Ly, d, 500 + o))
+    sx = cuda(np.linspace(0.6, 1.4, Nx))
+    k = sig.SigPDE(sig.kernels.LinearKernel(), o, precision="fp32")
+    n = min(Nx, Ny)
+
+    def run():
+        return [host(k.gram(X, Y)), host(k.gram(X, Y, sx)), host(k.gram(Y)), host(k.pairwise(X[:n], Y[:n]))]
+
+    paired = run()
+    monkeypatch.setenv("SIGK_NO_PAIRED_F32", "1")
+    single = run()
+    monkeypatch.delenv("SIGK_NO_PAIRED_F32")
+    for a, b in zip(paired, single):
+        assert np.all(np.isfinite(a))
+        np.testing.assert_array_equal(a, b)
+
+
 def test_static_scale_and_broadcast(sig, oracle):
     x = oracle.brownian(4, 12, 3, 11)
     y = oracle.brownian(4, 12, 3, 12)
