@@ -22,7 +22,7 @@ LIB = os.path.join(HERE, "libsigk.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 SOURCES = ["sigk_api.cu", "kernels_pair_f64.cu", "kernels_pair_f32.cu", "kernels_norm.cu", "kernels_stream.cu",
-           "kernels_stream_reg_f64.cu", "kernels_stream_reg_f32.cu", "kernels_stream_reg_f32x2.cu", "kernels_ragged.cu", "kernels_tc.cu", "kernels_norm_pipe.cu",
+           "kernels_stream_reg_f64.cu", "kernels_stream_reg_f32.cu", "kernels_stream_reg_f32x2.cu", "kernels_stream_reg_f64x2.cu", "kernels_ragged.cu", "kernels_tc.cu", "kernels_norm_pipe.cu",
            "kernels_grad.cu"]
 HEADERS = ["wave.cuh", "sigk_kernels.cuh", "stream.cuh", "dispatch.h", "kernels_stream_reg.inc", "ragged.cuh", "tc.cuh", "norm_pipe.cuh", "dgemm_inc.cuh", "static_inc.cuh", "grad.cuh"]
 

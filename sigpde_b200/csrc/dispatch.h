@@ -54,6 +54,8 @@ StreamFn get_stream_reg_kernel_f64(int R, int O, int D);
 StreamFn get_stream_reg_kernel_f32(int R, int O, int D);
 // float32 cells, two pairs per lane on paired float32 instructions (same shapes)
 StreamFn get_stream_reg_kernel_f32x2(int R, int O, int D);
+// float64 cells, two Gram entries of one x path per lane (kOpGram only)
+StreamFn get_stream_reg_kernel_f64x2(int R, int O, int D);
 StreamFn get_stream_smem_kernel(bool f64cells, int R, int O);
 DeltaFn get_delta_kernel(bool f64cells, bool in64);
 // mat: increments from a precomputed matrix (tensor-core modes) instead of differences

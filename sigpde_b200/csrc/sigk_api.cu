@@ -1249,7 +1249,13 @@ int run_pairs(int op, const void *x, const void *y, int64_t nx, int64_t ny, int6
         sp.nitems = nitems;
         // float32 cells with register dx: two pairs per lane on paired instructions
         const bool paired = !f64 && pl.D && nitems >= 2 && !env_flag("SIGK_NO_PAIRED_F32");
+        // float64 cells of a Gram with register dx: two entries of one x path per lane
+        StreamFn dual_fn = (f64 && pl.D && op == kOpGram && ny >= 2 && !env_flag("SIGK_NO_DUAL_F64"))
+                               ? get_stream_reg_kernel_f64x2(pl.R, pl.O, pl.D)
+                               : nullptr;
+        const bool dual = dual_fn != nullptr;
         StreamFn fn = paired  ? get_stream_reg_kernel_f32x2(pl.R, pl.O, pl.D)
+                      : dual  ? dual_fn
                       : pl.D ? get_stream_reg_kernel(f64, pl.R, pl.O, pl.D)
                              : get_stream_smem_kernel(f64, pl.R, pl.O);
         if (!fn) return fail(SIGK_EUNSUPPORTED, "no stream kernel for R=%d O=%d D=%d", pl.R, pl.O, pl.D);
@@ -1257,11 +1263,12 @@ int run_pairs(int op, const void *x, const void *y, int64_t nx, int64_t ny, int6
         int nb = 0;
         if ((st = blocks_per_sm((const void *)fn, smem, &nb))) return st;
         int64_t nwarps = (int64_t)nsm * nb * kWarpsPerBlock;
-        const int64_t units = paired ? (nitems + 1) / 2 : nitems; // pipeline slots
+        const int64_t units = paired ? (nitems + 1) / 2 : dual ? nx * ((ny + 1) / 2) : nitems; // pipeline slots
         if (nwarps > units) nwarps = units;
         sp.per_warp = (units + nwarps - 1) / nwarps;
         if (paired) sp.per_warp *= 2; // an even run per warp: no half-empty slot but the last warp's
-        const int64_t used = (nitems + sp.per_warp - 1) / sp.per_warp;
+        if (dual) sp.nitems = units;  // the dual kernel walks entry pairs
+        const int64_t used = (sp.nitems + sp.per_warp - 1) / sp.per_warp;
         const int64_t blocks = (used + kWarpsPerBlock - 1) / kWarpsPerBlock;
         fn<<<(unsigned)blocks, kWarpsPerBlock * 32, smem, stream>>>(sp);
         count_launch();

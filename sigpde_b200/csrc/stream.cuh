@@ -376,6 +376,133 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_reg_paired_kernel(
     }
 }
 
+// Two Gram entries per lane with float64 cells: the lane advances entries
+// (xi, ya) and (xi, ya + 1) of one x path together, so each cell operation
+// comes as two independent float64 instructions (twice the instruction-level
+// parallelism of stream_reg_kernel, with dx held once).  Each half is exactly
+// stream_reg_kernel<double>'s arithmetic.  kOpGram only; items are entry pairs
+// t: xi = t / hy, ya = 2 (t % hy), hy = ceil(ny / 2) (the second entry is
+// absent when ya + 1 == ny).
+struct Dbl2 {
+    double x, y;
+};
+
+template <>
+__device__ __forceinline__ void stencil_coefs<Dbl2>(Dbl2 c, Dbl2 &A, Dbl2 &B)
+{
+    stencil_coefs<double>(c.x, A.x, B.x);
+    stencil_coefs<double>(c.y, A.y, B.y);
+}
+
+template <>
+__device__ __forceinline__ Dbl2 stencil_cell<Dbl2>(Dbl2 k00, Dbl2 k01, Dbl2 k10, Dbl2 A, Dbl2 B)
+{
+    return Dbl2{stencil_cell<double>(k00.x, k01.x, k10.x, A.x, B.x), stencil_cell<double>(k00.y, k01.y, k10.y, A.y, B.y)};
+}
+
+template <int R, int O, int D>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) stream_reg_dual_kernel(StreamParams p)
+{
+    using BS = BlockShape<R, O>;
+    constexpr int C = BS::C;
+    constexpr int RC = BS::RC;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int64_t gwarp = (int64_t)blockIdx.x * kWarpsPerBlock + wib;
+    const int64_t first = gwarp * p.per_warp;
+    if (first >= p.nitems) return; // warp-uniform
+    const int cnt = (int)((p.nitems - first) < p.per_warp ? (p.nitems - first) : p.per_warp);
+    const double *dX = reinterpret_cast<const double *>(p.dx);
+    const double *dY = reinterpret_cast<const double *>(p.dy);
+    const int ncx = (int)p.ncx, ncy = (int)p.ncy;
+    const int n = ncx << p.order;
+    const int nsteps = (ncy << p.order) / C;
+    const int ci0 = (lane * R) >> p.order;
+    const int lstar = (n - 1) / R, rstar = (n - 1) % R;
+    const int64_t hy = (p.ny + 1) >> 1;
+    const Dbl2 one{1.0, 1.0};
+
+    double dx[RC][D];
+    int64_t cur_x = -1;
+    Dbl2 left[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) left[r] = one;
+    Dbl2 bot[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) bot[c] = one;
+    Dbl2 corner_next = one;
+    int q = 0, k = 0;
+    int64_t xi = 0, ya = 0;
+    bool hasb = false;
+    const double *dypa = dY, *dypb = dY;
+
+    const int total = cnt * nsteps + 31;
+    for (int s = 0; s < total; ++s) {
+        Dbl2 top[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            top[c].x = __shfl_up_sync(kFullMask, bot[c].x, 1);
+            top[c].y = __shfl_up_sync(kFullMask, bot[c].y, 1);
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int c = 0; c < C; ++c) top[c] = one;
+        }
+        if (s >= lane && k < cnt) {
+            if (q == 0) { // this lane starts entries (xi, ya), (xi, ya + 1)
+                const int64_t t = first + k;
+                xi = t / hy;
+                ya = 2 * (t - xi * hy);
+                hasb = ya + 1 < p.ny;
+                dypa = dY + ya * (int64_t)D * ncy;
+                dypb = hasb ? dypa + (int64_t)D * ncy : dypa;
+                if (xi != cur_x) {
+                    cur_x = xi;
+                    const double *src = dX + xi * (int64_t)D * ncx;
+#pragma unroll
+                    for (int rc = 0; rc < RC; ++rc) {
+                        const int ci = ci0 + (RC > 1 ? rc : 0);
+#pragma unroll
+                        for (int kk = 0; kk < D; ++kk) dx[rc][kk] = (ci < ncx) ? src[kk * ncx + ci] : 0.0;
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < R; ++r) left[r] = one;
+            }
+            const Dbl2 corner = (q == 0) ? one : corner_next;
+            corner_next = top[C - 1];
+            const int cj = (O <= 3) ? q : ((q * C) >> p.order);
+            Dbl2 cc[RC];
+#pragma unroll
+            for (int rc = 0; rc < RC; ++rc) cc[rc] = Dbl2{0.0, 0.0};
+            const double *dyra = dypa + cj;
+            const double *dyrb = dypb + cj;
+#pragma unroll
+            for (int kk = 0; kk < D; ++kk) {
+                const double da = dyra[kk * ncy], db = dyrb[kk * ncy];
+#pragma unroll
+                for (int rc = 0; rc < RC; ++rc) {
+                    cc[rc].x = fma(dx[rc][kk], da, cc[rc].x);
+                    cc[rc].y = fma(dx[rc][kk], db, cc[rc].y);
+                }
+            }
+            Dbl2 A[RC], B[RC];
+#pragma unroll
+            for (int rc = 0; rc < RC; ++rc) stencil_coefs(cc[rc], A[rc], B[rc]);
+            stream_block<Dbl2, R, O>(left, top, corner, A, B, bot);
+            if (q == nsteps - 1 && lane == lstar) {
+                const Dbl2 v = pick_row(left, rstar);
+                stream_store(p, 0, xi, ya, v.x);
+                if (hasb) stream_store(p, 0, xi, ya + 1, v.y);
+            }
+            if (++q == nsteps) {
+                q = 0;
+                ++k;
+            }
+        }
+    }
+}
+
 template <typename T, int R, int O>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_smem_kernel(StreamParams p)
 {

@@ -272,6 +272,31 @@ def test_paired_fp32_stream_bit_identical(sig, oracle, monkeypatch, Nx, Ny, Lx, 
         np.testing.assert_array_equal(a, b)
 
 
+@pytest.mark.parametrize("Nx,Ny,Lx,Ly,d,o", STREAM_SHAPES + [(7, 5, 128, 130, 8, 2), (3, 2, 60, 64, 5, 1),
+                                                     (2, 1, 60, 64, 5, 1), (4, 3, 40, 40, 32, 0)])
+def test_dual_fp64_stream_bit_identical(sig, oracle, monkeypatch, Nx, Ny, Lx, Ly, d, o):
+    """float64 cells: the two-entries-per-lane Gram kernel returns exactly the
+    one-entry kernel's values (odd and even numbers of y paths, scaled and
+    unscaled, float32 and float64 inputs)."""
+    X = cuda(oracle.brownian(Nx, Lx, d, 600 + o), torch.float64)
+    Y = cuda(oracle.brownian(Ny, Ly, d, 700 + o), torch.float64)
+    sx = cuda(np.linspace(0.6, 1.4, Nx), torch.float64)
+    sy = cuda(np.linspace(1.2, 0.8, Ny), torch.float64)
+    k = sig.SigPDE(sig.kernels.LinearKernel(), o)
+
+    def run():
+        return [host(k.gram(X, Y)), host(k.gram(X, Y, sx, sy)), host(k.gram(X.float(), Y.float()))]
+
+    dual = run()
+    monkeypatch.setenv("SIGK_NO_DUAL_F64", "1")
+    single = run()
+    monkeypatch.delenv("SIGK_NO_DUAL_F64")
+    for a, b in zip(dual, single):
+        assert np.all(np.isfinite(a))
+        np.testing.assert_array_equal(a, b)
+    assert_rel(dual[0], oracle.gram(host(X), host(Y), o), RTOL64, "dual fp64 gram vs oracle")
+
+
 def test_static_scale_and_broadcast(sig, oracle):
     x = oracle.brownian(4, 12, 3, 11)
     y = oracle.brownian(4, 12, 3, 12)
