@@ -101,6 +101,101 @@ __global__ void __launch_bounds__(256, 3) dgemm_inc_kernel(DgemmIncParams p)
     }
 }
 
+// The same entries for d <= KD (16 or 32), pipelined: a CTA stages its A
+// tile (64 x-rows by d) once and walks the n tiles blockIdx.y,
+// blockIdx.y + gridDim.y, ... (for kTcLower only those below the diagonal, a
+// prefix of the walk); the next n tile's B values are loaded into registers
+// while the current tile is computed and stored, and B is double-buffered in
+// shared memory with one barrier per tile.  dgemm_inc_kernel stages, waits,
+// computes and stores each tile in turn (one tile per CTA), so its loads are
+// never overlapped with its own math.  Summation order and results are those
+// of dgemm_inc_kernel.
+template <int KD>
+__global__ void __launch_bounds__(256, 3) dgemm_inc_pipe_kernel(DgemmIncParams p)
+{
+    constexpr int TILE = kDgTile;
+    constexpr int LPT = KD * TILE / 256; // B (and A) values a thread stages per tile
+    extern __shared__ __align__(16) double dg_smem[];
+    double(*As)[TILE + 1] = reinterpret_cast<double(*)[TILE + 1]>(dg_smem);
+    double(*Bs)[KD][TILE + 1] = reinterpret_cast<double(*)[KD][TILE + 1]>(dg_smem + KD * (TILE + 1));
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int mm = threadIdx.x & (TILE - 1), kq = threadIdx.x / TILE;
+    const int64_t m0 = (int64_t)blockIdx.x * TILE;
+    const int64_t n_rows = p.npaths_y * p.ncy;
+    const int kd = (int)p.d;
+    int64_t n_end = n_rows;
+    if (p.mode == kTcLower) { // tiles with n0 / ncy > i_hi + x0 lie above the diagonal of path pairs
+        int64_t i_hi = (m0 + TILE - 1) / p.rows_x;
+        if (i_hi >= p.npaths_x) i_hi = p.npaths_x - 1;
+        const int64_t lim = (i_hi + p.x0 + 1) * p.ncy;
+        if (lim < n_end) n_end = lim;
+    }
+    const int64_t step = (int64_t)gridDim.y * TILE;
+    int64_t n0 = (int64_t)blockIdx.y * TILE;
+    if (n0 >= n_end) return; // uniform across the CTA, before any barrier
+    {
+        const int64_t m = m0 + mm;
+        const int64_t px = m / p.rows_x, cx = m - px * p.rows_x;
+        const bool a_ok = px < p.npaths_x && cx < p.ncx;
+        const double *a_src = p.dx + (a_ok ? px * p.d * p.ncx + cx : 0);
+#pragma unroll
+        for (int r = 0; r < LPT; ++r) {
+            const int kk = kq + r * (256 / TILE);
+            As[kk][mm] = (a_ok && kk < kd) ? a_src[kk * p.ncx] : 0.0;
+        }
+    }
+    double bv[LPT];
+    auto load_b = [&](int64_t nb) {
+        const int64_t n = nb + mm;
+        const int64_t qy = n / p.ncy, cy = n - qy * p.ncy;
+        const bool b_ok = n < n_rows;
+        const double *b_src = p.dy + (b_ok ? qy * p.d * p.ncy + cy : 0);
+#pragma unroll
+        for (int r = 0; r < LPT; ++r) {
+            const int kk = kq + r * (256 / TILE);
+            bv[r] = 0.0;
+            if (b_ok && kk < kd) bv[r] = b_src[kk * p.ncy];
+        }
+    };
+    load_b(n0);
+    int buf = 0;
+    for (; n0 < n_end; n0 += step) {
+#pragma unroll
+        for (int r = 0; r < LPT; ++r) Bs[buf][kq + r * (256 / TILE)][mm] = bv[r];
+        __syncthreads(); // this tile's B (and, the first time, A) is visible; the other buffer is free
+        if (n0 + step < n_end) load_b(n0 + step);
+        double acc[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+        for (int kk = 0; kk < kd; ++kk) {
+            double a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = As[kk][tx + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = Bs[buf][kk][ty + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int64_t n = n0 + ty + 16 * j;
+            if (n >= n_rows) continue;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int64_t m = m0 + tx + 16 * i;
+                if (m < p.ld) p.out[n * p.ld + m] = acc[i][j];
+            }
+        }
+        buf ^= 1;
+    }
+}
+
+constexpr size_t dgemm_pipe_smem_bytes(int kd) { return (size_t)3 * kd * (kDgTile + 1) * sizeof(double); }
+
 // ------------------------------------------------------------------ uneven batches
 // Float64 increments of an uneven batch from the tensor-core plan's tables
 // (fp64 cells with d >= 16): the pairs' scaled differences as float64 row

@@ -75,6 +75,9 @@ TcGemmFn get_tc_gemm_kernel();
 TcRaggedImageFn get_tc_ragged_image_kernel(bool in64);
 // float64 increment matrix on the CUDA cores (dgemm_inc.cuh)
 DgemmIncFn get_dgemm_inc_kernel();
+// pipelined variant for d <= 32 (null above), and its dynamic shared memory
+DgemmIncFn get_dgemm_inc_pipe_kernel(int64_t d);
+size_t dgemm_inc_pipe_smem(int64_t d);
 // float64 increment matrix of the RBF / L1-RBF static kernel from the path points (static_inc.cuh);
 // null for dim > 32
 StaticIncFn get_static_inc_kernel(int kind, int64_t dim);

@@ -48,6 +48,15 @@ TcGemmFn get_tc_gemm_kernel() { return tc_gemm_kernel<kTcBN>; }
 
 DgemmIncFn get_dgemm_inc_kernel() { return dgemm_inc_kernel<kDgTile>; }
 
+DgemmIncFn get_dgemm_inc_pipe_kernel(int64_t d)
+{
+    if (d <= 16) return dgemm_inc_pipe_kernel<16>;
+    if (d <= 32) return dgemm_inc_pipe_kernel<32>;
+    return nullptr;
+}
+
+size_t dgemm_inc_pipe_smem(int64_t d) { return dgemm_pipe_smem_bytes(d <= 16 ? 16 : 32); }
+
 RaggedImage64Fn get_ragged_image64_kernel(bool in64)
 {
     return in64 ? ragged_image64_kernel<double> : ragged_image64_kernel<float>;

@@ -644,6 +644,36 @@ constexpr int kDgMinDim = 16;
 
 // Layout of a float64 increment matrix plan; diffs: room for the scaled
 // differences of both sides (the linear kernel's GEMM operands).
+// The float64 increment GEMM over gp's matrix: pipelined (dgemm_inc_pipe_kernel,
+// about 8 waves of 3 CTAs per SM, each CTA walking a share of the n tiles) for
+// d <= 32, else one tile per CTA.  SIGK_NO_DGEMM_PIPE=1 selects the latter always.
+int launch_dgemm_inc(const DgemmIncParams &gp, cudaStream_t stream)
+{
+    const int64_t mt = (gp.ld + kDgTile - 1) / kDgTile;
+    int64_t nt = (gp.npaths_y * gp.ncy + kDgTile - 1) / kDgTile;
+    if (mt > 0x7fffffffLL) return fail(SIGK_EUNSUPPORTED, "increment matrix too large");
+    DgemmIncFn pipe = env_flag("SIGK_NO_DGEMM_PIPE") ? nullptr : get_dgemm_inc_pipe_kernel(gp.d);
+    if (pipe) {
+        const size_t smem = dgemm_inc_pipe_smem(gp.d);
+        if (smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute((const void *)pipe, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+        }
+        int64_t g = ((int64_t)sm_count() * 3 * 8 + mt - 1) / mt;
+        if (g > nt) g = nt;
+        if (g > 65535) g = 65535;
+        if (g < 1) g = 1;
+        pipe<<<dim3((unsigned)mt, (unsigned)g), 256, smem, stream>>>(gp);
+    } else {
+        if (nt > 65535) nt = 65535;
+        get_dgemm_inc_kernel()<<<dim3((unsigned)mt, (unsigned)nt), 256, 0, stream>>>(gp);
+    }
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? SIGK_OK : cuda_fail(e, "float64 increment GEMM launch");
+}
+
 TcPlan mat64_layout(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, int64_t d, int order, bool diffs)
 {
     TcPlan t{};
@@ -747,14 +777,7 @@ int run_pairs_mat64(const TcPlan &t, int op, const void *x, const void *y, int64
         gp.x0 = i0;
         gp.out = mat;
         gp.ld = nxc * t.rows_x;
-        const int64_t mt = (gp.ld + kDgTile - 1) / kDgTile;
-        int64_t nt = (gp.npaths_y * ncy + kDgTile - 1) / kDgTile;
-        if (nt > 65535) nt = 65535;
-        if (mt > 0x7fffffffLL) return fail(SIGK_EUNSUPPORTED, "increment matrix too large");
-        get_dgemm_inc_kernel()<<<dim3((unsigned)mt, (unsigned)nt), 256, 0, stream>>>(gp);
-        count_launch();
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return cuda_fail(e, "float64 increment GEMM launch");
+        if ((st = launch_dgemm_inc(gp, stream))) return st;
         if ((st = consume_matrix(t, op, mat, true, gp.ld, err, i0, i1, nx, ny, ncx, ncy, d, order, out, out_ld, in64,
                                  precision, dtype, wsb, stream)))
             return st;
@@ -972,11 +995,7 @@ int run_backward(const GradPlan &g, int op, const void *x, const void *y, int64_
             gp.x0 = i0;
             gp.out = mat;
             gp.ld = ld;
-            const int64_t mt = (ld + kDgTile - 1) / kDgTile;
-            int64_t nt = (ny * ncy + kDgTile - 1) / kDgTile;
-            if (nt > 65535) nt = 65535;
-            get_dgemm_inc_kernel()<<<dim3((unsigned)mt, (unsigned)nt), 256, 0, stream>>>(gp);
-            if ((st = launched("increment GEMM launch"))) return st;
+            if ((st = launch_dgemm_inc(gp, stream))) return st;
         }
         if ((st = run_rows(dx + i0 * d * ncx, nxc, ncx, g.rows_x, dxt))) return st;
         GradParams gp{};

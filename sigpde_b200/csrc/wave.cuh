@@ -152,6 +152,41 @@ __device__ __forceinline__ void load_mat_vals(const TM *row, int ci0, int ncx, T
     }
 }
 
+// The same values as load_mat_vals, left in the matrix's type so that the
+// registers can be read a step later: no conversion (which would wait for the
+// load) happens here, and the zero fill is a predicated load, not a select.
+template <typename TM, int RC>
+__device__ __forceinline__ void load_mat_raw(const TM *row, int ci0, int ncx, TM (&v)[RC])
+{
+    if constexpr (RC == 1) {
+        v[0] = TM(0);
+        if (ci0 < ncx) v[0] = row[ci0];
+    } else if constexpr (sizeof(TM) == 8) {
+#pragma unroll
+        for (int q = 0; q < RC / 2; ++q) {
+            double2 t = make_double2(0.0, 0.0);
+            if (ci0 + 2 * q < ncx) t = *reinterpret_cast<const double2 *>(row + ci0 + 2 * q);
+            v[2 * q + 0] = t.x;
+            v[2 * q + 1] = t.y;
+        }
+    } else if constexpr (RC == 2) {
+        float2 t = make_float2(0.f, 0.f);
+        if (ci0 < ncx) t = *reinterpret_cast<const float2 *>(row + ci0);
+        v[0] = t.x;
+        v[1] = t.y;
+    } else {
+#pragma unroll
+        for (int q = 0; q < RC / 4; ++q) {
+            float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (ci0 + 4 * q < ncx) t = *reinterpret_cast<const float4 *>(row + ci0 + 4 * q);
+            v[4 * q + 0] = t.x;
+            v[4 * q + 1] = t.y;
+            v[4 * q + 2] = t.z;
+            v[4 * q + 3] = t.w;
+        }
+    }
+}
+
 template <typename T, int RC, typename TM = float>
 struct MatIncs {
     const TM *base;

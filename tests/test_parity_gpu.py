@@ -297,6 +297,30 @@ def test_dual_fp64_stream_bit_identical(sig, oracle, monkeypatch, Nx, Ny, Lx, Ly
     assert_rel(dual[0], oracle.gram(host(X), host(Y), o), RTOL64, "dual fp64 gram vs oracle")
 
 
+@pytest.mark.parametrize("Nx,Ny,L,d,o", [(9, 7, 40, 16, 1), (6, 11, 33, 24, 0), (5, 4, 70, 32, 2), (13, 1, 20, 17, 3)])
+def test_pipelined_dgemm_increments_bit_identical(sig, oracle, monkeypatch, Nx, Ny, L, d, o):
+    """fp64 Grams of wide paths take their increments from a float64 GEMM; the
+    pipelined GEMM (A tile kept, B tiles prefetched) gives exactly the
+    one-tile-per-CTA GEMM's results (Gram, scaled, symmetric)."""
+    X = cuda(oracle.brownian(Nx, L, d, 800 + d), torch.float64)
+    Y = cuda(oracle.brownian(Ny, L + 5, d, 900 + d), torch.float64)
+    sx = cuda(np.linspace(0.7, 1.3, Nx), torch.float64)
+    k = sig.SigPDE(sig.kernels.LinearKernel(), o)
+
+    def run():
+        return [host(k.gram(X, Y)), host(k.gram(X, Y, sx)), host(k.gram(X)), host(k.gram(X, None, sx))]
+
+    pipe = run()
+    monkeypatch.setenv("SIGK_NO_DGEMM_PIPE", "1")
+    single = run()
+    monkeypatch.delenv("SIGK_NO_DGEMM_PIPE")
+    for a, b in zip(pipe, single):
+        assert np.all(np.isfinite(a))
+        np.testing.assert_array_equal(a, b)
+    assert_rel(pipe[0], oracle.gram(host(X), host(Y), o), RTOL64, "pipelined dgemm gram vs oracle")
+    assert_rel(pipe[2], oracle.gram(host(X), None, o), RTOL64, "pipelined dgemm sym gram vs oracle")
+
+
 def test_static_scale_and_broadcast(sig, oracle):
     x = oracle.brownian(4, 12, 3, 11)
     y = oracle.brownian(4, 12, 3, 12)
