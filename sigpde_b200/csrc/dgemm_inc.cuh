@@ -311,4 +311,100 @@ __global__ void __launch_bounds__(256, 3) ragged_dgemm_kernel(RaggedDgemmParams 
     }
 }
 
+// ragged_dgemm_kernel for d <= KD (16 or 32), pipelined: the unit of work is
+// the half-tile (tile t, A block mi) whose 4 pieces share their 64 A rows.
+// The CTA stages those rows (all of K) once and walks the half-tile's pieces,
+// loading the next piece's B rows into registers during the current piece's
+// FMAs and stores (B single-buffered in shared memory, two barriers a piece,
+// so that KD = 32 stays within 48 KB of static shared memory).  Summation
+// order, stored rows and error reporting are those of ragged_dgemm_kernel.
+template <int KD>
+__global__ void __launch_bounds__(256, 3) ragged_dgemm_pipe_kernel(RaggedDgemmParams p)
+{
+    constexpr int TILE = kDgTile;
+    constexpr int LPT = KD * TILE / 256; // values a thread stages per block of A or B
+    __shared__ double As[KD][TILE + 1];
+    __shared__ double Bs[KD][TILE + 1];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int kd = (int)p.d;
+    const int64_t nunits = p.ntiles * 2;
+    double bv[LPT];
+    for (int64_t u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const int64_t t = u >> 1;
+        const int mi = (int)(u & 1);
+        const int64_t *te = p.tiles + t * 6;
+        const int64_t a_row = te[0], b_row = te[1], m_valid = te[2], n_valid = te[3], out_off = te[4], ld = te[5];
+        const int64_t m0 = (int64_t)mi * TILE;
+        const int64_t m_store = ((m_valid + 3) & ~3LL);
+        if (m0 >= m_store || n_valid <= 0) continue; // uniform across the CTA
+        const bool ok = a_row >= 0 && b_row >= 0 && a_row + m_store <= p.a_rows &&
+                        b_row + n_valid <= p.b_rows && out_off >= 0 && ld >= m_store &&
+                        out_off + (n_valid - 1) * ld + m_store <= p.out_elems;
+        if (!ok) {
+            if (threadIdx.x == 0) atomicExch(p.err, 1u);
+            continue;
+        }
+        int npieces = (int)((n_valid + TILE - 1) / TILE);
+        if (npieces > 4) npieces = 4;
+        auto load_b = [&](int nj) {
+            const int64_t n0 = (int64_t)nj * TILE;
+#pragma unroll
+            for (int r = 0; r < LPT; ++r) {
+                const int e = threadIdx.x + r * 256;
+                const int mm = e / KD, kk = e - mm * KD;
+                const int64_t n = n0 + mm;
+                bv[r] = 0.0;
+                if (kk < kd && n < n_valid) bv[r] = p.b[(b_row + n) * p.d + kk];
+            }
+        };
+        __syncthreads(); // the previous unit's reads of As and Bs are done
+#pragma unroll
+        for (int r = 0; r < LPT; ++r) {
+            const int e = threadIdx.x + r * 256;
+            const int mm = e / KD, kk = e - mm * KD;
+            const int64_t m = m0 + mm;
+            As[kk][mm] = (kk < kd && m < m_store) ? p.a[(a_row + m) * p.d + kk] : 0.0;
+        }
+        load_b(0);
+        for (int nj = 0; nj < npieces; ++nj) {
+            if (nj > 0) __syncthreads(); // the previous piece's reads of Bs are done
+#pragma unroll
+            for (int r = 0; r < LPT; ++r) {
+                const int e = threadIdx.x + r * 256;
+                const int mm = e / KD, kk = e - mm * KD;
+                Bs[kk][mm] = bv[r];
+            }
+            __syncthreads(); // this piece's B (and the unit's A) is visible
+            if (nj + 1 < npieces) load_b(nj + 1);
+            double acc[4][4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+            for (int kk = 0; kk < kd; ++kk) {
+                double a[4], bb[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) a[i] = As[kk][tx + 16 * i];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) bb[j] = Bs[kk][ty + 16 * j];
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], bb[j], acc[i][j]);
+            }
+            const int64_t n0 = (int64_t)nj * TILE;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int64_t n = n0 + ty + 16 * j;
+                if (n >= n_valid) continue;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int64_t m = m0 + tx + 16 * i;
+                    if (m < m_store) p.out[out_off + n * ld + m] = acc[i][j];
+                }
+            }
+        }
+    }
+}
+
 } // namespace sigk

@@ -66,6 +66,8 @@ using RaggedImage64Fn = void (*)(TcRaggedImageParams, double *);
 RaggedImage64Fn get_ragged_image64_kernel(bool in64);
 using RaggedDgemmFn = void (*)(RaggedDgemmParams);
 RaggedDgemmFn get_ragged_dgemm_kernel();
+// pipelined variant (half-tiles sharing their A rows) for d <= 32, null above
+RaggedDgemmFn get_ragged_dgemm_pipe_kernel(int64_t d);
 RaggedDeltaFn get_ragged_delta_kernel(bool f64cells, bool in64);
 // Tensor-core increments (tc.cuh): operand images, the TF32x3 GEMM (N tile
 // kTcBN) and the streaming wavefront that reads its output.

@@ -64,6 +64,13 @@ RaggedImage64Fn get_ragged_image64_kernel(bool in64)
 
 RaggedDgemmFn get_ragged_dgemm_kernel() { return ragged_dgemm_kernel<kDgTile>; }
 
+RaggedDgemmFn get_ragged_dgemm_pipe_kernel(int64_t d)
+{
+    if (d <= 16) return ragged_dgemm_pipe_kernel<16>;
+    if (d <= 32) return ragged_dgemm_pipe_kernel<32>;
+    return nullptr;
+}
+
 namespace {
 template <int KIND>
 StaticIncFn static_by_dim(int64_t d)

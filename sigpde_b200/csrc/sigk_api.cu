@@ -2035,9 +2035,10 @@ int run_ragged(const void *x_pack, const int64_t *x_off, const int64_t *x_len, i
         gp.out = inc;
         gp.out_elems = tc->inc_elems;
         gp.err = gerr;
-        int64_t blocks = tc->ntiles * 8;
+        RaggedDgemmFn rpipe = env_flag("SIGK_NO_DGEMM_PIPE") ? nullptr : get_ragged_dgemm_pipe_kernel(dim);
+        int64_t blocks = tc->ntiles * (rpipe ? 2 : 8); // half-tiles / pieces
         if (blocks > (int64_t)nsm * 24) blocks = (int64_t)nsm * 24;
-        get_ragged_dgemm_kernel()<<<(unsigned)blocks, 256, 0, stream>>>(gp);
+        (rpipe ? rpipe : get_ragged_dgemm_kernel())<<<(unsigned)blocks, 256, 0, stream>>>(gp);
         count_launch();
         e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_fail(e, "ragged float64 increment GEMM launch");

@@ -132,6 +132,24 @@ def test_ragged_float64_increment_matrix(sig, oracle, monkeypatch, dim, dtype):
     assert _rel(got, fused) <= (1e-12 if dtype is torch.float64 else 2.5e-7)
 
 
+@pytest.mark.parametrize("dim", [16, 24, 32])
+def test_ragged_pipelined_dgemm_bit_identical(sig, oracle, monkeypatch, dim):
+    """The pipelined float64 GEMM (half-tiles sharing their A rows, next B rows
+    prefetched) gives exactly the one-piece-per-CTA GEMM's increments."""
+    specs = [(lx, ly, dim, o) for lx, ly, _, o in SPECS]
+    X, Y = _batch(oracle, specs, 11, torch.float64)
+    orders = [s[3] for s in specs]
+    sx = np.linspace(0.6, 1.3, len(specs))
+    pipe = sig.ragged.pairwise(X, Y, orders, x_scale=sx).cpu().numpy()
+    monkeypatch.setenv("SIGK_NO_DGEMM_PIPE", "1")
+    single = sig.ragged.pairwise(X, Y, orders, x_scale=sx).cpu().numpy()
+    monkeypatch.delenv("SIGK_NO_DGEMM_PIPE")
+    assert np.all(np.isfinite(pipe))
+    np.testing.assert_array_equal(pipe, single)
+    sxe = torch.tensor(sx, dtype=torch.float64).numpy()
+    assert _rel(pipe, _want(oracle, X, Y, orders, sxe, np.ones(len(specs)))) <= 1e-9
+
+
 def test_ragged_graph_replay_with_new_values(sig, oracle):
     specs = [(30 + 11 * i, 25 + 5 * i, 8, (i % 3) + 1) for i in range(20)]
     orders = [s[3] for s in specs]
