@@ -156,11 +156,12 @@ SIGK_API int sigk_gram_sym(const void *x, int64_t n, int64_t len, int64_t dim, i
  * (sigpde/torch/kernel.py:18-21,75-171, sigpde/torch/static_kernels.py:13-53,
  * sigpde/cuda_gram_kernels.py:8-164).  The static Gram is evaluated in
  * float64 (the reference uses the input dtype) and each increment is written
- * once to a float64 matrix in the workspace, which the wavefront reads; the
- * cells are float64, so precision must be SIGK_PREC_FP64 or SIGK_PREC_TC64,
- * and dim <= 32 (SIGK_EUNSUPPORTED otherwise: sigk_gram_inc takes any
- * increments).  Workspace: sigk_static_workspace_size(op, kind, ...) bytes,
- * 256-byte aligned.
+ * once to a matrix in the workspace, which the wavefront reads: float64 for
+ * float64 cells (SIGK_PREC_FP64 / SIGK_PREC_TC64), rounded once to float32
+ * for float32 cells (SIGK_PREC_FP32 / SIGK_PREC_TC32).  dim <= 32
+ * (SIGK_EUNSUPPORTED otherwise: sigk_gram_inc takes any increments).
+ * Workspace: sigk_static_workspace_size(op, kind, ...) bytes, 256-byte
+ * aligned.
  */
 SIGK_API size_t sigk_static_workspace_size(int op, int kind, int64_t n_x, int64_t n_y, int64_t len_x, int64_t len_y,
                                            int64_t dim, int order, int dtype, int precision);

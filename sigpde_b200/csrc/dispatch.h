@@ -82,7 +82,8 @@ DgemmIncFn get_dgemm_inc_pipe_kernel(int64_t d);
 size_t dgemm_inc_pipe_smem(int64_t d);
 // float64 increment matrix of the RBF / L1-RBF static kernel from the path points (static_inc.cuh);
 // null for dim > 32
-StaticIncFn get_static_inc_kernel(int kind, int64_t dim);
+// out64: float64 matrix (float64 cells), else float32 (float32 cells)
+StaticIncFn get_static_inc_kernel(int kind, int64_t dim, bool out64);
 // backward pass (grad.cuh): forward-with-derivatives and adjoint wavefronts for R rows a lane,
 // order O (R >= 2^O); null members where the combination is not built
 struct GradFns {

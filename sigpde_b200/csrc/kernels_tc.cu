@@ -72,22 +72,24 @@ RaggedDgemmFn get_ragged_dgemm_pipe_kernel(int64_t d)
 }
 
 namespace {
-template <int KIND>
+template <int KIND, typename TO>
 StaticIncFn static_by_dim(int64_t d)
 {
-    if (d <= 2) return static_inc_kernel<KIND, 2>;
-    if (d <= 4) return static_inc_kernel<KIND, 4>;
-    if (d <= 8) return static_inc_kernel<KIND, 8>;
-    if (d <= 16) return static_inc_kernel<KIND, 16>;
-    if (d <= 32) return static_inc_kernel<KIND, 32>;
+    if (d <= 2) return static_inc_kernel<KIND, 2, TO>;
+    if (d <= 4) return static_inc_kernel<KIND, 4, TO>;
+    if (d <= 8) return static_inc_kernel<KIND, 8, TO>;
+    if (d <= 16) return static_inc_kernel<KIND, 16, TO>;
+    if (d <= 32) return static_inc_kernel<KIND, 32, TO>;
     return nullptr;
 }
 } // namespace
 
-StaticIncFn get_static_inc_kernel(int kind, int64_t dim)
+StaticIncFn get_static_inc_kernel(int kind, int64_t dim, bool out64)
 {
-    if (kind == kStaticRbf) return static_by_dim<kStaticRbf>(dim);
-    if (kind == kStaticL1Rbf) return static_by_dim<kStaticL1Rbf>(dim);
+    if (kind == kStaticRbf)
+        return out64 ? static_by_dim<kStaticRbf, double>(dim) : static_by_dim<kStaticRbf, float>(dim);
+    if (kind == kStaticL1Rbf)
+        return out64 ? static_by_dim<kStaticL1Rbf, double>(dim) : static_by_dim<kStaticL1Rbf, float>(dim);
     return nullptr;
 }
 

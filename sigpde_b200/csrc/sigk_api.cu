@@ -787,7 +787,7 @@ int run_pairs_mat64(const TcPlan &t, int op, const void *x, const void *y, int64
 
 int run_pairs_static(const TcPlan &t, int op, int kind, double param, const void *x, const void *y, int64_t nx,
                      int64_t ny, int64_t lx, int64_t ly, int64_t d, int dtype, int order, const void *sx,
-                     const void *sy, void *out, int64_t out_ld, void *ws, cudaStream_t stream)
+                     const void *sy, void *out, int64_t out_ld, int precision, void *ws, cudaStream_t stream)
 {
     int st;
     const bool in64 = dtype == SIGK_F64;
@@ -795,8 +795,9 @@ int run_pairs_static(const TcPlan &t, int op, int kind, double param, const void
     const int64_t ncx = lx - 1, ncy = ly - 1;
     unsigned char *wsb = reinterpret_cast<unsigned char *>(ws);
     unsigned *err = reinterpret_cast<unsigned *>(wsb + t.err_off);
-    double *mat = reinterpret_cast<double *>(wsb + t.ct_off);
-    StaticIncFn fn = get_static_inc_kernel(kind, d);
+    void *mat = wsb + t.ct_off; // sized for float64 elements (float32 cells use half of it)
+    const bool f64cells = cell_prec(precision) == SIGK_PREC_FP64;
+    StaticIncFn fn = get_static_inc_kernel(kind, d, f64cells);
     if (!fn) return fail(SIGK_EUNSUPPORTED, "no static-kernel increment kernel for kind %d, dim %lld", kind,
                          (long long)d);
     cudaError_t e = cudaMemsetAsync(err, 0, sizeof(unsigned), stream);
@@ -831,8 +832,8 @@ int run_pairs_static(const TcPlan &t, int op, int kind, double param, const void
         count_launch();
         e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_fail(e, "static-kernel increment launch");
-        if ((st = consume_matrix(t, op, mat, true, sp.ld, err, i0, i1, nx, ny, ncx, ncy, d, order, out, out_ld, in64,
-                                 SIGK_PREC_FP64, dtype, wsb, stream)))
+        if ((st = consume_matrix(t, op, mat, f64cells, sp.ld, err, i0, i1, nx, ny, ncx, ncy, d, order, out, out_ld,
+                                 in64, precision, dtype, wsb, stream)))
             return st;
     }
     return SIGK_OK;
@@ -1485,9 +1486,6 @@ int sigk_gram_static(int op, int kind, double param, const void *x, const void *
     int st = check_common(dtype, precision, order);
     if (st) return st;
     if (!(param > 0.0) || !std::isfinite(param)) return fail(SIGK_EINVAL, "sigma must be finite and > 0");
-    if (precision != SIGK_PREC_FP64 && precision != SIGK_PREC_TC64)
-        return fail(SIGK_EUNSUPPORTED, "RBF / L1-RBF increments from points need float64 cells (SIGK_PREC_FP64 or "
-                                       "SIGK_PREC_TC64); use sigk_gram_inc for float32 cells");
     if (n_x < 1 || n_y < 1) return fail(SIGK_EINVAL, "path counts must be >= 1 (got %lld, %lld)", (long long)n_x,
                                         (long long)n_y);
     if (len_x < 2 || len_y < 2) return fail(SIGK_EINVAL, "path lengths must be >= 2 (got %lld, %lld)",
@@ -1506,7 +1504,7 @@ int sigk_gram_static(int op, int kind, double param, const void *x, const void *
                     workspace ? workspace_bytes : 0);
     if (((uintptr_t)workspace & 255) != 0) return fail(SIGK_EINVAL, "workspace must be 256-byte aligned");
     return run_pairs_static(t, kop, kind, param, x, y, n_x, n_y, len_x, len_y, dim, dtype, order, scale_x, scale_y,
-                            out, n_y, workspace, (cudaStream_t)stream);
+                            out, n_y, precision, workspace, (cudaStream_t)stream);
 }
 
 size_t sigk_backward_workspace_size(int op, int64_t n_x, int64_t n_y, int64_t len_x, int64_t len_y, int64_t dim,

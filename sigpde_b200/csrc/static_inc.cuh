@@ -47,7 +47,7 @@ struct StaticIncParams {
     const void *sx, *sy;  // per-path scales in the input dtype (x chunk-relative) or null
     int mode;             // kTcAll / kTcLower
     int64_t x0;           // kTcLower: global index of the first x path
-    double *out;
+    void *out;            // TO (double for float64 cells, float for float32 cells)
     int64_t ld;           // = npaths_x * rows_x
 };
 
@@ -124,9 +124,12 @@ __device__ __forceinline__ double static_k(const double (&xp)[DM], double xn, co
     return exp_nonpos(a);
 }
 
-template <int KIND, int DM>
+// TO: the matrix element type.  Every increment is formed in float64; float32
+// cells read it rounded once to float32 (the tensor-core modes' matrix type).
+template <int KIND, int DM, typename TO>
 __global__ void __launch_bounds__(kStWarps * 32) static_inc_kernel(StaticIncParams p)
 {
+    TO *const out = reinterpret_cast<TO *>(p.out);
     static_assert(DM % 2 == 0, "points are read as double2");
     __shared__ __align__(16) double ys[kStSlots][DM];
     __shared__ double yns[kStSlots];
@@ -186,12 +189,12 @@ __global__ void __launch_bounds__(kStWarps * 32) static_inc_kernel(StaticIncPara
         __syncthreads();
         if (pad) { // zero rows ncx .. rows_x - 1 of this path, every column of the tile
             for (int c = 0; c < nt; ++c)
-                for (int64_t r = 0; r < p.rows_x - ncx; ++r) p.out[(n0 + c) * p.ld + m + r] = 0.0;
+                for (int64_t r = 0; r < p.rows_x - ncx; ++r) out[(n0 + c) * p.ld + m + r] = TO(0);
         }
         // the tile's columns in runs within one y path: k(x, y_cj) of a column is k(x, y_cj+1) of the last
         int c = 0, s = 0;
         int cj = (int)(n0 - q0 * ncy);
-        double *o = p.out + n0 * p.ld + m;
+        TO *o = out + n0 * p.ld + m;
         while (c < nt) {
             const int run = (int)((nt - c) < (ncy - cj) ? (nt - c) : (ncy - cj));
             const double scl = sxf * ysc[c];
@@ -201,7 +204,7 @@ __global__ void __launch_bounds__(kStWarps * 32) static_inc_kernel(StaticIncPara
             for (int i = 1; i <= run; ++i) {
                 const double k_hi = static_k<KIND, DM>(xp, xn, ys[s + i], yns[s + i]);
                 const double k_hi_up = __shfl_down_sync(0xffffffffu, k_hi, 1);
-                if (row) *o = (((k_hi_up + k_lo) - k_lo_up) - k_hi) * scl;
+                if (row) *o = TO((((k_hi_up + k_lo) - k_lo_up) - k_hi) * scl);
                 o += p.ld;
                 k_lo = k_hi;
                 k_lo_up = k_hi_up;

@@ -456,11 +456,12 @@ class SigPDE:
         return result
 
     def _static_on_device(self, x):
-        """RBF / L1-RBF Grams with float64 cells and dim <= 32 evaluate the
-        static kernel from the points on the device (sigk_gram_static);
-        other cases build the increments with torch (the reference's route)."""
+        """RBF / L1-RBF Grams with dim <= 32 evaluate the static kernel from
+        the points on the device (sigk_gram_static; float64 increments for
+        float64 cells, rounded once to float32 for float32 cells); wider
+        paths build the increments with torch (the reference's route)."""
         return (getattr(self, "_device_static", True) and _static_kind(self.static_kernel) is not None
-                and self.precision in ("fp64", "tc64") and x.shape[2] <= 32)
+                and x.shape[2] <= 32)
 
     def _gram_static(self, op, x, y, sx, sy, result):
         kind, sigma = _static_kind(self.static_kernel)

@@ -135,9 +135,12 @@ def test_static_gram_argument_checks(built_lib):
     assert call(kind=7) == _lib.SIGK_EINVAL
     assert call(param=0.0) == _lib.SIGK_EINVAL
     assert call(param=float("nan")) == _lib.SIGK_EINVAL
-    assert call(prec=_lib.SIGK_PREC_FP32) == _lib.SIGK_EUNSUPPORTED
-    assert "float64 cells" in _lib.last_error()
-    assert call(prec=_lib.SIGK_PREC_TC32) == _lib.SIGK_EUNSUPPORTED
+    assert call(prec=9) == _lib.SIGK_EINVAL
+    # float32 cells are accepted (increments rounded once to float32): these calls get as far as
+    # the null path pointer
+    for prec in (_lib.SIGK_PREC_FP32, _lib.SIGK_PREC_TC32):
+        assert call(prec=prec) == _lib.SIGK_EINVAL
+        assert "x" in _lib.last_error()
     assert call(dim=33) == _lib.SIGK_EUNSUPPORTED
     assert "dim <= 32" in _lib.last_error()
     assert call(op=_lib.SIGK_OP_GRAM_SYM, y=1024) == _lib.SIGK_EINVAL

@@ -124,7 +124,7 @@ def test_static_chunks_and_tc64_are_bitwise_the_same(sig, oracle, monkeypatch):
 def test_static_matches_the_generic_route(sig, oracle):
     """The device-evaluated static Gram and the reference's route (torch static
     Gram and 4-term difference, then the increment solver) agree on float64
-    inputs; wide paths (d > 32) and float32 cells keep the reference's route."""
+    inputs; wide paths (d > 32) keep the reference's route."""
     from sigpde_b200.torch import kernel as kmod
     x = oracle.brownian(7, 30, 5, 61)
     y = oracle.brownian(6, 26, 5, 62)
@@ -154,3 +154,40 @@ def test_robust_gram_with_static_kernels(sig, oracle, kind):
     got = host(rk.gram(cuda(x), cuda(y)))
     want = oracle.gram(x, y, 1, lx, ly, static=kind, static_param=0.8)
     assert_rel(got, want, 1e-7, "robust gram")
+
+
+def _cs_err(got, want, kxx, kyy):
+    return np.abs(got - want) / np.sqrt(np.abs(kxx * kyy))
+
+
+@pytest.mark.parametrize("prec", ["fp32", "tc32"])
+@pytest.mark.parametrize("kind", ["rbf", "l1rbf"])
+@pytest.mark.parametrize("shape", [(9, 8, 40, 37, 8, 2), (5, 4, 9, 11, 3, 1), (3, 3, 70, 66, 5, 3), (7, 6, 33, 40, 17, 1)])
+def test_static_gram_float32_cells(sig, oracle, prec, kind, shape):
+    """Float32 cells (precision fp32 / tc32) read the device-evaluated increments
+    rounded once to float32.  Tolerance as for the linear kernel's float32 cells:
+    error normalised by sqrt(k(x,x) k(y,y)) at most 4x that of the reference's
+    own numerics on the same inputs (float64 arithmetic, float32 storage of
+    every cell: the oracle with store_f32=True), plus 1e-7."""
+    nx, ny, lx, ly, d, o = shape
+    x = oracle.brownian(nx, lx, d, 500 + lx)
+    y = oracle.brownian(ny, ly, d, 600 + ly)
+    sigma = 0.9
+    k = sig.SigPDE(static_kernel(sig, kind, sigma), o, precision=prec)
+    X, Y = cuda(x, torch.float32), cuda(y, torch.float32)
+    assert k._static_on_device(X)
+    xin, yin = host(X), host(Y)
+    got = host(k.gram(X, Y))
+    want = oracle.gram(xin, yin, o, static=kind, static_param=sigma)
+    ref = oracle.gram(xin, yin, o, static=kind, static_param=sigma, store_f32=True)
+    kxx = oracle.pairwise(xin, None, o, static=kind, static_param=sigma)[:, None]
+    kyy = oracle.pairwise(yin, None, o, static=kind, static_param=sigma)[None, :]
+    tol = 4.0 * float(_cs_err(ref, want, kxx, kyy).max()) + 1e-7
+    err = float(_cs_err(got, want, kxx, kyy).max())
+    assert err <= tol, f"{prec} {kind} {shape}: CS-normalised error {err:.3e} > {tol:.3e}"
+    G = host(k.gram(X))
+    assert np.array_equal(G, G.T)
+    wsym = oracle.gram(xin, None, o, static=kind, static_param=sigma)
+    rsym = oracle.gram(xin, None, o, static=kind, static_param=sigma, store_f32=True)
+    tol = 4.0 * float(_cs_err(rsym, wsym, kxx, kxx.T).max()) + 1e-7
+    assert float(_cs_err(G, wsym, kxx, kxx.T).max()) <= tol
