@@ -73,6 +73,8 @@ def parse():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "tc32", "tc64"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target length of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's Numba GPU path beside the default Gram")
     ap.add_argument("--autotune", action="store_true", help="uneven batches: measure rows per lane per bucket "
                     "before timing (sigpde_b200.torch.autotune)")
     ap.add_argument("--burst", action="store_true", help="serving traces: every request arrives at t=0 "
@@ -98,6 +100,15 @@ def workload_name(w):
     return f"SigPDE.gram {w['nx']}x{w['ny']}, L={w['L']}, d={w['d']}, dyadic_order={w['order']}, {kern}"
 
 
+def gram_config(w, world, precision):
+    """The `config` of a Gram workload's bench line, shared by every arm so that
+    the GPU line and the reference line describe the same workload."""
+    entries, _, _ = workload_units(w)
+    return {"workload": workload_name(w), "global_batch": entries * world, "seq_len": w["L"],
+            "parallelism": f"replicas x{world}", "precision": precision,
+            "l2": "GPU arm: flushed between timed steps (256 MB write); CPU arm: host memory"}
+
+
 def static_kernel_of(kernels, w):
     st = w.get("static", "linear")
     if st == "rbf":
@@ -116,28 +127,85 @@ def make_inputs(w, device=None, dtype=None):
 
 # ----------------------------------------------------------------------------- clocks
 class ClockSampler:
-    """nvidia-smi sampled every 200 ms during the timed region."""
+    """SM clock, power and clock-event reasons sampled during the timed region.
+
+    NVML is polled from a thread every `period_s` (20 ms: a config-2 run of 20
+    steps lasts ~0.1 s, which a 200 ms nvidia-smi loop sees once).  Reading NVML
+    changes no GPU setting.  Without NVML the sampler falls back to nvidia-smi.
+    """
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASON_BITS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+                   ("sw_power_cap", 0x4))
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, period_s=0.02):
         self.gpu_index = gpu_index
+        self.period_s = period_s
         self.proc = None
         self.path = None
+        self.thread = None
+        self.rows = []
+        self.stop_evt = threading.Event()
+        self.nvml = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        idx = self.gpu_index
+        try:  # CUDA_VISIBLE_DEVICES may renumber devices; torch knows the NVML index
+            idx = torch.cuda._get_nvml_device_index(self.gpu_index)
+        except Exception:
+            pass
+        return pynvml, pynvml.nvmlDeviceGetHandleByIndex(idx)
+
+    def _poll(self):
+        nv, h = self.nvml
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self.stop_evt.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                self.rows.append((sm, mx, pw, reasons))
+            except Exception:
+                pass
+            self.stop_evt.wait(self.period_s)
 
     def start(self):
+        try:
+            self.nvml = self._nvml_handle()
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.nvml = None
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu_index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                 "-lms", "50"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
 
     def stop(self):
+        if self.thread is not None:
+            self.stop_evt.set()
+            self.thread.join(timeout=5)
+            rows = self.rows
+            if not rows:
+                return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "source": "nvml"}
+            reasons = set()
+            for r in rows:
+                for name, bit in self.REASON_BITS:
+                    if r[3] & bit:
+                        reasons.add(name)
+            return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                    "reasons": sorted(reasons), "samples": len(rows), "power_w_max": max(r[2] for r in rows),
+                    "source": f"nvml every {int(self.period_s * 1000)} ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -169,7 +237,7 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(rows)}
+                "reasons": sorted(reasons), "samples": len(rows), "source": "nvidia-smi every 50 ms"}
 
 
 # ----------------------------------------------------------------------------- timing
@@ -323,8 +391,7 @@ def run_reference(args, w, rank):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic Brownian paths (seeded), float32 inputs upcast to float64",
-        "config": {"workload": workload_name(w), "global_batch": entries, "seq_len": w["L"], "parallelism": "cpu",
-                   "l2": "n/a (CPU)"},
+        "config": gram_config(w, args.gpus, "fp64"),
         "cells_per_s": value * cells / entries,
         "cpu_baseline": {"value": value, "unit": "entries/s", "cores": cores, "kind": "port",
                          "sample": f"per step: {sample}; float64 C restatement of the reference solver"},
@@ -439,9 +506,7 @@ def run_ours(args, w):
             "vs_baseline": None,
             "dtype": "f64" if fp64 else "f32",
             "data": "synthetic Brownian paths (seeded PCG64), float32",
-            "config": {"workload": "SigPDE.gram 256x256, L=128, d=8, dyadic_order=2, LinearKernel",
-                       "global_batch": entries * world, "seq_len": w["L"], "parallelism": f"replicas x{world}",
-                       "precision": args.precision, "l2": "flushed between timed steps (256 MB write)"},
+            "config": gram_config(w, world, args.precision),
             "cells_per_s": value * cells / entries,
             "accuracy": acc,
             "roofline": {"bound": "fp64" if fp64 else "fp32", "achieved": achieved, "peak": peak,
@@ -459,6 +524,18 @@ def run_ours(args, w):
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu
+        if world == 1 and not args.no_reference_gpu:
+            # the reference's own Numba GPU path on the same inputs, timed after (outside) our timed region
+            r = measure_reference_gpu(w, steps=3, warmup=2, accuracy=False)
+            if "unavailable" in r:
+                line["reference_numba_gpu"] = r
+            else:
+                line["reference_numba_gpu"] = {
+                    "ms_per_step": r["ms_per_step"], "entries_per_s": r["value"], "steps": 3, "warmup": 2,
+                    "speedup": value / r["value"],
+                    "note": "unmodified stojl/SigPDE from baseline/_ref through sigpde.torch.SigPDE.gram on this "
+                            "GPU, host-timed between synchronisations (the reference synchronises inside each "
+                            "call), measured after this line's timed region"}
     if world > 1:
         barrier()
         dist.destroy_process_group()
@@ -635,43 +712,40 @@ def run_ours_grad(args, w):
     print(json.dumps(line), flush=True)
 
 
-def run_reference_gpu(args, w):
-    """The reference's own GPU path: stojl/SigPDE installed unmodified under
+def measure_reference_gpu(w, steps, warmup, accuracy=True):
+    """Time the reference's own GPU path: stojl/SigPDE installed unmodified under
     baseline/_ref, called through its public API (sigpde.torch.SigPDE.gram with
     the default max_batch / max_threads) on the same float32 inputs.  The
     reference synchronises the device inside every call, so each call is timed
-    on the host between two synchronisations; the L2 is flushed between calls."""
+    on the host between two synchronisations; the L2 is flushed between calls.
+    Returns the fields of a bench line, or {"unavailable": why}."""
     import numpy as np
     import torch
 
     ref_dir = os.path.join(ROOT, "baseline", "_ref")
     entries, cells, _ = workload_units(w)
-    base = {"impl": "reference-gpu", "metric": "gram_entries_per_s", "unit": "entries/s"}
     if not os.path.isdir(os.path.join(ref_dir, "sigpde")):
-        print(json.dumps(dict(base, unavailable="reference not installed under baseline/_ref")), flush=True)
-        return
-    sys.path.insert(0, ref_dir)
+        return {"unavailable": "reference not installed under baseline/_ref"}
+    if ref_dir not in sys.path:
+        sys.path.insert(0, ref_dir)
     try:
         import warnings
         warnings.filterwarnings("ignore")
         import sigpde.torch as refsig
     except Exception as e:  # numba or its CUDA target missing
-        print(json.dumps(dict(base, unavailable=f"import failed: {type(e).__name__}: {e}"[:300])), flush=True)
-        return
-    dev = torch.device("cuda", 0)
+        return {"unavailable": f"import failed: {type(e).__name__}: {e}"[:300]}
+    dev = torch.device("cuda", torch.cuda.current_device())
     X, Y = make_inputs(w, device=dev)
     k = refsig.SigPDE(static_kernel_of(refsig.kernels, w), w["order"])
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
     try:
         out = k.gram(X, Y)
     except Exception as e:
-        print(json.dumps(dict(base, unavailable=f"reference call failed: {type(e).__name__}: {e}"[:300])),
-              flush=True)
-        return
-    for _ in range(max(0, args.warmup - 1)):
+        return {"unavailable": f"reference call failed: {type(e).__name__}: {e}"[:300]}
+    for _ in range(max(0, warmup - 1)):
         k.gram(X, Y)
     times = []
-    for _ in range(args.steps):
+    for _ in range(steps):
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -680,7 +754,7 @@ def run_reference_gpu(args, w):
         times.append((time.perf_counter() - t0) * 1e3)
     ms = statistics.mean(times)
     acc = None
-    if not args.no_cpu_baseline:
+    if accuracy:
         from oracle import oracle
         G = out.double().cpu().numpy()
         rng = np.random.default_rng(1)
@@ -694,15 +768,24 @@ def run_reference_gpu(args, w):
         acc = {"max_rel_err": float(np.max(np.abs(got - want) / np.abs(want))),
                "max_cs_err": float(np.max(np.abs(got - want) / np.sqrt(kxx * kyy))),
                "sample": "64 random entries vs the float64 oracle"}
-    line = dict(base, value=entries / (ms * 1e-3), n_gpus=1, steps=args.steps, warmup=args.warmup,
-                ms_per_step=ms, p50_ms=percentile(times, 0.5), p99_ms=percentile(times, 0.99),
-                higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32 storage / f64 arithmetic",
-                data="synthetic Brownian paths (seeded PCG64), float32",
-                config={"workload": workload_name(w), "global_batch": entries, "seq_len": w["L"],
-                        "parallelism": "single GPU", "l2": "flushed between timed calls (256 MB write)"},
-                cells_per_s=cells / (ms * 1e-3), accuracy=acc,
+    return dict(value=entries / (ms * 1e-3), steps=steps, warmup=warmup, ms_per_step=ms,
+                p50_ms=percentile(times, 0.5), p99_ms=percentile(times, 0.99), cells_per_s=cells / (ms * 1e-3),
+                accuracy=acc)
+
+
+def run_reference_gpu(args, w):
+    """The reference's Numba GPU path as its own bench line (--impl reference-gpu)."""
+    entries, _, _ = workload_units(w)
+    base = {"impl": "reference-gpu", "metric": "gram_entries_per_s", "unit": "entries/s"}
+    r = measure_reference_gpu(w, args.steps, args.warmup, accuracy=not args.no_cpu_baseline)
+    if "unavailable" in r:
+        print(json.dumps(dict(base, **r)), flush=True)
+        return
+    line = dict(base, n_gpus=1, higher_is_better=True, scaling="weak", vs_baseline=None,
+                dtype="f32 storage / f64 arithmetic", data="synthetic Brownian paths (seeded PCG64), float32",
+                config=gram_config(w, 1, "reference (float64 arithmetic, float32 storage)"),
                 note="unmodified stojl/SigPDE (Numba CUDA) through sigpde.torch.SigPDE.gram, host-timed "
-                     "(the reference synchronises inside each call)")
+                     "(the reference synchronises inside each call)", **r)
     print(json.dumps(line), flush=True)
 
 

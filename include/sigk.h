@@ -110,7 +110,7 @@ SIGK_API size_t sigk_workspace_size(int op, int64_t n_x, int64_t n_y, int64_t le
  * Pairwise signature kernel with the linear static kernel.
  * Replaces SigPDE.pairwise's increment build + PairwisePDESolver.solve /
  * solve_scaled (sigpde/torch/kernel.py:31-65, sigpde/torch/kernel.py:13-16,
- * sigpde/PDESolvers.py:56-84, sigpde/cuda_pairwise_kernels.py:8-97).
+ * sigpde/PDESolvers.py:56-84, sigpde/cuda_pairwise_kernels.py:8-85).
  *   x: (batch, len_x, dim), y: (batch, len_y, dim); out: (batch,)
  *   static_scale: LinearKernel(scale) factor (sigpde/torch/static_kernels.py:4-8)
  *   scale_x / scale_y: (batch,) per-pair path scales or NULL (NULL = 1)
@@ -224,7 +224,7 @@ SIGK_API int sigk_self_norms(const void *x, int64_t n, int64_t len, int64_t dim,
  * where k(x,x) < 1.
  * Replaces RobustSigPDE._norm_factors + PairwisePDESolver.solve_norms
  * (sigpde/torch/kernel.py:180-195, sigpde/PDESolvers.py:86-101,
- * sigpde/cuda_pairwise_kernels.py:100-178).
+ * sigpde/cuda_pairwise_kernels.py:88-165).
  *   fnorm == NULL: the default normaliser f(s) = 2 - 1/(1 + log s)
  *                  (sigpde/torch/kernel.py:23-24) is applied on the device and
  *                  knorm receives k(x,x) (if knorm != NULL).
@@ -265,7 +265,7 @@ SIGK_API int sigk_gram_inc(const void *inc, int64_t n_x, int64_t n_y, int64_t nc
 
 /*
  * sigk_normalize_inc replaces PairwisePDESolver.solve_norms
- * (sigpde/PDESolvers.py:86-101, sigpde/cuda_pairwise_kernels.py:100-178) for
+ * (sigpde/PDESolvers.py:86-101, sigpde/cuda_pairwise_kernels.py:88-165) for
  * precomputed self-increments inc: (n, nc, nc) with strides (s0, s1, s2).
  * knorm and fnorm are float64 inputs (k(x,x) and f(k(x,x))).
  */

@@ -162,7 +162,7 @@ def solve_increments(incs, order: int, sx=None, sy=None, store_f32: bool = False
 def py_solve(inc, order: int, scale: float = 1.0) -> float:
     """Pure-Python restatement of the anti-diagonal loop, for tiny cases only.
 
-    Walks anti-diagonals p = 2..N-1 exactly as sigpde/cuda_pairwise_kernels.py:29-51,
+    Walks anti-diagonals p = 2..N-1 exactly as sigpde/cuda_pairwise_kernels.py:17-39,
     with a full (lx, ly) grid instead of the 3-slot rotation.
     """
     inc = _f64(inc)

@@ -11,12 +11,12 @@
  *       (rows i in [1,lx-1], columns j in [1,ly-1], coarse increment at
  *        ((i-1)>>order, (j-1)>>order), boundary K = 1 on row 0 / column 0,
  *        result = K[lx-1][ly-1])
- *   - the scaled variant           sigpde/cuda_pairwise_kernels.py:53-97
+ *   - the scaled variant           sigpde/cuda_pairwise_kernels.py:41-85
  *       (inc * scale_x * scale_y)
  *   - the LinearKernel increments  sigpde/torch/kernel.py:13-21 with
  *                                  sigpde/torch/static_kernels.py:3-11
  *       (4-term second difference of the static Gram, divided by 4^order)
- *   - the Chandrupatla lambda loop sigpde/cuda_pairwise_kernels.py:100-178
+ *   - the Chandrupatla lambda loop sigpde/cuda_pairwise_kernels.py:88-165
  *       with the argument order of sigpde/torch/kernel.py:180-195
  *   - the gradient of a solve with respect to its increments (the adjoint of
  *     the scheme; the reference has none): sko_grad_solve, checked against
@@ -55,7 +55,7 @@ static inline double store(double v, int store_f32) { return store_f32 ? (double
  * inc: (ncx, ncy) row-major coarse increments (already divided by 4^order).
  * Row-by-row order gives the same values as the reference's anti-diagonal
  * order: every cell reads the same three neighbours either way.
- * Follows sigpde/cuda_pairwise_kernels.py:17-39 (scale == 1) and :53-97.
+ * Follows sigpde/cuda_pairwise_kernels.py:17-39 (scale == 1) and :41-85.
  */
 double sko_solve(const double *inc, int64_t ncx, int64_t ncy, int order, double scale, int store_f32,
                  double *row_buf /* 2*(ly) doubles or NULL */)
@@ -114,7 +114,7 @@ void sko_increments_linear(const double *x, const double *y, int64_t Lx, int64_t
 /*
  * Batched solve over precomputed increments.
  * incs: (npairs, ncx, ncy); sx, sy: per-pair scales or NULL (scaled kernels
- * multiply inc by scale_x * scale_y, cuda_pairwise_kernels.py:73,81).
+ * multiply inc by scale_x * scale_y, cuda_pairwise_kernels.py:61,69).
  */
 void sko_solve_batch(const double *incs, int64_t npairs, int64_t ncx, int64_t ncy, int order, const double *sx,
                      const double *sy, int store_f32, double *out)
@@ -189,7 +189,7 @@ void sko_gram_linear(const double *x, const double *y, int64_t Nx, int64_t Ny, i
 
 /*
  * Chandrupatla root-find for the robust normalisation of one path.
- * Restates sigpde/cuda_pairwise_kernels.py:100-178 as called from
+ * Restates sigpde/cuda_pairwise_kernels.py:88-165 as called from
  * sigpde/torch/kernel.py:180-195:
  *   the kernel parameter `norms` receives fk = f(k(x,x)) and `f_norms`
  *   receives k = k(x,x), so the bracket is lambda in [0,1] for

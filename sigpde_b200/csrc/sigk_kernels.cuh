@@ -174,7 +174,7 @@ struct NormParams {
 };
 
 // k(x,x), f(k) and the Chandrupatla iteration for one path, given solve(s) =
-// k at increments scaled by s: sigpde/cuda_pairwise_kernels.py:100-178 with
+// k at increments scaled by s: sigpde/cuda_pairwise_kernels.py:88-165 with
 // the argument order of sigpde/torch/kernel.py:186-193: g(l) = k(l x) - f(k),
 // g(0) = 1 - f(k), g(1) = k - f(k).  All bracket state is float64 and uniform
 // across the threads that call it (solve returns the same value to all of

@@ -231,7 +231,7 @@ def _generic_differentiable(solver, op, x, y, x_scale, y_scale, max_batch):
         parts = []
         for s0, s1 in _batches(B, max_batch):
             inc = pairwise_inner_product(x[s0:s1], yv[s0:s1], solver.static_kernel, solver.dyadic_order).to(x.dtype)
-            if scaled:  # in torch, so that autograd reaches the scales (sigpde/cuda_pairwise_kernels.py:73,81)
+            if scaled:  # in torch, so that autograd reaches the scales (sigpde/cuda_pairwise_kernels.py:61,69)
                 inc = inc * (sx[s0:s1] * sy[s0:s1])[:, None, None]
             parts.append(_IncSolve.apply(inc, None, None, solver))
         return torch.cat(parts)

@@ -5,7 +5,7 @@ tests or fixtures of its own.  It runs unmodified under Numba's CUDA simulator
 (NUMBA_ENABLE_CUDASIM=1) once four harness-side shims are installed:
 
   (i)   numba.cuda.jit drops the ``max_registers`` keyword, which the simulator
-        rejects (sigpde/cuda_pairwise_kernels.py:100);
+        rejects (sigpde/cuda_pairwise_kernels.py:88);
   (ii)  CPU torch tensors expose ``__cuda_array_interface__`` (read by
         sigpde/utils.py:15-16 and the solve methods of sigpde/PDESolvers.py);
   (iii) ``numba.cuda.as_cuda_array`` (absent from the simulator) maps a tensor to
@@ -20,7 +20,7 @@ hand; the tests read the committed file and never need the reference.
 
 The robust (Chandrupatla) kernel raises ZeroDivisionError under the simulator
 once its bracket collapses (Python float division at
-sigpde/cuda_pairwise_kernels.py:169); cases where that happens are recorded as
+sigpde/cuda_pairwise_kernels.py:157); cases where that happens are recorded as
 skipped and the float64 oracle restatement is pinned on the remaining cases.
 """
 from __future__ import annotations
@@ -71,8 +71,8 @@ def install_shims():
     # shim (iv): deterministic barrier scheduling.  The simulator releases all
     # threads of a block at once after each syncthreads and lets the GIL pick
     # the order.  The reference's lambda kernel reads sol_1[b,0,0] right after
-    # its last barrier (sigpde/cuda_pairwise_kernels.py:144) and thread 0 may
-    # overwrite that slot at the first diagonal of the next iteration (:128-132)
+    # its last barrier (sigpde/cuda_pairwise_kernels.py:132) and thread 0 may
+    # overwrite that slot at the first diagonal of the next iteration (:116-123)
     # with no barrier in between, so free-running Python threads make the
     # scalar bracket state diverge between threads.  Here the threads of a
     # block run one at a time between barriers, highest thread id first: a
