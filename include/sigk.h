@@ -96,6 +96,19 @@ SIGK_API const char *sigk_last_error_string(void);
 SIGK_API uint64_t sigk_launch_count(void);
 
 /*
+ * Bound of the uneven-batch kernels' band waits (a band of a pair waits for
+ * the band above it to publish its bottom row, sigk_pairwise_ragged*): a
+ * wait gives up after `polls` polls of ~64 ns each, sets the timeout bit of
+ * the launch's error word and the pair's result becomes NaN; the kernel
+ * still returns.  polls < 0 restores the default (2^26 polls, ~4 s); 0 gives
+ * up at the first poll that finds nothing published.  Applies to launches
+ * enqueued afterwards, from every thread; returns the previous setting (-1 for
+ * the default).  It has no counterpart in the reference, whose kernels have
+ * no waits; it exists so that the timeout path can be exercised on purpose.
+ */
+SIGK_API int64_t sigk_set_wait_limit(int64_t polls);
+
+/*
  * Bytes of caller-provided scratch an entry point needs for the given shape.
  * `op` is a sigk_op; len_x / len_y are path lengths before refinement; for
  * SIGK_OP_PAIRWISE n_x is the batch, for the Gram ops n_x / n_y are the path
@@ -361,6 +374,17 @@ SIGK_API int sigk_pairwise_ragged_tc(const void *x_pack, const int64_t *x_off, c
                                      sigk_stream_t stream);
 
 /*
+ * Outcome of the last uneven-batch launch that used `workspace`: synchronises
+ * `stream`, then reads the launch's error word.  SIGK_ETIMEDOUT: a band wait
+ * ran out (see sigk_set_wait_limit) or the increment GEMM gave up a wait;
+ * SIGK_EINVAL: an item broke the plan rules; either way those pairs are NaN
+ * and the others are exact.  The device and the library stay usable.
+ * The reference reports failures as NaN -> inf in its results only
+ * (sigpde/torch/kernel.py:183, sigpde/cuda_pairwise_kernels.py:132).
+ */
+SIGK_API int sigk_ragged_status(const void *workspace, sigk_stream_t stream);
+
+/*
  * sigk_gram_noalloc -- sigk_gram for callers that cannot allocate device
  * memory.  It has no counterpart in the reference.
  *
@@ -374,7 +398,10 @@ SIGK_API int sigk_pairwise_ragged_tc(const void *x_pack, const int64_t *x_off, c
  *
  * The first call on a device looks up the array's device address (with that
  * device current) and caches it; make that first call before any stream
- * capture.  Every call shares the one array and leaves its contents behind;
+ * capture.  The cached address belongs to the device's primary context: after
+ * cudaDeviceReset the array is loaded again, possibly elsewhere, and this entry
+ * point must not be called again in that process.
+ * Every call shares the one array and leaves its contents behind;
  * each call overwrites the part it reads before reading it.  Calls that
  * overlap on the GPU (two streams, or two host threads, on one device) race on
  * the array: serialise them.

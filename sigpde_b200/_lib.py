@@ -56,6 +56,7 @@ SIGNATURES = {
     "sigk_version": (ctypes.c_char_p, []),
     "sigk_last_error_string": (ctypes.c_char_p, []),
     "sigk_launch_count": (ctypes.c_uint64, []),
+    "sigk_set_wait_limit": (_i64, [_i64]),
     "sigk_workspace_size": (_sz, [_int, _i64, _i64, _i64, _i64, _i64, _int, _int, _int]),
     "sigk_pairwise": (_int, [_vp, _vp, _i64, _i64, _i64, _i64, _int, _int, _dbl, _vp, _vp, _vp, _int, _vp, _sz,
                              _vp]),
@@ -86,6 +87,7 @@ SIGNATURES = {
     "sigk_ragged_tc_workspace_size": (_sz, [_i64, _i64, _i64, _i64, _int, _plan_p]),
     "sigk_pairwise_ragged_tc": (_int, [_vp, _vp, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _vp,
                                        _i64, _i64, _i64, _int, _dbl, _vp, _vp, _vp, _int, _plan_p, _vp, _sz, _vp]),
+    "sigk_ragged_status": (_int, [_vp, _vp]),
     "sigk_gram_noalloc": (_int, [_vp, _vp, _i64, _i64, _i64, _i64, _i64, _int, _int, _dbl, _vp, _vp, _vp, _int, _vp]),
 }
 
@@ -139,3 +141,9 @@ def version() -> str:
 def launch_count() -> int:
     """Kernels enqueued by libsigk.so since it was loaded (all threads)."""
     return int(lib().sigk_launch_count())
+
+
+def set_wait_limit(polls: int) -> int:
+    """Polls an uneven-batch band wait makes before it gives up (< 0: the default,
+    ~4 s); returns the previous setting.  See sigk_set_wait_limit in sigk.h."""
+    return int(lib().sigk_set_wait_limit(int(polls)))

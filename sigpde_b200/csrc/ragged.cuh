@@ -86,9 +86,14 @@ struct RaggedParams {
     const int64_t *inc_off;
     int64_t inc_elems;
     const unsigned *tc_err;     // non-zero: the GEMM skipped a tile, the matrix is incomplete
+    long long poll_limit;       // polls of a band wait before it gives up (kProgressPollLimit by default)
 };
 
 constexpr long long kProgressPollLimit = 1ll << 26; // ~4 s with 64 ns sleeps
+// Bits of a launch's error word: an item broke the plan rules (or its increments are missing), and a band
+// wait ran out.  Either way the affected pair's result is NaN.
+constexpr int kErrInvalidItem = 1;
+constexpr int kErrWaitTimeout = 2;
 constexpr int kProgressStride = 16;                 // column blocks between publications
 
 __device__ __forceinline__ int ld_acquire(const int *p)
@@ -103,12 +108,13 @@ __device__ __forceinline__ void st_release(int *p, int v)
     asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Spin (with a bounded number of polls) until *prog >= need; returns the value seen, or -1 on timeout.
-__device__ __forceinline__ int wait_progress(const int *prog, int need)
+// Spin (with at most `limit` polls after the first read) until *prog >= need; returns the value seen, or
+// -1 on timeout.
+__device__ __forceinline__ int wait_progress(const int *prog, int need, long long limit)
 {
     int v = ld_acquire(prog);
     for (long long i = 0; v < need; ++i) {
-        if (i >= kProgressPollLimit) return -1;
+        if (i >= limit) return -1;
         __nanosleep(64);
         v = ld_acquire(prog);
     }
@@ -124,7 +130,8 @@ __device__ __forceinline__ int wait_progress(const int *prog, int need)
 // pub_stride: column blocks between publications of the band's progress.
 template <typename T, int R, int O, class Src>
 __device__ T band_solve(const SolveGeom &g, Src &src, int band, bool last, const T *top_buf, const int *top_prog,
-                        T *bot_buf, int *bot_prog, int *error, int prog_base = 0, int pub_stride = kProgressStride)
+                        T *bot_buf, int *bot_prog, int *error, int prog_base = 0, int pub_stride = kProgressStride,
+                        long long poll_limit = kProgressPollLimit)
 {
     using BS = BlockShape<R, O>;
     constexpr int C = BS::C;
@@ -157,11 +164,11 @@ __device__ T band_solve(const SolveGeom &g, Src &src, int band, bool last, const
                 for (int c = 0; c < C; ++c) top[c] = T(1);
             } else if (active) {
                 if (!poisoned && seen <= q) {
-                    const int v0 = wait_progress(top_prog, prog_base + (int)q + 1);
+                    const int v0 = wait_progress(top_prog, prog_base + (int)q + 1, poll_limit);
                     const int v = (v0 < 0 || v0 == 0x7fffffff) ? v0 : v0 - prog_base;
                     if (v < 0 || v == 0x7fffffff) { // ran out, or the band above was refused
                         poisoned = true;
-                        if (v < 0) *error = 1;
+                        if (v < 0) atomicOr(error, kErrWaitTimeout);
                     } else {
                         seen = v;
                     }
@@ -228,7 +235,8 @@ struct BandSource {
 
 template <typename T, int R, int O, bool MAT, typename TM>
 __device__ T ragged_band(const BandSource &bs, int64_t ncx, int64_t ncy, int order, T *stage, int stage_cap, int band,
-                         bool last, const T *top_buf, const int *top_prog, T *bot_buf, int *bot_prog, int *error)
+                         bool last, const T *top_buf, const int *top_prog, T *bot_buf, int *bot_prog, int *error,
+                         long long poll_limit)
 {
     using BS = BlockShape<R, O>;
     const SolveGeom g = make_geom<R, O>(ncx, ncy, order);
@@ -237,7 +245,8 @@ __device__ T ragged_band(const BandSource &bs, int64_t ncx, int64_t ncy, int ord
         src.base = reinterpret_cast<const TM *>(bs.mat);
         src.ld = bs.ld;
         src.ncy = ncy;
-        return band_solve<T, R, O>(g, src, band, last, top_buf, top_prog, bot_buf, bot_prog, error);
+        return band_solve<T, R, O>(g, src, band, last, top_buf, top_prog, bot_buf, bot_prog, error, 0,
+                                   kProgressStride, poll_limit);
     } else {
         DeltaIncs<T, BS::RC> src;
         src.dX = reinterpret_cast<const T *>(bs.dX);
@@ -245,21 +254,23 @@ __device__ T ragged_band(const BandSource &bs, int64_t ncx, int64_t ncy, int ord
         src.d = bs.d;
         src.ncy = ncy;
         src.dxs = ((int64_t)BS::RC * bs.d * 32 <= stage_cap) ? stage : nullptr;
-        return band_solve<T, R, O>(g, src, band, last, top_buf, top_prog, bot_buf, bot_prog, error);
+        return band_solve<T, R, O>(g, src, band, last, top_buf, top_prog, bot_buf, bot_prog, error, 0,
+                                   kProgressStride, poll_limit);
     }
 }
 
 template <typename T, int R, bool MAT, typename TM>
 __device__ T ragged_band_by_o(const BandSource &bs, int64_t ncx, int64_t ncy, int order, T *stage, int stage_cap,
-                              int band, bool last, const T *tb, const int *tp, T *bb, int *bp, int *error)
+                              int band, bool last, const T *tb, const int *tp, T *bb, int *bp, int *error,
+                              long long pl)
 {
     switch (order) {
-    case 0: return ragged_band<T, R, 0, MAT, TM>(bs, ncx, ncy, order, stage, stage_cap, band, last, tb, tp, bb, bp, error);
-    case 1: return ragged_band<T, R, 1, MAT, TM>(bs, ncx, ncy, order, stage, stage_cap, band, last, tb, tp, bb, bp, error);
-    case 2: return ragged_band<T, R, 2, MAT, TM>(bs, ncx, ncy, order, stage, stage_cap, band, last, tb, tp, bb, bp, error);
-    case 3: return ragged_band<T, R, 3, MAT, TM>(bs, ncx, ncy, order, stage, stage_cap, band, last, tb, tp, bb, bp, error);
+    case 0: return ragged_band<T, R, 0, MAT, TM>(bs, ncx, ncy, order, stage, stage_cap, band, last, tb, tp, bb, bp, error, pl);
+    case 1: return ragged_band<T, R, 1, MAT, TM>(bs, ncx, ncy, order, stage, stage_cap, band, last, tb, tp, bb, bp, error, pl);
+    case 2: return ragged_band<T, R, 2, MAT, TM>(bs, ncx, ncy, order, stage, stage_cap, band, last, tb, tp, bb, bp, error, pl);
+    case 3: return ragged_band<T, R, 3, MAT, TM>(bs, ncx, ncy, order, stage, stage_cap, band, last, tb, tp, bb, bp, error, pl);
     default:
-        return ragged_band<T, R, 4, MAT, TM>(bs, ncx, ncy, order, stage, stage_cap, band, last, tb, tp, bb, bp, error);
+        return ragged_band<T, R, 4, MAT, TM>(bs, ncx, ncy, order, stage, stage_cap, band, last, tb, tp, bb, bp, error, pl);
     }
 }
 
@@ -287,7 +298,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) ragged_kernel(RaggedParam
         const int band = p.item_band[it];
         if (b < 0 || b >= p.npairs) { // cannot even name a pair: release any consumer and skip
             if (lane == 0) {
-                *p.error = 1;
+                atomicOr(p.error, kErrInvalidItem);
                 st_release(p.progress + it, 0x7fffffff);
             }
             continue;
@@ -325,7 +336,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) ragged_kernel(RaggedParam
         }
         if (!ok) {
             if (lane == 0) {
-                *p.error = 1;
+                atomicOr(p.error, (MAT && *p.tc_err) ? kErrWaitTimeout : kErrInvalidItem);
                 out[b] = nan;
                 st_release(p.progress + it, 0x7fffffff); // the band below sees the sentinel and yields NaN
             }
@@ -346,10 +357,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) ragged_kernel(RaggedParam
         const int cap = p.stage_elems_per_warp;
         T v;
         switch (R) {
-        case 2: v = ragged_band_by_o<T, 2, MAT, TM>(bs, ncx, ncy, order, stage, cap, band, last, tb, tp, bb, bp, p.error); break;
-        case 4: v = ragged_band_by_o<T, 4, MAT, TM>(bs, ncx, ncy, order, stage, cap, band, last, tb, tp, bb, bp, p.error); break;
-        case 8: v = ragged_band_by_o<T, 8, MAT, TM>(bs, ncx, ncy, order, stage, cap, band, last, tb, tp, bb, bp, p.error); break;
-        default: v = ragged_band_by_o<T, 16, MAT, TM>(bs, ncx, ncy, order, stage, cap, band, last, tb, tp, bb, bp, p.error); break;
+        case 2: v = ragged_band_by_o<T, 2, MAT, TM>(bs, ncx, ncy, order, stage, cap, band, last, tb, tp, bb, bp, p.error, p.poll_limit); break;
+        case 4: v = ragged_band_by_o<T, 4, MAT, TM>(bs, ncx, ncy, order, stage, cap, band, last, tb, tp, bb, bp, p.error, p.poll_limit); break;
+        case 8: v = ragged_band_by_o<T, 8, MAT, TM>(bs, ncx, ncy, order, stage, cap, band, last, tb, tp, bb, bp, p.error, p.poll_limit); break;
+        default: v = ragged_band_by_o<T, 16, MAT, TM>(bs, ncx, ncy, order, stage, cap, band, last, tb, tp, bb, bp, p.error, p.poll_limit); break;
         }
         if (last && lane == 0) out[b] = TIN(v);
     }

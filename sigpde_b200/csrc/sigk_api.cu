@@ -86,6 +86,13 @@ size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 // Kernels enqueued by this library since load (sigk_launch_count).
 std::atomic<uint64_t> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+// Polls of a ragged band wait before it gives up (sigk_set_wait_limit; < 0: kProgressPollLimit).
+std::atomic<long long> g_wait_limit{-1};
+long long wait_limit()
+{
+    const long long v = g_wait_limit.load(std::memory_order_relaxed);
+    return v < 0 ? kProgressPollLimit : v;
+}
 
 bool env_flag(const char *name)
 {
@@ -674,7 +681,10 @@ int launch_dgemm_inc(const DgemmIncParams &gp, cudaStream_t stream)
     return e == cudaSuccess ? SIGK_OK : cuda_fail(e, "float64 increment GEMM launch");
 }
 
-TcPlan mat64_layout(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, int64_t d, int order, bool diffs)
+// es: bytes per element of the increment matrix (8 for float64 cells, 4 for float32 cells); the chunk of x
+// paths per launch and the matrix's share of the workspace follow it.
+TcPlan mat64_layout(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, int64_t d, int order, bool diffs,
+                    size_t es = sizeof(double))
 {
     TcPlan t{};
     const int64_t n = ncx << order, m = ncy << order;
@@ -693,7 +703,7 @@ TcPlan mat64_layout(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, in
     t.rows_x = (ncx + 3) / 4 * 4;
     t.rows_y = ncy;
     const int64_t ny_paths = op == kOpGram ? ny : nx;
-    const size_t per_x = (size_t)t.rows_x * (size_t)(ny_paths * ncy) * sizeof(double);
+    const size_t per_x = (size_t)t.rows_x * (size_t)(ny_paths * ncy) * es;
     int64_t chunk = (int64_t)(tc_chunk_cap() / per_x);
     if (chunk < 1) chunk = 1;
     if (chunk > nx) chunk = nx;
@@ -719,10 +729,11 @@ TcPlan make_mat64_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy,
 // matrix layout, read by the same wavefront kernels.
 constexpr int64_t kStaticMaxDim = 32;
 
-TcPlan make_static_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, int64_t d, int order)
+TcPlan make_static_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, int64_t d, int order, int precision)
 {
     if (op == kOpPairwise || d > kStaticMaxDim) return TcPlan{};
-    return mat64_layout(op, nx, ny, ncx, ncy, d, order, false);
+    const size_t es = cell_prec(precision) == SIGK_PREC_FP64 ? sizeof(double) : sizeof(float);
+    return mat64_layout(op, nx, ny, ncx, ncy, d, order, false, es);
 }
 
 int run_pairs_mat64(const TcPlan &t, int op, const void *x, const void *y, int64_t nx, int64_t ny, int64_t lx,
@@ -795,7 +806,7 @@ int run_pairs_static(const TcPlan &t, int op, int kind, double param, const void
     const int64_t ncx = lx - 1, ncy = ly - 1;
     unsigned char *wsb = reinterpret_cast<unsigned char *>(ws);
     unsigned *err = reinterpret_cast<unsigned *>(wsb + t.err_off);
-    void *mat = wsb + t.ct_off; // sized for float64 elements (float32 cells use half of it)
+    void *mat = wsb + t.ct_off; // float64 elements for float64 cells, float32 for float32 cells
     const bool f64cells = cell_prec(precision) == SIGK_PREC_FP64;
     StaticIncFn fn = get_static_inc_kernel(kind, d, f64cells);
     if (!fn) return fail(SIGK_EUNSUPPORTED, "no static-kernel increment kernel for kind %d, dim %lld", kind,
@@ -1396,6 +1407,11 @@ const char *sigk_last_error_string(void) { return g_last_error.c_str(); }
 
 uint64_t sigk_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
+int64_t sigk_set_wait_limit(int64_t polls)
+{
+    return (int64_t)g_wait_limit.exchange(polls < 0 ? -1 : (long long)polls, std::memory_order_relaxed);
+}
+
 size_t sigk_workspace_size(int op, int64_t n_x, int64_t n_y, int64_t len_x, int64_t len_y, int64_t dim, int order,
                            int dtype, int precision)
 {
@@ -1458,7 +1474,8 @@ size_t sigk_static_workspace_size(int op, int kind, int64_t n_x, int64_t n_y, in
         n_y = n_x;
         len_y = len_x;
     }
-    TcPlan t = make_static_plan(op == SIGK_OP_GRAM ? kOpGram : kOpGramSym, n_x, n_y, len_x - 1, len_y - 1, dim, order);
+    TcPlan t = make_static_plan(op == SIGK_OP_GRAM ? kOpGram : kOpGramSym, n_x, n_y, len_x - 1, len_y - 1, dim, order,
+                                precision);
     return t.ok ? t.ws_bytes : 0;
 }
 
@@ -1497,7 +1514,7 @@ int sigk_gram_static(int op, int kind, double param, const void *x, const void *
     if ((st = check_dev(x, "x", false)) || (st = check_dev(y, "y", false)) || (st = check_dev(out, "out", false)) ||
         (st = check_dev(scale_x, "scale_x", true)) || (st = check_dev(scale_y, "scale_y", true)))
         return st;
-    TcPlan t = make_static_plan(kop, n_x, n_y, len_x - 1, len_y - 1, dim, order);
+    TcPlan t = make_static_plan(kop, n_x, n_y, len_x - 1, len_y - 1, dim, order, precision);
     if (!t.ok) return fail(SIGK_EUNSUPPORTED, "no static-kernel plan");
     if (!workspace || workspace_bytes < t.ws_bytes)
         return fail(SIGK_ENOMEM, "workspace of %zu bytes needed (got %zu)", t.ws_bytes,
@@ -2118,6 +2135,7 @@ int run_ragged(const void *x_pack, const int64_t *x_off, const int64_t *x_len, i
     p.progress = reinterpret_cast<int *>(wsb + pl.progress_off);
     p.pool = wsb + pl.pool_off;
     p.stage_elems_per_warp = tc ? 0 : (int)(kRaggedStageBytesPerWarp / ts);
+    p.poll_limit = wait_limit();
     RaggedFn fn = get_ragged_kernel(f64, in64, tc != nullptr, mat64);
     const size_t smem = tc ? 0 : kRaggedStageBytesPerWarp * kWarpsPerBlock;
     int nb = 0;
@@ -2146,6 +2164,22 @@ extern "C" int sigk_pairwise_ragged(const void *x_pack, const int64_t *x_off, co
     return run_ragged(x_pack, x_off, x_len, x_points, y_pack, y_off, y_len, y_points, order, item_pair, item_band,
                       nitems, pair_rows, pair_bands, pair_bnd_off, bnd_elems, npairs, dim, dtype, static_scale,
                       scale_x, scale_y, out, precision, nullptr, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+extern "C" int sigk_ragged_status(const void *workspace, sigk_stream_t stream)
+{
+    if (!workspace) return fail(SIGK_EINVAL, "workspace is NULL");
+    cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+    int word = 0;
+    e = cudaMemcpy(&word, reinterpret_cast<const unsigned char *>(workspace) + 8, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy of the error word");
+    if (word & kErrWaitTimeout)
+        return fail(SIGK_ETIMEDOUT, "a band wait of the last uneven-batch launch ran out (or its increment GEMM gave "
+                                    "up a wait); the affected pairs are NaN");
+    if (word & kErrInvalidItem)
+        return fail(SIGK_EINVAL, "an item of the last uneven-batch launch broke the plan rules; its pair is NaN");
+    return SIGK_OK;
 }
 
 extern "C" size_t sigk_ragged_tc_workspace_size(int64_t npairs, int64_t dim, int64_t nitems, int64_t bnd_elems,

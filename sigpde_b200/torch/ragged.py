@@ -260,8 +260,14 @@ class RaggedPairwise:
         return self
 
     def error_flag(self):
-        """1 if the last launch refused an item or a band wait ran out (synchronises)."""
+        """Error word of the last launch (synchronises): bit 1 an item was refused,
+        bit 2 a band wait ran out; 0 when every pair was solved."""
         return int(self.ws[8:12].view(torch.int32).item())
+
+    def check(self):
+        """Raise SigkError (SIGK_ETIMEDOUT / SIGK_EINVAL) if the last launch left a
+        pair unsolved (its result is NaN); synchronises the current stream."""
+        _lib.call("sigk_ragged_status", _ptr(self.ws), _stream())
 
     def solve(self):
         with torch.cuda.device(self.device):

@@ -163,18 +163,21 @@ def _cs_err(got, want, kxx, kyy):
 @pytest.mark.parametrize("prec", ["fp32", "tc32"])
 @pytest.mark.parametrize("kind", ["rbf", "l1rbf"])
 @pytest.mark.parametrize("shape", [(9, 8, 40, 37, 8, 2), (5, 4, 9, 11, 3, 1), (3, 3, 70, 66, 5, 3), (7, 6, 33, 40, 17, 1)])
-def test_static_gram_float32_cells(sig, oracle, prec, kind, shape):
+@pytest.mark.parametrize("in64", [False, True])
+def test_static_gram_float32_cells(sig, oracle, prec, kind, shape, in64):
     """Float32 cells (precision fp32 / tc32) read the device-evaluated increments
-    rounded once to float32.  Tolerance as for the linear kernel's float32 cells:
-    error normalised by sqrt(k(x,x) k(y,y)) at most 4x that of the reference's
-    own numerics on the same inputs (float64 arithmetic, float32 storage of
-    every cell: the oracle with store_f32=True), plus 1e-7."""
+    rounded once to float32, from float32 or float64 input paths.  Tolerance as
+    for the linear kernel's float32 cells: error normalised by
+    sqrt(k(x,x) k(y,y)) at most 4x that of the reference's own numerics on the
+    same inputs (float64 arithmetic, float32 storage of every cell: the oracle
+    with store_f32=True), plus 1e-7."""
     nx, ny, lx, ly, d, o = shape
     x = oracle.brownian(nx, lx, d, 500 + lx)
     y = oracle.brownian(ny, ly, d, 600 + ly)
     sigma = 0.9
     k = sig.SigPDE(static_kernel(sig, kind, sigma), o, precision=prec)
-    X, Y = cuda(x, torch.float32), cuda(y, torch.float32)
+    dt = torch.float64 if in64 else torch.float32
+    X, Y = cuda(x, dt), cuda(y, dt)
     assert k._static_on_device(X)
     xin, yin = host(X), host(Y)
     got = host(k.gram(X, Y))

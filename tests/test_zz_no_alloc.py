@@ -26,28 +26,28 @@ def _paths(n, length, dim, seed):
     return synthetic.brownian(n, length, dim, seed, device="cuda")
 
 
-def _gram_with_workspace(lib, X, Y, order, sx, sy):
+def _gram_with_workspace(lib, X, Y, order, sx, sy, prec=0):
     from sigpde_b200 import _lib
     nx, lx, d = X.shape
     ny, ly, _ = Y.shape
     out = torch.empty((nx, ny), device="cuda", dtype=X.dtype)
-    nws = lib.sigk_workspace_size(_lib.SIGK_OP_GRAM, nx, ny, lx, ly, d, order, _lib.SIGK_F32, _lib.SIGK_PREC_FP64)
+    nws = lib.sigk_workspace_size(_lib.SIGK_OP_GRAM, nx, ny, lx, ly, d, order, _lib.SIGK_F32, prec)
     ws = torch.empty(max(nws, 1), dtype=torch.uint8, device="cuda")
     st = lib.sigk_gram(X.data_ptr(), Y.data_ptr(), nx, ny, lx, ly, d, _lib.SIGK_F32, order, 1.0,
                        None if sx is None else sx.data_ptr(), None if sy is None else sy.data_ptr(), out.data_ptr(),
-                       _lib.SIGK_PREC_FP64, ws.data_ptr(), nws, torch.cuda.current_stream().cuda_stream)
+                       prec, ws.data_ptr(), nws, torch.cuda.current_stream().cuda_stream)
     assert st == 0, _lib.last_error()
     return out, nws
 
 
-def _gram_noalloc(lib, X, Y, order, sx, sy):
+def _gram_noalloc(lib, X, Y, order, sx, sy, prec=0):
     from sigpde_b200 import _lib
     nx, lx, d = X.shape
     ny, ly, _ = Y.shape
     out = torch.full((nx, ny), float("nan"), device="cuda", dtype=X.dtype)
     st = lib.sigk_gram_noalloc(X.data_ptr(), Y.data_ptr(), nx, ny, lx, ly, d, _lib.SIGK_F32, order, 1.0,
                                None if sx is None else sx.data_ptr(), None if sy is None else sy.data_ptr(),
-                               out.data_ptr(), _lib.SIGK_PREC_FP64, torch.cuda.current_stream().cuda_stream)
+                               out.data_ptr(), prec, torch.cuda.current_stream().cuda_stream)
     assert st == 0, _lib.last_error()
     return out
 
@@ -74,6 +74,28 @@ def test_noalloc_gram_matches_gram_on_two_calls():
         assert np.all(np.isfinite(g)), f"call {i}: unwritten entries"
         err = np.max(np.abs(g - w) / np.abs(w))
         assert err <= RTOL_OUT32, f"call {i}: max rel diff {err:.3e}"
+
+
+def test_noalloc_gram_matches_gram_on_the_matrix_routes():
+    """The two routes whose scratch holds an increment matrix: tensor-core
+    increments (tc64: split-TF32 GEMM into a float32 matrix, float64 cells) and
+    float64 increments from the FP64 GEMM (fp64 with dim >= 16).  Both fit the
+    8 MiB array at these sizes; each is called twice in a row with other paths."""
+    from sigpde_b200 import _lib
+    lib = _lib.lib()
+    for prec, d in ((_lib.SIGK_PREC_TC64, 8), (_lib.SIGK_PREC_FP64, 16)):
+        for i in range(2):
+            X = _paths(24, 40, d, 700 + 10 * prec + i)
+            Y = _paths(20, 37, d, 800 + 10 * prec + i)
+            want, nws = _gram_with_workspace(lib, X, Y, 1, None, None, prec)
+            assert 0 < nws <= NOALLOC_BYTES
+            got = _gram_noalloc(lib, X, Y, 1, None, None, prec)
+            torch.cuda.synchronize()
+            g = got.double().cpu().numpy()
+            w = want.double().cpu().numpy()
+            assert np.all(np.isfinite(g)), f"precision {prec} call {i}: unwritten entries"
+            err = np.max(np.abs(g - w) / np.abs(w))
+            assert err <= RTOL_OUT32, f"precision {prec} call {i}: max rel diff {err:.3e}"
 
 
 def test_noalloc_gram_refuses_more_than_its_scratch():
