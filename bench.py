@@ -73,6 +73,9 @@ def parse():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "tc32", "tc64"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target length of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shard", action="store_true",
+                    help="N > 1: the ranks solve row blocks of ONE Gram and all-gather them (strong scaling, "
+                         "sigpde_b200.distributed) instead of one replica each")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's Numba GPU path beside the default Gram")
     ap.add_argument("--autotune", action="store_true", help="uneven batches: measure rows per lane per bucket "
@@ -427,16 +430,25 @@ def run_ours(args, w):
     k = sig.SigPDE(sig.kernels.LinearKernel(), w["order"], precision=args.precision)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
 
-    out = k.gram(X, Y)  # also loads libsigk.so
+    shard = args.shard and world > 1
+    if shard:  # one Gram, its rows split over the ranks and all-gathered (NCCL)
+        from sigpde_b200 import distributed as D
+
+        def gram(a, b):
+            return D.sharded_gram(a, b, static_kernel=sig.kernels.LinearKernel(), dyadic_order=w["order"],
+                                  precision=args.precision)
+    else:
+        gram = k.gram
+    out = gram(X, Y)  # also loads libsigk.so
     torch.cuda.synchronize()
 
     clocks = ClockSampler(local)
     clocks.start()
-    times = timed_steps(torch, lambda: k.gram(X, Y), args.steps, args.warmup, flush, barrier)
+    times = timed_steps(torch, lambda: gram(X, Y), args.steps, args.warmup, flush, barrier)
     launches = LAUNCHES["last"]
     clk = clocks.stop()
     total_ms = max_over_ranks(torch, dist, world, sum(times), dev)
-    value = job_rate(world, entries, args.steps, total_ms)
+    value = job_rate(1 if shard else world, entries, args.steps, total_ms)
 
     # end to end through the public API: pinned host paths -> device -> Gram -> pinned host result
     Xh = X.cpu().pin_memory()
@@ -446,11 +458,11 @@ def run_ours(args, w):
     def e2e_step():
         Xd = Xh.to(dev, non_blocking=True)
         Yd = Yh.to(dev, non_blocking=True)
-        Rh.copy_(k.gram(Xd, Yd), non_blocking=True)
+        Rh.copy_(gram(Xd, Yd), non_blocking=True)
 
     e2e_times = timed_steps(torch, e2e_step, args.steps, args.warmup, flush, barrier)
     e2e_ms = max_over_ranks(torch, dist, world, sum(e2e_times), dev)
-    e2e_value = job_rate(world, entries, args.steps, e2e_ms)
+    e2e_value = job_rate(1 if shard else world, entries, args.steps, e2e_ms)
 
     line = None
     if rank == 0:
@@ -502,11 +514,12 @@ def run_ours(args, w):
             "p50_ms": percentile(times, 0.5),
             "p99_ms": percentile(times, 0.99),
             "higher_is_better": True,
-            "scaling": "weak",
+            "scaling": "strong" if shard else "weak",
             "vs_baseline": None,
             "dtype": "f64" if fp64 else "f32",
             "data": "synthetic Brownian paths (seeded PCG64), float32",
-            "config": gram_config(w, world, args.precision),
+            "config": (dict(gram_config(w, 1, args.precision), parallelism=f"Gram rows sharded x{world}")
+                       if shard else gram_config(w, world, args.precision)),
             "cells_per_s": value * cells / entries,
             "accuracy": acc,
             "roofline": {"bound": "fp64" if fp64 else "fp32", "achieved": achieved, "peak": peak,
