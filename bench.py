@@ -865,13 +865,21 @@ def run_ours_ragged(args, w):
     Y = [torch.tensor(a, dtype=torch.float32, device=dev) for a in ys]
     tuning = None
     tuner = None
-    if args.autotune:  # rows per lane (bands per pair) measured per bucket, before and outside the timed region
+    if args.autotune:  # increment source, tile width and rows per lane, measured before and outside the timed region
         import time as _time
         t0 = _time.perf_counter()
         tuner = sig.autotune.RaggedTuner(w["d"], args.precision, torch.float32, dev)
         tuner.tune_for(lx, ly, orders)
-        tuning = {"seconds": _time.perf_counter() - t0,
-                  "rows_per_lane": {f"n<=2^{k[0]},o={k[1]}": r for k, r in sorted(tuner.table.items())}}
+        tuning = dict(tuner.report(), seconds=_time.perf_counter() - t0,
+                      batch_timings_ms={str(k): v for k, v in tuner.batch_timings.items()})
+        # the default rule on the same batch, for comparison (timed like the tuned plan below)
+        dflt = sig.ragged.RaggedPairwise(lx, ly, orders, w["d"], torch.float32, dev, args.precision)
+        dflt.load(X, Y)
+        dflt.capture()
+        fl = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+        tuning["default_rule_ms_per_step"] = statistics.mean(
+            timed_steps(torch, dflt.solve, args.steps, args.warmup, fl, lambda: None))
+        del dflt, fl
     solver = sig.ragged.RaggedPairwise(lx, ly, orders, w["d"], torch.float32, dev, args.precision, tuner=tuner)
     solver.load(X, Y)
     solver.capture()

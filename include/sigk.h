@@ -336,13 +336,16 @@ SIGK_API int sigk_pairwise_ragged(const void *x_pack, const int64_t *x_off, cons
  *   a_row0[b]: first row of pair b's row path in the A operand image (a
  *     multiple of 8, the pair taking round_up(rows_b, 8) rows); a_rows: image
  *     rows, at least the last pair's end + 128;
- *   b_row0[b], b_rows: the same for the column paths (end + 256);
+ *   b_row0[b], b_rows: the same for the column paths (end + N, N below);
  *   inc_off[b]: offset (floats, a multiple of 4) of pair b's block in a matrix
  *     of inc_elems floats;
- *   tiles (ntiles x 6 int64): one 128 x 256 GEMM tile each,
+ *   tile_n: 0 or 256 for 128 x 256 GEMM tiles, 128 for 128 x 128 tiles
+ *     (tensor-core precisions only; an autotuner knob, same results); with
+ *     N = tile_n (256 when 0) and b_rows >= the last pair's end + N:
+ *   tiles (ntiles x 6 int64): one 128 x N GEMM tile each,
  *     {a_row, b_row, m_valid, n_valid, out_off, ld}: a_row = a_row0[b] + 128 i,
- *     b_row = b_row0[b] + 256 j, m_valid = min(128, rows_b - 128 i),
- *     n_valid = min(256, cols_b - 256 j), out_off = inc_off[b] + 256 j ld_b +
+ *     b_row = b_row0[b] + N j, m_valid = min(128, rows_b - 128 i),
+ *     n_valid = min(N, cols_b - N j), out_off = inc_off[b] + N j ld_b +
  *     128 i, ld = ld_b, for every tile (i, j) of every pair.
  * A tile entry outside these buffers is skipped and the affected pairs give
  * NaN (with the error flag of the ragged launch set).  The remaining
@@ -359,6 +362,7 @@ typedef struct {
     int64_t inc_elems;
     const int64_t *tiles;
     int64_t ntiles;
+    int64_t tile_n;
 } sigk_ragged_tc_plan;
 
 SIGK_API size_t sigk_ragged_tc_workspace_size(int64_t npairs, int64_t dim, int64_t nitems, int64_t bnd_elems,

@@ -47,7 +47,7 @@ class RaggedTcPlan(ctypes.Structure):
     """sigk_ragged_tc_plan (include/sigk.h)."""
     _fields_ = [("a_row0", ctypes.c_void_p), ("b_row0", ctypes.c_void_p), ("a_rows", ctypes.c_int64),
                 ("b_rows", ctypes.c_int64), ("inc_off", ctypes.c_void_p), ("inc_elems", ctypes.c_int64),
-                ("tiles", ctypes.c_void_p), ("ntiles", ctypes.c_int64)]
+                ("tiles", ctypes.c_void_p), ("ntiles", ctypes.c_int64), ("tile_n", ctypes.c_int64)]
 
 
 _plan_p = ctypes.POINTER(RaggedTcPlan)

@@ -73,7 +73,7 @@ RaggedDeltaFn get_ragged_delta_kernel(bool f64cells, bool in64);
 // kTcBN) and the streaming wavefront that reads its output.
 constexpr int kTcBN = 256;
 TcImageFn get_tc_image_kernel(bool in64);
-TcGemmFn get_tc_gemm_kernel();
+TcGemmFn get_tc_gemm_kernel(int bn = kTcBN); // 128 x bn tiles, bn in {128, 256}
 TcRaggedImageFn get_tc_ragged_image_kernel(bool in64);
 // float64 increment matrix on the CUDA cores (dgemm_inc.cuh)
 DgemmIncFn get_dgemm_inc_kernel();

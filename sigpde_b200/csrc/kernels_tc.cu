@@ -44,7 +44,7 @@ StreamIncFn get_stream_inc_kernel(bool f64cells, int R, int O, bool mat64, int W
 
 TcImageFn get_tc_image_kernel(bool in64) { return in64 ? tc_image_kernel<double> : tc_image_kernel<float>; }
 
-TcGemmFn get_tc_gemm_kernel() { return tc_gemm_kernel<kTcBN>; }
+TcGemmFn get_tc_gemm_kernel(int bn) { return bn == 128 ? tc_gemm_kernel<128> : tc_gemm_kernel<kTcBN>; }
 
 DgemmIncFn get_dgemm_inc_kernel() { return dgemm_inc_kernel<kDgTile>; }
 

@@ -441,26 +441,28 @@ int encode_out_map(CUtensorMap *map, float *out, int64_t ld, int64_t n_rows)
     return SIGK_OK;
 }
 
-int tc_gemm(const TcGemmParams &gp, cudaStream_t stream)
+// bn: tile width of the GEMM (kTcBN = 256; 128 for the uneven-batch plans that ask for it).
+int tc_gemm(const TcGemmParams &gp, cudaStream_t stream, int bn = kTcBN)
 {
-    TcGemmFn fn = get_tc_gemm_kernel();
-    const size_t smem = tc_gemm_smem(kTcBN, gp.kp);
+    TcGemmFn fn = get_tc_gemm_kernel(bn);
+    const size_t smem = tc_gemm_smem(bn, gp.kp);
+    const int w = bn == 128 ? 0 : 1;
     static std::mutex mu;
-    static bool attr_set[64] = {};
+    static bool attr_set[2][64] = {};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     {
         std::lock_guard<std::mutex> lk(mu);
         if (dev < 0 || dev >= 64) return fail(SIGK_EINVAL, "device index %d out of range", dev);
-        if (!attr_set[dev]) {
+        if (!attr_set[w][dev]) {
             int optin = 0;
             e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
             if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
             if ((size_t)optin < smem) return fail(SIGK_ELAUNCH, "GEMM needs %zu bytes of shared memory", smem);
             e = cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
             if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
-            attr_set[dev] = true;
+            attr_set[w][dev] = true;
         }
     }
     CUtensorMap map;
@@ -1969,8 +1971,12 @@ int run_ragged(const void *x_pack, const int64_t *x_off, const int64_t *x_len, i
             return fail(SIGK_EINVAL, "a plan needs precision SIGK_PREC_TC32, _TC64 or _FP64");
         if (!mat64 && dim > 32)
             return fail(SIGK_EUNSUPPORTED, "tensor-core increments support dim <= 32 (got %lld)", (long long)dim);
-        if (tc->a_rows < kTcM || tc->b_rows < kTcBN || tc->inc_elems < 4 || tc->ntiles < 1 ||
-            (tc->a_rows & 7) || (tc->b_rows & 7))
+        if (tc->tile_n != 0 && tc->tile_n != 128 && tc->tile_n != kTcBN)
+            return fail(SIGK_EINVAL, "plan.tile_n must be 0, 128 or 256 (got %lld)", (long long)tc->tile_n);
+        if (mat64 && tc->tile_n == 128)
+            return fail(SIGK_EINVAL, "128-column tiles apply to tensor-core precisions only");
+        if (tc->a_rows < kTcM || tc->b_rows < (tc->tile_n ? tc->tile_n : kTcBN) || tc->inc_elems < 4 ||
+            tc->ntiles < 1 || (tc->a_rows & 7) || (tc->b_rows & 7))
             return fail(SIGK_EINVAL, "tensor-core plan sizes are inconsistent");
         if ((st = check_dev(tc->a_row0, "plan.a_row0", false)) || (st = check_dev(tc->b_row0, "plan.b_row0", false)) ||
             (st = check_dev(tc->inc_off, "plan.inc_off", false)) || (st = check_dev(tc->tiles, "plan.tiles", false)))
@@ -2109,7 +2115,7 @@ int run_ragged(const void *x_pack, const int64_t *x_off, const int64_t *x_len, i
         gp.a_rows = tc->a_rows;
         gp.b_rows = tc->b_rows;
         gp.out_elems = tc->inc_elems;
-        if ((st = tc_gemm(gp, stream))) return st;
+        if ((st = tc_gemm(gp, stream, tc->tile_n == 128 ? 128 : kTcBN))) return st;
         p.inc = inc;
         p.inc_off = tc->inc_off;
         p.inc_elems = tc->inc_elems;

@@ -103,7 +103,17 @@ def tc_plan(x_lengths, y_lengths, tile_m=128, tile_n=256):
                       np.minimum(tile_n, cols[pb] - tile_n * j), inc_off[pb] + tile_n * j * ld[pb] + tile_m * i,
                       ld[pb]], axis=1).astype(np.int64)
     return {"a_row0": a_row0, "b_row0": b_row0, "a_rows": int(r8.sum()) + tile_m, "b_rows": int(c8.sum()) + tile_n,
-            "inc_off": inc_off, "inc_elems": int(blk.sum()), "tiles": tiles.reshape(-1, 6)}
+            "inc_off": inc_off, "inc_elems": int(blk.sum()), "tiles": tiles.reshape(-1, 6), "tile_n": int(tile_n)}
+
+
+def default_source(precision, dim):
+    """Where a batch's increments come from when nothing was tuned: a GEMM into
+    per-pair blocks for the tensor-core precisions (dim <= 32) and for fp64 with
+    dim >= MAT64_MIN_DIM (the d FMAs per coarse cell dominate the fused form
+    there), else formed inside the wavefront."""
+    if precision in ("tc32", "tc64"):
+        return "matrix" if dim <= 32 else "fused"
+    return "matrix" if precision == "fp64" and dim >= MAT64_MIN_DIM else "fused"
 
 
 def plan(x_lengths, y_lengths, orders, dim, tsize, staged=True, rows_fn=None):
@@ -144,7 +154,7 @@ class RaggedPairwise:
     the rows per lane (hence bands) per pair instead of the default rule."""
 
     def __init__(self, x_lengths, y_lengths, orders, dim, dtype=torch.float32, device="cuda", precision="fp64",
-                 static_scale=1.0, tuner=None, rows_fn=None):
+                 static_scale=1.0, tuner=None, rows_fn=None, source=None, tile_n=None):
         if precision not in _PREC:
             raise ValueError(f"precision must be one of {sorted(_PREC)}")
         x_lengths = [int(v) for v in x_lengths]
@@ -173,13 +183,27 @@ class RaggedPairwise:
         self.x_off, self.y_off = xo.to(self.device), yo.to(self.device)
         self.order = od.to(self.device)
         tsize = 8 if precision in ("fp64", "tc64") else 4
-        use_tc = precision in ("tc32", "tc64") and self.dim <= 32
-        # fp64 with d >= MAT64_MIN_DIM: float64 increments of all pairs from one FP64 GEMM over the same
-        # plan's tiles, read by the wavefront (the d FMAs per coarse cell dominate the fused form there)
-        use_tc = use_tc or (precision == "fp64" and self.dim >= MAT64_MIN_DIM)
-        if rows_fn is None and tuner is not None:  # rows per lane from measurements (autotune.py)
-            tuner.tune_for(x_lengths, y_lengths, orders)
-            rows_fn = tuner.rows_for
+        if tuner is not None:  # increment source, tile width and rows per lane from measurements (autotune.py)
+            choice = tuner.tune_for(x_lengths, y_lengths, orders)
+            source = choice["source"] if source is None else source
+            tile_n = choice["tile_n"] if tile_n is None else tile_n
+            if rows_fn is None:
+                rows_fn = tuner.rows_for
+        if source is None:
+            source = default_source(precision, self.dim)
+        if source not in ("matrix", "fused"):
+            raise ValueError("source must be 'matrix' or 'fused'")
+        # "matrix": the increments of all pairs from one GEMM into per-pair blocks (tensor cores for tc32 /
+        # tc64 with dim <= 32, the FP64 GEMM for fp64), read by the wavefront; "fused": each lane forms its
+        # increments from staged differences on the CUDA cores (the tensor-core precisions then keep their
+        # cells, with float64 dot products)
+        use_tc = source == "matrix" and (precision == "fp64" or (precision in ("tc32", "tc64") and self.dim <= 32))
+        self.source = "matrix" if use_tc else "fused"
+        if tile_n is None or not use_tc or precision == "fp64":
+            tile_n = 256
+        if tile_n not in (128, 256):
+            raise ValueError("tile_n must be 128 or 256")
+        self.tile_n = int(tile_n)
         pl = plan(x_lengths, y_lengths, orders, self.dim, tsize, staged=not use_tc, rows_fn=rows_fn)
         self.item_pair = torch.as_tensor(pl["item_pair"], device=self.device)
         self.item_band = torch.as_tensor(pl["item_band"], dtype=torch.int32, device=self.device)
@@ -195,12 +219,12 @@ class RaggedPairwise:
         self.y_points = int(yl.sum())
         self.tc = None
         if use_tc:
-            tp = tc_plan(x_lengths, y_lengths)
+            tp = tc_plan(x_lengths, y_lengths, tile_n=self.tile_n)
             self._tc_arrays = {k: torch.as_tensor(tp[k], device=self.device)
                                for k in ("a_row0", "b_row0", "inc_off", "tiles")}
             self.tc = _lib.RaggedTcPlan(_ptr(self._tc_arrays["a_row0"]), _ptr(self._tc_arrays["b_row0"]), tp["a_rows"],
                                         tp["b_rows"], _ptr(self._tc_arrays["inc_off"]), tp["inc_elems"],
-                                        _ptr(self._tc_arrays["tiles"]), int(tp["tiles"].shape[0]))
+                                        _ptr(self._tc_arrays["tiles"]), int(tp["tiles"].shape[0]), self.tile_n)
             nws = _lib.lib().sigk_ragged_tc_workspace_size(self.n, self.dim, self.nitems, self.bnd_elems, self.prec,
                                                            self.tc)
         else:
