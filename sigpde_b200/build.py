@@ -23,8 +23,8 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 SOURCES = ["sigk_api.cu", "kernels_pair_f64.cu", "kernels_pair_f32.cu", "kernels_norm.cu", "kernels_stream.cu",
            "kernels_stream_reg_f64.cu", "kernels_stream_reg_f32.cu", "kernels_stream_reg_f32x2.cu", "kernels_stream_reg_f64x2.cu", "kernels_ragged.cu", "kernels_tc.cu", "kernels_norm_pipe.cu",
-           "kernels_grad.cu"]
-HEADERS = ["wave.cuh", "sigk_kernels.cuh", "stream.cuh", "dispatch.h", "kernels_stream_reg.inc", "ragged.cuh", "tc.cuh", "norm_pipe.cuh", "dgemm_inc.cuh", "static_inc.cuh", "grad.cuh"]
+           "kernels_grad.cu", "kernels_fused_tc.cu"]
+HEADERS = ["wave.cuh", "sigk_kernels.cuh", "stream.cuh", "dispatch.h", "kernels_stream_reg.inc", "ragged.cuh", "tc.cuh", "norm_pipe.cuh", "dgemm_inc.cuh", "static_inc.cuh", "grad.cuh", "fused_tc.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",

@@ -20,6 +20,7 @@ struct StaticIncParams;
 struct GradParams;
 struct RaggedDgemmParams;
 struct GradContractParams;
+struct FusedTcParams;
 }
 struct CUtensorMap_st; // cuda.h
 namespace sigk {
@@ -106,5 +107,9 @@ GradAuxFns get_grad_aux_kernels();
 // mat64: the increment matrix holds float64 (dgemm_inc_kernel) instead of float32 (tensor cores)
 // W: lanes a pair pipeline (32, or 16 for pairs of at most 16 R rows with R <= 8)
 StreamIncFn get_stream_inc_kernel(bool f64cells, int R, int O, bool mat64, int W = 32);
+// Fused tensor-core Gram (fused_tc.cuh): tcgen05 increments handed to the wavefront through shared
+// memory; R rows a lane at order O (R >= 2^O, R >> O <= 4), null where not built
+using FusedTcFn = void (*)(FusedTcParams);
+FusedTcFn get_fused_tc_kernel(int R, int O);
 
 } // namespace sigk

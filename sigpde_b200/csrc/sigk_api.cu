@@ -26,6 +26,7 @@
 #include "dgemm_inc.cuh"
 #include "static_inc.cuh"
 #include "grad.cuh"
+#include "fused_tc.cuh"
 
 namespace sigk {
 namespace {
@@ -383,10 +384,12 @@ TcPlan make_tc_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, in
     return t;
 }
 
+// quad_rc > 0: the fused Gram's permuted A layout (TcImageParams::quad_rc)
 int tc_image(bool in64, const void *x, int64_t npaths, int64_t len, int64_t d, int64_t rows_per_path, int64_t tile_rows,
-             int64_t ntiles, int kp, double f, const void *s, float *hi, float *lo, cudaStream_t stream)
+             int64_t ntiles, int kp, double f, const void *s, float *hi, float *lo, cudaStream_t stream, int quad_rc = 0)
 {
     TcImageParams ip{};
+    ip.quad_rc = quad_rc;
     ip.x = x;
     ip.npaths = npaths;
     ip.len = len;
@@ -569,6 +572,105 @@ int consume_matrix(const TcPlan &t, int op, const void *mat, bool mat64, int64_t
     count_launch();
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? SIGK_OK : cuda_fail(e, "stream increment kernel launch");
+}
+
+// Fused tensor-core Gram (fused_tc.cuh): the tcgen05 increments go from TMEM
+// through shared memory to the wavefront, never to HBM.  Workspace: error word,
+// then the hi / lo operand images (128 rows per x path, T rows per y path).
+struct FtPlan {
+    bool ok = false;
+    int R = 0, O = 0, kp = 0, T = 0;
+    size_t err_off = 0, a_off = 0, a_bytes = 0, b_off = 0, b_bytes = 0, ws_bytes = 0;
+};
+
+FtPlan make_fused_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, int64_t d, int order, int precision)
+{
+    FtPlan f;
+    // opt-in (SIGK_FUSED_TC=1): measured slower than the two-phase route on every shape tried (TMEM holds
+    // at most 8 pair streams per SM; at low orders each chunk boundary's TMEM loads dominate)
+    if (op != kOpGram || precision != SIGK_PREC_TC64 || d > 16 || order > 3 || ncx > kTcM || !env_flag("SIGK_FUSED_TC"))
+        return f;
+    const int64_t n = ncx << order;
+    if (n > 32 * 16) return f; // one band
+    const int R = pick_rows(n);
+    if ((R >> order) < 1 || ((R >> order) << order) != R || (R >> order) * 32 > kTcM) return f;
+    if (!get_fused_tc_kernel(R, order)) return f;
+    f.ok = true;
+    f.R = R;
+    f.O = order;
+    f.kp = (int)((d + 7) / 8 * 8);
+    f.T = (int)((ncy + kFtChunk - 1) / kFtChunk * kFtChunk);
+    f.err_off = 0;
+    f.a_off = 256;
+    f.a_bytes = align256((size_t)((nx + 3) / 4) * (R >> order) * kTcM * f.kp * sizeof(float));
+    f.b_off = f.a_off + 2 * f.a_bytes;
+    f.b_bytes = align256((size_t)ny * f.T * f.kp * sizeof(float));
+    f.ws_bytes = f.b_off + 2 * f.b_bytes;
+    return f;
+}
+
+int run_pairs_fused(const FtPlan &f, const void *x, const void *y, int64_t nx, int64_t ny, int64_t lx, int64_t ly,
+                    int64_t d, int dtype, int order, double static_scale, const void *sx, const void *sy, void *out,
+                    int64_t out_ld, void *ws, cudaStream_t stream)
+{
+    int st;
+    const bool in64 = dtype == SIGK_F64;
+    unsigned char *wsb = reinterpret_cast<unsigned char *>(ws);
+    unsigned *err = reinterpret_cast<unsigned *>(wsb + f.err_off);
+    float *a_hi = reinterpret_cast<float *>(wsb + f.a_off), *a_lo = reinterpret_cast<float *>(wsb + f.a_off + f.a_bytes);
+    float *b_hi = reinterpret_cast<float *>(wsb + f.b_off), *b_lo = reinterpret_cast<float *>(wsb + f.b_off + f.b_bytes);
+    cudaError_t e = cudaMemsetAsync(err, 0, sizeof(unsigned), stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+    const double fs = static_scale * std::ldexp(1.0, -2 * order); // x side: static scale * 4^-order * scale_x
+    const int rc = f.R >> f.O;
+    if ((st = tc_image(in64, x, nx, lx, d, kTcM, kTcM, (nx + 3) / 4 * rc, f.kp, fs, sx, a_hi, a_lo, stream, rc)))
+        return st;
+    if ((st = tc_image(in64, y, ny, ly, d, f.T, f.T, ny, f.kp, 1.0, sy, b_hi, b_lo, stream))) return st;
+    FusedTcFn fn = get_fused_tc_kernel(f.R, f.O);
+    const size_t smem = fused_tc_smem(rc, f.kp);
+    int dev = 0;
+    e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    {
+        static std::mutex mu;
+        static std::unordered_map<uint64_t, bool> done; // (device, function) opted in to the maximum
+        const uint64_t key = ((uint64_t)(uintptr_t)fn << 8) ^ (uint64_t)dev;
+        std::lock_guard<std::mutex> lk(mu);
+        if (!done[key]) {
+            int optin = 0;
+            e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
+            if ((size_t)optin < smem) return fail(SIGK_ELAUNCH, "fused kernel needs %zu bytes of shared memory", smem);
+            // the device maximum, not this call's size: a later call with a wider dimension needs more
+            e = cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+            done[key] = true;
+        }
+    }
+    FusedTcParams fp{};
+    fp.a_hi = a_hi;
+    fp.a_lo = a_lo;
+    fp.b_hi = b_hi;
+    fp.b_lo = b_lo;
+    fp.nx = nx;
+    fp.ny = ny;
+    fp.ncx = (int)(lx - 1);
+    fp.ncy = (int)(ly - 1);
+    fp.kp = f.kp;
+    fp.T = f.T;
+    fp.ngroups = (nx + kFtWarps - 1) / kFtWarps * ny;
+    const int64_t cap = 2 * (int64_t)sm_count(); // two CTAs per SM (TMEM: 2 x 256 columns)
+    const int64_t ctas0 = fp.ngroups < cap ? fp.ngroups : cap;
+    fp.per_cta = (fp.ngroups + ctas0 - 1) / ctas0;
+    const int64_t ctas = (fp.ngroups + fp.per_cta - 1) / fp.per_cta;
+    fp.in64 = in64;
+    fp.out = out;
+    fp.out_ld = out_ld;
+    fp.err = err;
+    fn<<<(unsigned)ctas, (kFtWarps + 1) * 32, smem, stream>>>(fp);
+    count_launch();
+    e = cudaGetLastError();
+    return e == cudaSuccess ? SIGK_OK : cuda_fail(e, "fused tensor-core kernel launch");
 }
 
 int run_pairs_tc(const TcPlan &t, int op, const void *x, const void *y, int64_t nx, int64_t ny, int64_t lx, int64_t ly,
@@ -1180,6 +1282,14 @@ int run_pairs(int op, const void *x, const void *y, int64_t nx, int64_t ny, int6
         (st = check_dev(sx, "scale_x", true)) || (st = check_dev(sy, "scale_y", true)))
         return st;
     if (is_tc(precision)) {
+        const FtPlan f = make_fused_plan(op, nx, ny, lx - 1, ly - 1, d, order, precision);
+        if (f.ok) {
+            if (!ws || ws_bytes < f.ws_bytes)
+                return fail(SIGK_ENOMEM, "workspace of %zu bytes needed (got %zu)", f.ws_bytes, ws ? ws_bytes : 0);
+            if (((uintptr_t)ws & 255) != 0) return fail(SIGK_EINVAL, "workspace must be 256-byte aligned");
+            return run_pairs_fused(f, x, y, nx, ny, lx, ly, d, dtype, order, static_scale, sx, sy, out, out_ld, ws,
+                                   stream);
+        }
         TcPlan t = make_tc_plan(op, nx, ny, lx - 1, ly - 1, d, order, tsize_of(precision));
         if (t.ok) {
             if (!ws || ws_bytes < t.ws_bytes)
@@ -1427,6 +1537,9 @@ size_t sigk_workspace_size(int op, int64_t n_x, int64_t n_y, int64_t len_x, int6
     if (op == SIGK_OP_PAIRWISE) n_y = n_x;
     if (op == SIGK_OP_NORMALIZE) return norm_plan(n_x, len_x - 1, dim > 0 ? dim : 1, order, dim == 0).ws_bytes;
     if (is_tc(precision) && dim > 0) {
+        const int kop = op == SIGK_OP_PAIRWISE ? kOpPairwise : op == SIGK_OP_GRAM ? kOpGram : kOpGramSym;
+        const FtPlan f = make_fused_plan(kop, n_x, n_y, len_x - 1, len_y - 1, dim, order, precision);
+        if (f.ok) return f.ws_bytes;
         TcPlan t = make_tc_plan(op, n_x, n_y, len_x - 1, len_y - 1, dim, order, tsize_of(precision));
         if (t.ok) return t.ws_bytes;
         precision = cell_prec(precision); // as the entry points: CUDA-core increments, same cells

@@ -63,6 +63,9 @@ struct TcImageParams {
     double f;              // scale f * s[p]
     const void *s;         // per-path scale in TIN or null
     float *hi, *lo;
+    // quad_rc > 0: the fused Gram's A layout (fused_tc.cuh).  Blocks of 4 x paths, each block quad_rc
+    // tiles of 128 rows; in tile k of block a, row 32 w + i holds coarse row quad_rc * i + k of path 4a + w
+    int quad_rc;
 };
 
 // Image layout (group-major): element (row m, k) sits at float offset
@@ -96,8 +99,15 @@ __global__ void tc_image_kernel(TcImageParams p)
         const int64_t g = rest / nkc;
         const int64_t m = g * 8 + r8;
         const int64_t k = kc * 4 + k4;
-        const int64_t path = m / p.rows_per_path;
-        const int64_t c = m - path * p.rows_per_path;
+        int64_t path, c;
+        if (p.quad_rc > 0) {
+            const int64_t per_block = (int64_t)p.quad_rc * 128, rem = m % per_block;
+            path = 4 * (m / per_block) + (rem >> 5 & 3);
+            c = (int64_t)p.quad_rc * (rem & 31) + rem / 128;
+        } else {
+            path = m / p.rows_per_path;
+            c = m - path * p.rows_per_path;
+        }
         float hi = 0.f, lo = 0.f;
         if (path < p.npaths && c < nc && k < p.d) {
             const TIN *xp = x + (path * p.len + c) * p.d + k;

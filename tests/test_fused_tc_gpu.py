@@ -1,0 +1,86 @@
+"""The fused tensor-core Gram (fused_tc.cuh): tcgen05 increments handed from
+TMEM through shared memory to the wavefront, no increment matrix in HBM.
+
+The route is opt-in (SIGK_FUSED_TC=1; it measured slower than the two-phase
+route).  Its arithmetic is the two-phase path's (tc_gemm_kernel writing the
+float32 increment matrix, stream_inc_kernel reading it): the same split-TF32
+MMAs per increment and the same float64 cells, so the results must be bitwise
+equal to that path.  Against the float64 oracle the
+tc64 bound applies: error normalised by sqrt(k(x,x) k(y,y)) at most 1e-5.
+Shapes cover every instantiated (rows per lane, order), time lines padded to
+16 columns, a last block of fewer than 4 y paths, fewer groups than CTAs,
+scales, float64 inputs and dimensions 1..16.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+CS_TC64 = 1e-5
+
+SHAPES = [
+    # (nx, ny, len_x, len_y, dim, order)
+    (48, 37, 128, 128, 8, 2),   # config 2's path shape: 16 rows a lane, 4 coarse rows
+    (9, 11, 40, 57, 3, 1),      # 78 rows: 4 rows a lane
+    (5, 6, 20, 33, 16, 0),      # 19 rows: 2 rows a lane at order 0
+    (7, 13, 100, 71, 8, 1),     # 198 rows: 8 a lane
+    (6, 5, 64, 40, 5, 3),       # 504 rows at order 3: 16 a lane, 2 coarse rows
+    (3, 2, 30, 18, 1, 2),       # 116 rows: 4 a lane at order 2 (1 coarse row); 1 group
+    (33, 3, 17, 129, 16, 0),    # one y block of 3 paths, ncy = 128
+    (4, 9, 66, 64, 8, 2),       # 260 rows: 16 a lane, 4 coarse rows (one row of padding)
+]
+
+
+def host(t):
+    return t.detach().double().cpu().numpy()
+
+
+@pytest.fixture(scope="module")
+def sig():
+    import sigpde_b200.torch as s
+    return s
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+@pytest.mark.parametrize("in64", [False, True])
+def test_fused_equals_two_phase_and_oracle(sig, oracle, monkeypatch, shape, in64):
+    nx, ny, lx, ly, d, o = shape
+    dt = torch.float64 if in64 else torch.float32
+    X = torch.tensor(oracle.brownian(nx, lx, d, 1000 + lx), dtype=dt, device="cuda")
+    Y = torch.tensor(oracle.brownian(ny, ly, d, 2000 + ly), dtype=dt, device="cuda")
+    sx = torch.linspace(0.6, 1.4, nx, dtype=dt, device="cuda")
+    k = sig.SigPDE(sig.kernels.LinearKernel(0.8), o, precision="tc64")
+    for scales in ((None, None), (sx, None)):
+        monkeypatch.setenv("SIGK_FUSED_TC", "1")
+        fused = k.gram(X, Y, *scales)
+        monkeypatch.delenv("SIGK_FUSED_TC", raising=False)
+        two = k.gram(X, Y, *scales)
+        torch.cuda.synchronize()
+        assert torch.equal(fused, two), f"{shape} in64={in64} scaled={scales[0] is not None}"
+    monkeypatch.setenv("SIGK_FUSED_TC", "1")
+    G = host(k.gram(X, Y))
+    monkeypatch.delenv("SIGK_FUSED_TC", raising=False)
+    x, y = host(X), host(Y)
+    want = oracle.gram(x, y, o, static_param=0.8)
+    kxx = oracle.pairwise(x, None, o, static_param=0.8)[:, None]
+    kyy = oracle.pairwise(y, None, o, static_param=0.8)[None, :]
+    assert float(np.max(np.abs(G - want) / np.sqrt(kxx * kyy))) <= CS_TC64
+
+
+def test_fused_route_is_taken_and_small(sig):
+    """The fused route's workspace holds only the operand images (no increment
+    matrix): 256 x 256 paths of length 128 in 8 dims need ~2.2 MB, against
+    4.26 GB for the two-phase matrix."""
+    import os
+    from sigpde_b200 import _lib
+    lib = _lib.lib()
+    os.environ["SIGK_FUSED_TC"] = "1"
+    try:
+        fused = lib.sigk_workspace_size(_lib.SIGK_OP_GRAM, 256, 256, 128, 128, 8, 2, _lib.SIGK_F32,
+                                        _lib.SIGK_PREC_TC64)
+    finally:
+        os.environ.pop("SIGK_FUSED_TC", None)
+    two = lib.sigk_workspace_size(_lib.SIGK_OP_GRAM, 256, 256, 128, 128, 8, 2, _lib.SIGK_F32, _lib.SIGK_PREC_TC64)
+    assert fused < 8 << 20 < (1 << 30) < two
