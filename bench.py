@@ -103,6 +103,30 @@ def workload_name(w):
     return f"SigPDE.gram {w['nx']}x{w['ny']}, L={w['L']}, d={w['d']}, dyadic_order={w['order']}, {kern}"
 
 
+def issue_roofline(w, precision, ms, gemm_tflops):
+    """The wavefront's arithmetic pipe in instructions rather than FLOPs.
+
+    A refined cell is 3 instructions of the cell type (float64: add, mul, fma;
+    the stencil's add and mul each take a full issue slot but count as one FLOP),
+    and a coarse cell adds 4 for its coefficients plus d fmas for its increment
+    when the CUDA cores form it (fp64 / fp32; tc32 / tc64 take it from the tensor
+    cores).  float32 cells take 5 instructions a cell (the one-rounding form).
+    The ceiling is the pipe's measured fma rate: the in-run cuBLAS GEMM's FLOP/s
+    over 2, so a kernel that kept the pipe busy with useful instructions would
+    read 1.0."""
+    entries, cells, _ = workload_units(w)
+    coarse = entries * (w["L"] - 1) ** 2
+    per_cell = 3 if precision in ("fp64", "tc64") else 5
+    per_coarse = 4 + (w["d"] if precision in ("fp64", "fp32") else 0)
+    instr = per_cell * cells + per_coarse * coarse
+    achieved = instr / (ms * 1e-3) / 1e12
+    peak = gemm_tflops / 2
+    return {"unit": "T instructions/s", "achieved": achieved, "peak": peak, "frac": achieved / peak,
+            "instructions_per_launch": instr,
+            "note": "same time and GEMM as frac above, counted in pipe instructions (ncu's FP64-pipe activity "
+                    "reads the same quantity)"}
+
+
 def gram_config(w, world, precision):
     """The `config` of a Gram workload's bench line, shared by every arm so that
     the GPU line and the reference line describe the same workload."""
@@ -524,6 +548,7 @@ def run_ours(args, w):
             "accuracy": acc,
             "roofline": {"bound": "fp64" if fp64 else "fp32", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
+                         "issue": issue_roofline(w, args.precision, ms, peak),
                          "peak_source": ("measured cuBLAS " + ("DGEMM" if fp64 else "SGEMM (no TF32)") +
                                          " 4096^3 on this device (the wavefront is bound by the "
                                          + ("FP64" if fp64 else "FP32") + " pipe, not HBM or tensor cores)"),
