@@ -76,6 +76,8 @@ def parse():
     ap.add_argument("--shard", action="store_true",
                     help="N > 1: the ranks solve row blocks of ONE Gram and all-gather them (strong scaling, "
                          "sigpde_b200.distributed) instead of one replica each")
+    ap.add_argument("--no-other-workloads", action="store_true",
+                    help="skip the short runs of robust512, uneven4096 and serve_light after the default Gram")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's Numba GPU path beside the default Gram")
     ap.add_argument("--autotune", action="store_true", help="uneven batches: measure rows per lane per bucket "
@@ -125,6 +127,50 @@ def issue_roofline(w, precision, ms, gemm_tflops):
             "instructions_per_launch": instr,
             "note": "same time and GEMM as frac above, counted in pipe instructions (ncu's FP64-pipe activity "
                     "reads the same quantity)"}
+
+
+def other_workloads(args):
+    """Short runs of the other benchmark configurations, after (outside) the
+    default Gram's timed region, so that one bench line records them too: the
+    robust Gram (robust512), the uneven batch (uneven4096) and the serving trace
+    (serve_light, burst arrivals: served stream against per-request plain
+    launches).  Each runner prints its own line; the figures kept here are its
+    times, with 5 timed steps after 3 warm-ups and no CPU baselines."""
+    import argparse
+    import contextlib
+    import io
+
+    def run(fn, workload, **over):
+        a = argparse.Namespace(**vars(args))
+        a.steps, a.warmup, a.no_cpu_baseline, a.autotune, a.burst = 5, 3, True, False, False
+        for k, v in over.items():
+            setattr(a, k, v)
+        buf = io.StringIO()
+        try:
+            with contextlib.redirect_stdout(buf):
+                fn(a, WORKLOADS[workload])
+            return json.loads([l for l in buf.getvalue().splitlines() if l.startswith("{")][-1])
+        except Exception as e:  # a failed side run must not lose the headline line
+            return {"error": f"{type(e).__name__}: {e}"[:200]}
+
+    out = {"note": "5 timed steps after 3 warm-ups each, measured after the headline's timed region"}
+    for prec in ("fp64", "tc64"):
+        r = run(run_ours_robust, "robust512", precision=prec)
+        out[f"robust512_{prec}"] = {k: r.get(k) for k in ("ms_per_step", "value", "unit", "phases_ms", "error")
+                                    if k in r}
+        r = run(run_ours_ragged, "uneven4096", precision=prec)
+        out[f"uneven4096_{prec}"] = {k: r.get(k) for k in ("ms_per_step", "value", "unit", "error") if k in r}
+    r = run(run_serve, "serve_light", precision="tc64", burst=True)
+    out["serve_light_tc64_burst"] = {
+        "served_requests_per_s": r.get("served", {}).get("requests_per_s"),
+        "plain_requests_per_s": r.get("per_request_plain_launches", {}).get("requests_per_s"),
+        "throughput_ratio_vs_plain": r.get("throughput_ratio_vs_plain"),
+        "served_p50_p99_ms": [r.get("served", {}).get("p50_ms"), r.get("served", {}).get("p99_ms")],
+        "plain_p50_p99_ms": [r.get("per_request_plain_launches", {}).get("p50_ms"),
+                             r.get("per_request_plain_launches", {}).get("p99_ms")],
+        "results_identical_alone_and_in_mix": r.get("results_identical_alone_and_in_mix"),
+        **({"error": r["error"]} if "error" in r else {})}
+    return out
 
 
 def gram_config(w, world, precision):
@@ -562,6 +608,8 @@ def run_ours(args, w):
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu
+        if world == 1 and not args.no_other_workloads:
+            line["other_workloads"] = other_workloads(args)
         if world == 1 and not args.no_reference_gpu:
             # the reference's own Numba GPU path on the same inputs, timed after (outside) our timed region
             r = measure_reference_gpu(w, steps=3, warmup=2, accuracy=False)
