@@ -150,92 +150,6 @@ __device__ __forceinline__ T pick_row(const T (&left)[R], int rstar)
     return v;
 }
 
-template <typename T, int R, int O, int D>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) stream_reg_kernel(StreamParams p)
-{
-    using BS = BlockShape<R, O>;
-    constexpr int C = BS::C;
-    constexpr int RC = BS::RC;
-    const int lane = threadIdx.x & 31;
-    const int wib = threadIdx.x >> 5;
-    const int64_t gwarp = (int64_t)blockIdx.x * kWarpsPerBlock + wib;
-    const int64_t first = gwarp * p.per_warp;
-    if (first >= p.nitems) return; // warp-uniform
-    const int cnt = (int)((p.nitems - first) < p.per_warp ? (p.nitems - first) : p.per_warp);
-    const T *dX = reinterpret_cast<const T *>(p.dx);
-    const T *dY = reinterpret_cast<const T *>(p.dy);
-    const int ncx = (int)p.ncx, ncy = (int)p.ncy;
-    const int n = ncx << p.order;
-    const int nsteps = (ncy << p.order) / C;
-    const int ci0 = (lane * R) >> p.order; // first coarse row of this lane
-    const int lstar = (n - 1) / R, rstar = (n - 1) % R;
-
-    T dx[RC][D];
-    int64_t cur_x = -1;
-    T left[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) left[r] = T(1);
-    T bot[C];
-#pragma unroll
-    for (int c = 0; c < C; ++c) bot[c] = T(1);
-    T corner_next = T(1);
-    int q = 0, k = 0;
-    int64_t item = first, xi = 0, yj = 0;
-    const T *dyp = dY;
-
-    const int total = cnt * nsteps + 31;
-    for (int s = 0; s < total; ++s) {
-        T top[C];
-#pragma unroll
-        for (int c = 0; c < C; ++c) top[c] = __shfl_up_sync(kFullMask, bot[c], 1);
-        if (lane == 0) {
-#pragma unroll
-            for (int c = 0; c < C; ++c) top[c] = T(1);
-        }
-        if (s >= lane && k < cnt) {
-            if (q == 0) { // this lane starts pair `first + k`
-                item = first + k;
-                stream_decode(p, item, xi, yj);
-                dyp = dY + yj * (int64_t)D * ncy;
-                if (xi != cur_x) {
-                    cur_x = xi;
-                    const T *src = dX + xi * (int64_t)D * ncx;
-#pragma unroll
-                    for (int rc = 0; rc < RC; ++rc) {
-                        const int ci = ci0 + (RC > 1 ? rc : 0);
-#pragma unroll
-                        for (int kk = 0; kk < D; ++kk) dx[rc][kk] = (ci < ncx) ? src[kk * ncx + ci] : T(0);
-                    }
-                }
-#pragma unroll
-                for (int r = 0; r < R; ++r) left[r] = T(1);
-            }
-            const T corner = (q == 0) ? T(1) : corner_next;
-            corner_next = top[C - 1];
-            const int cj = (O <= 3) ? q : ((q * C) >> p.order); // C = 2^order when order <= 3
-            T cc[RC];
-#pragma unroll
-            for (int rc = 0; rc < RC; ++rc) cc[rc] = T(0);
-            const T *dyr = dyp + cj;
-#pragma unroll
-            for (int kk = 0; kk < D; ++kk) {
-                const T dy = dyr[kk * ncy];
-#pragma unroll
-                for (int rc = 0; rc < RC; ++rc) cc[rc] = fma(dx[rc][kk], dy, cc[rc]);
-            }
-            T A[RC], B[RC];
-#pragma unroll
-            for (int rc = 0; rc < RC; ++rc) stencil_coefs(cc[rc], A[rc], B[rc]);
-            stream_block<T, R, O>(left, top, corner, A, B, bot);
-            if (q == nsteps - 1 && lane == lstar) stream_store(p, item, xi, yj, pick_row(left, rstar));
-            if (++q == nsteps) {
-                q = 0;
-                ++k;
-            }
-        }
-    }
-}
-
 // Paired float32 cells.  A float32 lane of stream_reg_kernel is issue-bound
 // (5 float32 instructions per cell plus the per-step shuffles and loads), so
 // here each lane advances two pairs at once and every cell operation is one
@@ -400,6 +314,135 @@ __device__ __forceinline__ Dbl2 stencil_cell<Dbl2>(Dbl2 k00, Dbl2 k01, Dbl2 k10,
     return Dbl2{stencil_cell<double>(k00.x, k01.x, k10.x, A.x, B.x), stencil_cell<double>(k00.y, k01.y, k10.y, A.y, B.y)};
 }
 
+// Increments one step ahead (stream_reg_kernel, stream_reg_dual_kernel).  A
+// step's increments take D loads of dy and RC x D dependent fma chains; formed
+// at the start of the step, they put a load latency and D fmas on the critical
+// path ahead of the first cell.  So a lane forms the increments of its NEXT
+// step (the same fma chains, bitwise) in the same basic block as the current
+// step's cells, where the loads and dot products, which do not depend on the
+// cells, fill the cells' latency gaps (Gram 256 x 256, L = 128, d = 8, order
+// 2: 5.13 ms against 5.31 ms with the increments formed in-step).  The next
+// entry of the run is decoded one entry ahead, when the current one starts;
+// when it has another x path, the dot products formed with the old dx are
+// discarded and redone after the dx reload (rare: a run moves to a new x path
+// at most a few times).
+template <typename T, int D, int RC>
+__device__ __forceinline__ void stream_dot(const T (&dx)[RC][D], const T *dyr, int64_t ncy, T (&cc)[RC])
+{
+#pragma unroll
+    for (int rc = 0; rc < RC; ++rc) cc[rc] = T(0);
+#pragma unroll
+    for (int kk = 0; kk < D; ++kk) {
+        const T dy = dyr[kk * ncy];
+#pragma unroll
+        for (int rc = 0; rc < RC; ++rc) cc[rc] = fma(dx[rc][kk], dy, cc[rc]);
+    }
+}
+
+template <typename T, int D, int RC>
+__device__ __forceinline__ void stream_load_dx(const T *dX, int64_t xi, int ncx, int ci0, T (&dx)[RC][D])
+{
+    const T *src = dX + xi * (int64_t)D * ncx;
+#pragma unroll
+    for (int rc = 0; rc < RC; ++rc) {
+        const int ci = ci0 + (RC > 1 ? rc : 0);
+#pragma unroll
+        for (int kk = 0; kk < D; ++kk) dx[rc][kk] = (ci < ncx) ? src[kk * ncx + ci] : T(0);
+    }
+}
+
+// Three CTAs (12 warps) per SM, except for blocks of 8 or more coarse rows a lane,
+// whose coefficient arrays need more than 168 registers.
+template <typename T, int R, int O, int D>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, (BlockShape<R, O>::RC >= 8 ? 2 : 3))
+    stream_reg_kernel(StreamParams p)
+{
+    using BS = BlockShape<R, O>;
+    constexpr int C = BS::C;
+    constexpr int RC = BS::RC;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int64_t gwarp = (int64_t)blockIdx.x * kWarpsPerBlock + wib;
+    const int64_t first = gwarp * p.per_warp;
+    if (first >= p.nitems) return; // warp-uniform
+    const int cnt = (int)((p.nitems - first) < p.per_warp ? (p.nitems - first) : p.per_warp);
+    const T *dX = reinterpret_cast<const T *>(p.dx);
+    const T *dY = reinterpret_cast<const T *>(p.dy);
+    const int ncx = (int)p.ncx, ncy = (int)p.ncy;
+    const int n = ncx << p.order;
+    const int nsteps = (ncy << p.order) / C;
+    const int ci0 = (lane * R) >> p.order;
+    const int lstar = (n - 1) / R, rstar = (n - 1) % R;
+    const int64_t ystride = (int64_t)D * ncy;
+
+    // the entry being solved and the next one of the run (decoded when the current one starts)
+    int64_t item = first, xi = 0, yj = 0;
+    int64_t nxi, nyj;
+    stream_decode(p, first, nxi, nyj);
+    const T *dyp = dY + nyj * ystride, *ndyp = dyp;
+    T dx[RC][D];
+    int64_t cur_x = nxi;
+    stream_load_dx<T, D, RC>(dX, nxi, ncx, ci0, dx);
+    T cc[RC]; // increments of this lane's next step
+    stream_dot<T, D, RC>(dx, dyp, ncy, cc);
+
+    T left[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) left[r] = T(1);
+    T bot[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) bot[c] = T(1);
+    T corner_next = T(1);
+    int q = 0, k = 0;
+
+    const int total = cnt * nsteps + 31;
+    for (int s = 0; s < total; ++s) {
+        T top[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) top[c] = __shfl_up_sync(kFullMask, bot[c], 1);
+        if (lane == 0) {
+#pragma unroll
+            for (int c = 0; c < C; ++c) top[c] = T(1);
+        }
+        if (s >= lane && k < cnt) {
+            if (q == 0) { // this lane starts entry `first + k`, decoded at the previous start
+                item = first + k;
+                xi = nxi;
+                yj = nyj;
+                dyp = ndyp;
+                if (xi != cur_x) { // the ahead increments used the previous x path's dx
+                    cur_x = xi;
+                    stream_load_dx<T, D, RC>(dX, xi, ncx, ci0, dx);
+                    stream_dot<T, D, RC>(dx, dyp, ncy, cc);
+                }
+                if (k + 1 < cnt) {
+                    stream_decode(p, item + 1, nxi, nyj);
+                    ndyp = dY + nyj * ystride;
+                }
+#pragma unroll
+                for (int r = 0; r < R; ++r) left[r] = T(1);
+            }
+            const T corner = (q == 0) ? T(1) : corner_next;
+            corner_next = top[C - 1];
+            T A[RC], B[RC];
+#pragma unroll
+            for (int rc = 0; rc < RC; ++rc) stencil_coefs(cc[rc], A[rc], B[rc]);
+            // the next step: q + 1 of this entry, or step 0 of the next one
+            const int qn = (q + 1 == nsteps) ? 0 : q + 1;
+            const int cjn = (O <= 3) ? qn : ((qn * C) >> p.order);
+            stream_dot<T, D, RC>(dx, ((qn == 0) ? ndyp : dyp) + cjn, ncy, cc);
+            stream_block<T, R, O>(left, top, corner, A, B, bot);
+            if (q == nsteps - 1 && lane == lstar) stream_store(p, item, xi, yj, pick_row(left, rstar));
+            if (++q == nsteps) {
+                q = 0;
+                ++k;
+            }
+        }
+    }
+}
+
+// Two entries of one x path per lane, increments one step ahead as in
+// stream_reg_kernel.
 template <int R, int O, int D>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) stream_reg_dual_kernel(StreamParams p)
 {
@@ -420,10 +463,30 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) stream_reg_dual_kernel
     const int ci0 = (lane * R) >> p.order;
     const int lstar = (n - 1) / R, rstar = (n - 1) % R;
     const int64_t hy = (p.ny + 1) >> 1;
+    const int64_t ystride = (int64_t)D * ncy;
     const Dbl2 one{1.0, 1.0};
 
+    // entry pair t -> x path t / hy, y paths ya = 2 (t % hy) and ya + 1 (absent when ya + 1 == ny)
+    auto decode = [&](int64_t t, int64_t &x, int64_t &ya, bool &hasb, const double *&pa, const double *&pb) {
+        x = t / hy;
+        ya = 2 * (t - x * hy);
+        hasb = ya + 1 < p.ny;
+        pa = dY + ya * ystride;
+        pb = hasb ? pa + ystride : pa;
+    };
+    int64_t xi = 0, ya = 0, nxi, nya;
+    bool hasb = false, nhasb;
+    const double *dypa, *dypb, *ndypa, *ndypb;
+    decode(first, nxi, nya, nhasb, ndypa, ndypb);
+    dypa = ndypa;
+    dypb = ndypb;
     double dx[RC][D];
-    int64_t cur_x = -1;
+    int64_t cur_x = nxi;
+    stream_load_dx<double, D, RC>(dX, nxi, ncx, ci0, dx);
+    double cca[RC], ccb[RC]; // increments of this lane's next step, entries a and b
+    stream_dot<double, D, RC>(dx, dypa, ncy, cca);
+    stream_dot<double, D, RC>(dx, dypb, ncy, ccb);
+
     Dbl2 left[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) left[r] = one;
@@ -432,9 +495,6 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) stream_reg_dual_kernel
     for (int c = 0; c < C; ++c) bot[c] = one;
     Dbl2 corner_next = one;
     int q = 0, k = 0;
-    int64_t xi = 0, ya = 0;
-    bool hasb = false;
-    const double *dypa = dY, *dypb = dY;
 
     const int total = cnt * nsteps + 31;
     for (int s = 0; s < total; ++s) {
@@ -449,46 +509,31 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) stream_reg_dual_kernel
             for (int c = 0; c < C; ++c) top[c] = one;
         }
         if (s >= lane && k < cnt) {
-            if (q == 0) { // this lane starts entries (xi, ya), (xi, ya + 1)
-                const int64_t t = first + k;
-                xi = t / hy;
-                ya = 2 * (t - xi * hy);
-                hasb = ya + 1 < p.ny;
-                dypa = dY + ya * (int64_t)D * ncy;
-                dypb = hasb ? dypa + (int64_t)D * ncy : dypa;
-                if (xi != cur_x) {
+            if (q == 0) { // this lane starts entry pair `first + k`, decoded at the previous start
+                xi = nxi;
+                ya = nya;
+                hasb = nhasb;
+                dypa = ndypa;
+                dypb = ndypb;
+                if (xi != cur_x) { // the ahead increments used the previous x path's dx
                     cur_x = xi;
-                    const double *src = dX + xi * (int64_t)D * ncx;
-#pragma unroll
-                    for (int rc = 0; rc < RC; ++rc) {
-                        const int ci = ci0 + (RC > 1 ? rc : 0);
-#pragma unroll
-                        for (int kk = 0; kk < D; ++kk) dx[rc][kk] = (ci < ncx) ? src[kk * ncx + ci] : 0.0;
-                    }
+                    stream_load_dx<double, D, RC>(dX, xi, ncx, ci0, dx);
+                    stream_dot<double, D, RC>(dx, dypa, ncy, cca);
+                    stream_dot<double, D, RC>(dx, dypb, ncy, ccb);
                 }
+                if (k + 1 < cnt) decode(first + k + 1, nxi, nya, nhasb, ndypa, ndypb);
 #pragma unroll
                 for (int r = 0; r < R; ++r) left[r] = one;
             }
             const Dbl2 corner = (q == 0) ? one : corner_next;
             corner_next = top[C - 1];
-            const int cj = (O <= 3) ? q : ((q * C) >> p.order);
-            Dbl2 cc[RC];
-#pragma unroll
-            for (int rc = 0; rc < RC; ++rc) cc[rc] = Dbl2{0.0, 0.0};
-            const double *dyra = dypa + cj;
-            const double *dyrb = dypb + cj;
-#pragma unroll
-            for (int kk = 0; kk < D; ++kk) {
-                const double da = dyra[kk * ncy], db = dyrb[kk * ncy];
-#pragma unroll
-                for (int rc = 0; rc < RC; ++rc) {
-                    cc[rc].x = fma(dx[rc][kk], da, cc[rc].x);
-                    cc[rc].y = fma(dx[rc][kk], db, cc[rc].y);
-                }
-            }
             Dbl2 A[RC], B[RC];
 #pragma unroll
-            for (int rc = 0; rc < RC; ++rc) stencil_coefs(cc[rc], A[rc], B[rc]);
+            for (int rc = 0; rc < RC; ++rc) stencil_coefs(Dbl2{cca[rc], ccb[rc]}, A[rc], B[rc]);
+            const int qn = (q + 1 == nsteps) ? 0 : q + 1;
+            const int cjn = (O <= 3) ? qn : ((qn * C) >> p.order);
+            stream_dot<double, D, RC>(dx, ((qn == 0) ? ndypa : dypa) + cjn, ncy, cca);
+            stream_dot<double, D, RC>(dx, ((qn == 0) ? ndypb : dypb) + cjn, ncy, ccb);
             stream_block<Dbl2, R, O>(left, top, corner, A, B, bot);
             if (q == nsteps - 1 && lane == lstar) {
                 const Dbl2 v = pick_row(left, rstar);
