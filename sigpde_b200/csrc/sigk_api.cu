@@ -384,12 +384,12 @@ TcPlan make_tc_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, in
     return t;
 }
 
-// quad_rc > 0: the fused Gram's permuted A layout (TcImageParams::quad_rc)
+// fused_rc > 0: the fused Gram's permuted A layout (TcImageParams::fused_rc)
 int tc_image(bool in64, const void *x, int64_t npaths, int64_t len, int64_t d, int64_t rows_per_path, int64_t tile_rows,
-             int64_t ntiles, int kp, double f, const void *s, float *hi, float *lo, cudaStream_t stream, int quad_rc = 0)
+             int64_t ntiles, int kp, double f, const void *s, float *hi, float *lo, cudaStream_t stream, int fused_rc = 0)
 {
     TcImageParams ip{};
-    ip.quad_rc = quad_rc;
+    ip.fused_rc = fused_rc;
     ip.x = x;
     ip.npaths = npaths;
     ip.len = len;
@@ -576,7 +576,9 @@ int consume_matrix(const TcPlan &t, int op, const void *mat, bool mat64, int64_t
 
 // Fused tensor-core Gram (fused_tc.cuh): the tcgen05 increments go from TMEM
 // through shared memory to the wavefront, never to HBM.  Workspace: error word,
-// then the hi / lo operand images (128 rows per x path, T rows per y path).
+// then the hi / lo operand images (2 RC tiles of 128 rows per block of 8 x
+// paths, T rows per y path).
+constexpr size_t kFtMaxSmem = 227 * 1024; // the B200's per-block opt-in limit
 struct FtPlan {
     bool ok = false;
     int R = 0, O = 0, kp = 0, T = 0;
@@ -586,14 +588,15 @@ struct FtPlan {
 FtPlan make_fused_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, int64_t d, int order, int precision)
 {
     FtPlan f;
-    // opt-in (SIGK_FUSED_TC=1): measured slower than the two-phase route on every shape tried (TMEM holds
-    // at most 8 pair streams per SM; at low orders each chunk boundary's TMEM loads dominate)
-    if (op != kOpGram || precision != SIGK_PREC_TC64 || d > 16 || order > 3 || ncx > kTcM || !env_flag("SIGK_FUSED_TC"))
+    // opt-in (SIGK_FUSED_TC=1) until measured against the two-phase and float64 routes
+    if (op != kOpGram || precision != SIGK_PREC_TC64 || d > 16 || order > 3 || !env_flag("SIGK_FUSED_TC"))
         return f;
     const int64_t n = ncx << order;
     if (n > 32 * 16) return f; // one band
     const int R = pick_rows(n);
-    if ((R >> order) < 1 || ((R >> order) << order) != R || (R >> order) * 32 > kTcM) return f;
+    const int rc = R >> order;
+    if (rc < 1 || (rc << order) != R || rc > 4 || 32 * R < n) return f;
+    if (fused_tc_smem(rc, (int)((d + 7) / 8 * 8)) > kFtMaxSmem) return f;
     if (!get_fused_tc_kernel(R, order)) return f;
     f.ok = true;
     f.R = R;
@@ -602,7 +605,7 @@ FtPlan make_fused_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy,
     f.T = (int)((ncy + kFtChunk - 1) / kFtChunk * kFtChunk);
     f.err_off = 0;
     f.a_off = 256;
-    f.a_bytes = align256((size_t)((nx + 3) / 4) * (R >> order) * kTcM * f.kp * sizeof(float));
+    f.a_bytes = align256((size_t)((nx + 7) / 8) * 2 * rc * kTcM * f.kp * sizeof(float));
     f.b_off = f.a_off + 2 * f.a_bytes;
     f.b_bytes = align256((size_t)ny * f.T * f.kp * sizeof(float));
     f.ws_bytes = f.b_off + 2 * f.b_bytes;
@@ -623,7 +626,7 @@ int run_pairs_fused(const FtPlan &f, const void *x, const void *y, int64_t nx, i
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
     const double fs = static_scale * std::ldexp(1.0, -2 * order); // x side: static scale * 4^-order * scale_x
     const int rc = f.R >> f.O;
-    if ((st = tc_image(in64, x, nx, lx, d, kTcM, kTcM, (nx + 3) / 4 * rc, f.kp, fs, sx, a_hi, a_lo, stream, rc)))
+    if ((st = tc_image(in64, x, nx, lx, d, kTcM, kTcM, (nx + 7) / 8 * 2 * rc, f.kp, fs, sx, a_hi, a_lo, stream, rc)))
         return st;
     if ((st = tc_image(in64, y, ny, ly, d, f.T, f.T, ny, f.kp, 1.0, sy, b_hi, b_lo, stream))) return st;
     FusedTcFn fn = get_fused_tc_kernel(f.R, f.O);
@@ -658,8 +661,9 @@ int run_pairs_fused(const FtPlan &f, const void *x, const void *y, int64_t nx, i
     fp.ncy = (int)(ly - 1);
     fp.kp = f.kp;
     fp.T = f.T;
-    fp.ngroups = (nx + kFtWarps - 1) / kFtWarps * ny;
-    const int64_t cap = 2 * (int64_t)sm_count(); // two CTAs per SM (TMEM: 2 x 256 columns)
+    fp.hy = (ny + 1) / 2;
+    fp.ngroups = (nx + 7) / 8 * fp.hy;
+    const int64_t cap = (int64_t)sm_count(); // one CTA per SM (TMEM: up to 512 columns)
     const int64_t ctas0 = fp.ngroups < cap ? fp.ngroups : cap;
     fp.per_cta = (fp.ngroups + ctas0 - 1) / ctas0;
     const int64_t ctas = (fp.ngroups + fp.per_cta - 1) / fp.per_cta;
@@ -667,7 +671,7 @@ int run_pairs_fused(const FtPlan &f, const void *x, const void *y, int64_t nx, i
     fp.out = out;
     fp.out_ld = out_ld;
     fp.err = err;
-    fn<<<(unsigned)ctas, (kFtWarps + 1) * 32, smem, stream>>>(fp);
+    fn<<<(unsigned)ctas, kFtWarps * 32, smem, stream>>>(fp);
     count_launch();
     e = cudaGetLastError();
     return e == cudaSuccess ? SIGK_OK : cuda_fail(e, "fused tensor-core kernel launch");

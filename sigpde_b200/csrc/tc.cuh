@@ -63,9 +63,11 @@ struct TcImageParams {
     double f;              // scale f * s[p]
     const void *s;         // per-path scale in TIN or null
     float *hi, *lo;
-    // quad_rc > 0: the fused Gram's A layout (fused_tc.cuh).  Blocks of 4 x paths, each block quad_rc
-    // tiles of 128 rows; in tile k of block a, row 32 w + i holds coarse row quad_rc * i + k of path 4a + w
-    int quad_rc;
+    // fused_rc > 0: the fused Gram's A layout (fused_tc.cuh).  Blocks of 8 x paths, each 2 fused_rc tiles
+    // of 128 rows, LO tiles (f = 0) then HI tiles (f = 1): tile f fused_rc + k.  Row 32 q + t of tile
+    // (f, k) holds coarse row fused_rc lam + k of path 8 a + 4 h + q, where lam = 16 f + t % 16 is
+    // the wavefront lane and h = (t / 16) xor f the warp set that owns the row.
+    int fused_rc;
 };
 
 // Image layout (group-major): element (row m, k) sits at float offset
@@ -100,10 +102,12 @@ __global__ void tc_image_kernel(TcImageParams p)
         const int64_t m = g * 8 + r8;
         const int64_t k = kc * 4 + k4;
         int64_t path, c;
-        if (p.quad_rc > 0) {
-            const int64_t per_block = (int64_t)p.quad_rc * 128, rem = m % per_block;
-            path = 4 * (m / per_block) + (rem >> 5 & 3);
-            c = (int64_t)p.quad_rc * (rem & 31) + rem / 128;
+        if (p.fused_rc > 0) {
+            const int64_t per_block = (int64_t)p.fused_rc * 256, rem = m % per_block;
+            const int64_t tile = rem >> 7, fam = tile / p.fused_rc, tk = tile - fam * p.fused_rc;
+            const int64_t t = rem & 31, h = (t >> 4) ^ fam, lam = 16 * fam + (t & 15);
+            path = 8 * (m / per_block) + 4 * h + (rem >> 5 & 3);
+            c = (int64_t)p.fused_rc * lam + tk;
         } else {
             path = m / p.rows_per_path;
             c = m - path * p.rows_per_path;
@@ -278,6 +282,26 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32])
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
     for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+// Two 16-column loads of the warp's lane quarter (32x32b.x16 each) and one wait.
+__device__ __forceinline__ void tmem_ld16x2(uint32_t ta, uint32_t tb, uint32_t (&a)[16], uint32_t (&b)[16])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                 "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+                 : "=r"(a[0]), "=r"(a[1]), "=r"(a[2]), "=r"(a[3]), "=r"(a[4]), "=r"(a[5]), "=r"(a[6]), "=r"(a[7]),
+                   "=r"(a[8]), "=r"(a[9]), "=r"(a[10]), "=r"(a[11]), "=r"(a[12]), "=r"(a[13]), "=r"(a[14]),
+                   "=r"(a[15])
+                 : "r"(ta)
+                 : "memory");
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                 "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+                 : "=r"(b[0]), "=r"(b[1]), "=r"(b[2]), "=r"(b[3]), "=r"(b[4]), "=r"(b[5]), "=r"(b[6]), "=r"(b[7]),
+                   "=r"(b[8]), "=r"(b[9]), "=r"(b[10]), "=r"(b[11]), "=r"(b[12]), "=r"(b[13]), "=r"(b[14]),
+                   "=r"(b[15])
+                 : "r"(tb)
+                 : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
 // ------------------------------------------------------------------ GEMM

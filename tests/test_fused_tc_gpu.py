@@ -1,15 +1,17 @@
 """The fused tensor-core Gram (fused_tc.cuh): tcgen05 increments handed from
 TMEM through shared memory to the wavefront, no increment matrix in HBM.
 
-The route is opt-in (SIGK_FUSED_TC=1; it measured slower than the two-phase
-route).  Its arithmetic is the two-phase path's (tc_gemm_kernel writing the
-float32 increment matrix, stream_inc_kernel reading it): the same split-TF32
-MMAs per increment and the same float64 cells, so the results must be bitwise
-equal to that path.  Against the float64 oracle the
-tc64 bound applies: error normalised by sqrt(k(x,x) k(y,y)) at most 1e-5.
-Shapes cover every instantiated (rows per lane, order), time lines padded to
-16 columns, a last block of fewer than 4 y paths, fewer groups than CTAs,
-scales, float64 inputs and dimensions 1..16.
+SIGK_FUSED_TC=1 selects the route here.  Its arithmetic is the two-phase
+path's (tc_gemm_kernel writing the float32 increment matrix, stream_inc_kernel
+reading it): the same split-TF32 MMAs per increment and the same float64
+cells, so the results must be bitwise equal to that path.  Against the float64
+oracle the tc64 bound applies: error normalised by sqrt(k(x,x) k(y,y)) at most
+1e-5.  Shapes cover every instantiated (rows per lane, order), time lines
+padded to 16 columns, odd numbers of x and y paths (a last x block of fewer
+than 8 paths, a last y pair of one path), fewer groups than CTAs, runs that
+cross x blocks (the A operand restaged mid-run), scales, float64 inputs and
+dimensions 1..16.  Each case first checks that the fused route is the one
+taken (its workspace has no increment matrix).
 """
 import numpy as np
 import pytest
@@ -30,7 +32,19 @@ SHAPES = [
     (3, 2, 30, 18, 1, 2),       # 116 rows: 4 a lane at order 2 (1 coarse row); 1 group
     (33, 3, 17, 129, 16, 0),    # one y block of 3 paths, ncy = 128
     (4, 9, 66, 64, 8, 2),       # 260 rows: 16 a lane, 4 coarse rows (one row of padding)
+    (64, 81, 40, 35, 4, 1),     # 328 groups on 148 CTAs: runs cross x blocks; last y pair of one path
 ]
+
+
+def _fused_taken(monkeypatch, nx, ny, lx, ly, d, o, in64):
+    from sigpde_b200 import _lib
+    lib = _lib.lib()
+    dt = _lib.SIGK_F64 if in64 else _lib.SIGK_F32
+    monkeypatch.setenv("SIGK_FUSED_TC", "1")
+    fused = lib.sigk_workspace_size(_lib.SIGK_OP_GRAM, nx, ny, lx, ly, d, o, dt, _lib.SIGK_PREC_TC64)
+    monkeypatch.delenv("SIGK_FUSED_TC", raising=False)
+    two = lib.sigk_workspace_size(_lib.SIGK_OP_GRAM, nx, ny, lx, ly, d, o, dt, _lib.SIGK_PREC_TC64)
+    return fused != two
 
 
 def host(t):
@@ -47,6 +61,7 @@ def sig():
 @pytest.mark.parametrize("in64", [False, True])
 def test_fused_equals_two_phase_and_oracle(sig, oracle, monkeypatch, shape, in64):
     nx, ny, lx, ly, d, o = shape
+    assert _fused_taken(monkeypatch, nx, ny, lx, ly, d, o, in64)
     dt = torch.float64 if in64 else torch.float32
     X = torch.tensor(oracle.brownian(nx, lx, d, 1000 + lx), dtype=dt, device="cuda")
     Y = torch.tensor(oracle.brownian(ny, ly, d, 2000 + ly), dtype=dt, device="cuda")
@@ -84,3 +99,28 @@ def test_fused_route_is_taken_and_small(sig):
         os.environ.pop("SIGK_FUSED_TC", None)
     two = lib.sigk_workspace_size(_lib.SIGK_OP_GRAM, 256, 256, 128, 128, 8, 2, _lib.SIGK_F32, _lib.SIGK_PREC_TC64)
     assert fused < 8 << 20 < (1 << 30) < two
+
+
+def test_fused_config2_size(sig, oracle, monkeypatch):
+    """The full 256 x 256 Gram at L = 128, d = 8, order 2 (28 groups per CTA,
+    each run crossing an x block): bitwise the two-phase result, and 16 sampled
+    entries within the tc64 bound of the float64 oracle."""
+    X = torch.tensor(oracle.brownian(256, 128, 8, 1), dtype=torch.float32, device="cuda")
+    Y = torch.tensor(oracle.brownian(256, 128, 8, 2), dtype=torch.float32, device="cuda")
+    assert _fused_taken(monkeypatch, 256, 256, 128, 128, 8, 2, False)
+    k = sig.SigPDE(sig.kernels.LinearKernel(), 2, precision="tc64")
+    monkeypatch.setenv("SIGK_FUSED_TC", "1")
+    fused = k.gram(X, Y)
+    monkeypatch.delenv("SIGK_FUSED_TC", raising=False)
+    two = k.gram(X, Y)
+    torch.cuda.synchronize()
+    assert torch.equal(fused, two)
+    G = host(fused)
+    x, y = host(X), host(Y)
+    rng = np.random.default_rng(3)
+    flat = rng.choice(256 * 256, 16, replace=False)
+    want = oracle.gram(x, y, 2, pairs=flat)
+    i, j = flat // 256, flat % 256
+    kxx = oracle.pairwise(x[i], None, 2)
+    kyy = oracle.pairwise(y[j], None, 2)
+    assert float(np.max(np.abs(G.reshape(-1)[flat] - want) / np.sqrt(kxx * kyy))) <= CS_TC64
