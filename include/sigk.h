@@ -40,7 +40,14 @@
  *                   precision.  The workspace holds
  *                   the increment matrix: up to 6 GiB per call (the x paths
  *                   are processed in chunks beyond that; SIGK_TC_CHUNK_MB
- *                   sets the chunk size).
+ *                   sets the chunk size).  Exception: sigk_gram with TC64 at
+ *                   order 2 or 3, x paths of one band and dim <= 8 (<= 16 at
+ *                   up to 2 coarse rows a lane) runs one fused kernel that
+ *                   hands the increments from TMEM through shared memory to
+ *                   the wavefront; its workspace holds only the operand
+ *                   images, and its results are bitwise those of the
+ *                   matrix route (SIGK_FUSED_TC=1: also at orders 0-1;
+ *                   SIGK_FUSED_TC=0: never).
  */
 #ifndef SIGK_H_
 #define SIGK_H_

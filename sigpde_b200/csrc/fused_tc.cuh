@@ -239,8 +239,8 @@ struct FtIssuer {
     }
 };
 
-// A thread's RC increments of one y path from its ring slot (16-, 8- or
-// 4-byte loads).
+// A thread's RC increments of one y path from its ring slot, and its RC values
+// of one chunk column into a ring slot (16-, 8- or 4-byte accesses).
 template <int RC>
 __device__ __forceinline__ void ft_ring_read(const float *src, float (&c)[RC])
 {
@@ -259,6 +259,17 @@ __device__ __forceinline__ void ft_ring_read(const float *src, float (&c)[RC])
     }
 }
 
+template <int RC>
+__device__ __forceinline__ void ft_ring_write(float *dst, const float (&v)[RC][kFtChunk], int c)
+{
+    if constexpr (RC == 4)
+        *reinterpret_cast<float4 *>(dst) = make_float4(v[0][c], v[1][c], v[2][c], v[3][c]);
+    else if constexpr (RC == 2)
+        *reinterpret_cast<float2 *>(dst) = make_float2(v[0][c], v[1][c]);
+    else
+        dst[0] = v[0][c];
+}
+
 template <int R, int O>
 __global__ void __launch_bounds__(kFtWarps * 32, 1) fused_tc_kernel(FusedTcParams p)
 {
@@ -273,7 +284,6 @@ __global__ void __launch_bounds__(kFtWarps * 32, 1) fused_tc_kernel(FusedTcParam
     const int h = warp >> 2, q = warp & 3;
     const int lam = h ? ((lane + 16) & 31) : lane; // the wavefront lane this thread plays
     const int ii = lam & 15;                       // its skew within its half
-    const bool mine_lo = lam < 16;                 // its increments come from the LO family
     const int64_t g0 = (int64_t)blockIdx.x * p.per_cta;
     if (g0 >= p.ngroups) return; // CTA-uniform, before anything is allocated
     const int64_t ng = (p.ngroups - g0) < p.per_cta ? (p.ngroups - g0) : p.per_cta;
@@ -344,14 +354,23 @@ __global__ void __launch_bounds__(kFtWarps * 32, 1) fused_tc_kernel(FusedTcParam
     const uint32_t tq = tmem + ((uint32_t)(q * 32) << 16); // this warp's TMEM lane quarter
     const uint32_t arrive_addr = smem_u32(&st->arrive[0]);
 
-    // Boundary kb: chunk kb's MMAs are done; the thread's increments for steps [16 kb, 16 kb + 16) come from
-    // chunks kb - 1 and kb (column c of chunk a is its step 16 a + c + ii); then the arrival, and the last
-    // arrival issues chunk kb + 1 into the TMEM slot of chunk kb - 1.  Arrivals are totally ordered by
-    // boundary (a warp passes boundary kb + 1 only after chunk kb + 1 was issued), so the arrival at
-    // boundary kb that returns 8 (kb + 1) - 1 is its last.
+    // Boundary kb: chunk kb's MMAs are done; the increments for steps [16 kb, 16 kb + 16) come from chunks
+    // kb - 1 and kb (column c of chunk a is step 16 a + c + ii of the thread that plays the row's lane).
+    // The two warps of a lane quarter share the work: set 0 loads the LO family, set 1 the HI family, and
+    // thread t writes the value of TMEM lane 32 q + t into the ring of the warp that owns the row (its own
+    // for t < 16, its partner's for t >= 16; thread t of either warp plays a lane congruent to t mod 16,
+    // so the ring offset and the skew ii are the same).  A 64-thread barrier of the pair before the copy
+    // (both warps are done reading the previous period's slots) and one after it (the slots are written)
+    // orders the cross-warp stores.  Then the arrival, and the last arrival issues chunk kb + 1 into the
+    // TMEM slot of chunk kb - 1.  Arrivals are totally ordered by boundary once past boundary 1 (a warp
+    // passes boundary kb + 1 only after chunk kb + 1 was issued), so the arrival that brings the count to
+    // 8 (kb + 1) is the last one of boundary kb.
+    float *dstring = lane < 16 ? myring : myring + (h ? -4 : 4) * kFtRing * kSlotF; // the row owner's ring
+    const int pair_bar = 1 + q; // named barrier of warps q and q + 4
     auto boundary = [&](int64_t kb) {
         if (!*cta_err && !mbar_wait(bar_mma + 8 * (uint32_t)(kb & 1), (uint32_t)((kb >> 1) & 1))) *cta_err = 1;
         tc_fence_after();
+        named_bar(pair_bar, 64);
         // tcgen05.ld is warp-collective: decide for the whole warp (another thread may set the flag)
         if (!__any_sync(kFullMask, *cta_err != 0)) {
 #pragma unroll 1
@@ -359,21 +378,36 @@ __global__ void __launch_bounds__(kFtWarps * 32, 1) fused_tc_kernel(FusedTcParam
                 const int base = (int)(kFtChunk * (a - kb)) + ii;
 #pragma unroll 1
                 for (int r = 0; r < 2; ++r) {
+                    float v[RC][kFtChunk]; // TMEM lane 32 q + lane of this warp's family, all RC tiles
+                    const uint32_t col = (uint32_t)((a & 1) * 64 * RC + r * 32 * RC + h * 16 * RC);
 #pragma unroll
-                    for (int t = 0; t < RC; ++t) {
-                        const uint32_t col = (uint32_t)((a & 1) * 64 * RC + r * 32 * RC + t * 16);
-                        uint32_t vl[16], vh[16];
-                        tmem_ld16x2(tq + col, tq + col + 16 * RC, vl, vh);
+                    for (int t = 0; t < RC; t += 2) {
+                        if constexpr (RC == 1) {
+                            uint32_t u[16], w[16];
+                            tmem_ld16x2(tq + col, tq + col, u, w);
 #pragma unroll
-                        for (int c = 0; c < kFtChunk; ++c) {
-                            const int j = base + c;
-                            if ((unsigned)j < (unsigned)kFtRing)
-                                myring[j * kSlotF + r * 32 * RC + t] = __uint_as_float(mine_lo ? vl[c] : vh[c]);
+                            for (int c = 0; c < kFtChunk; ++c) v[0][c] = __uint_as_float(u[c]);
+                        } else {
+                            uint32_t u[16], w[16];
+                            tmem_ld16x2(tq + col + t * 16, tq + col + (t + 1) * 16, u, w);
+#pragma unroll
+                            for (int c = 0; c < kFtChunk; ++c) {
+                                v[t][c] = __uint_as_float(u[c]);
+                                v[t + 1][c] = __uint_as_float(w[c]);
+                            }
                         }
+                    }
+                    // one RC-float store per ring slot; a thread's slots are RC-float aligned and the slot
+                    // stride is a multiple of 32 banks, so the warp's stores are conflict-free
+#pragma unroll
+                    for (int c = 0; c < kFtChunk; ++c) {
+                        const int j = base + c;
+                        if ((unsigned)j < (unsigned)kFtRing) ft_ring_write<RC>(dstring + j * kSlotF + r * 32 * RC, v, c);
                     }
                 }
             }
         }
+        named_bar(pair_bar, 64);
         tc_fence_before();
         __syncwarp();
         if (lane == 0) {

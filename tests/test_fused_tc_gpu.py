@@ -1,7 +1,9 @@
 """The fused tensor-core Gram (fused_tc.cuh): tcgen05 increments handed from
 TMEM through shared memory to the wavefront, no increment matrix in HBM.
 
-SIGK_FUSED_TC=1 selects the route here.  Its arithmetic is the two-phase
+The route is the default for tc64 Grams of order >= 2 where it applies;
+SIGK_FUSED_TC=1 takes it at every order and SIGK_FUSED_TC=0 never, which is
+how these tests choose the two routes.  Its arithmetic is the two-phase
 path's (tc_gemm_kernel writing the float32 increment matrix, stream_inc_kernel
 reading it): the same split-TF32 MMAs per increment and the same float64
 cells, so the results must be bitwise equal to that path.  Against the float64
@@ -42,7 +44,7 @@ def _fused_taken(monkeypatch, nx, ny, lx, ly, d, o, in64):
     dt = _lib.SIGK_F64 if in64 else _lib.SIGK_F32
     monkeypatch.setenv("SIGK_FUSED_TC", "1")
     fused = lib.sigk_workspace_size(_lib.SIGK_OP_GRAM, nx, ny, lx, ly, d, o, dt, _lib.SIGK_PREC_TC64)
-    monkeypatch.delenv("SIGK_FUSED_TC", raising=False)
+    monkeypatch.setenv("SIGK_FUSED_TC", "0")
     two = lib.sigk_workspace_size(_lib.SIGK_OP_GRAM, nx, ny, lx, ly, d, o, dt, _lib.SIGK_PREC_TC64)
     return fused != two
 
@@ -70,7 +72,7 @@ def test_fused_equals_two_phase_and_oracle(sig, oracle, monkeypatch, shape, in64
     for scales in ((None, None), (sx, None)):
         monkeypatch.setenv("SIGK_FUSED_TC", "1")
         fused = k.gram(X, Y, *scales)
-        monkeypatch.delenv("SIGK_FUSED_TC", raising=False)
+        monkeypatch.setenv("SIGK_FUSED_TC", "0")
         two = k.gram(X, Y, *scales)
         torch.cuda.synchronize()
         assert torch.equal(fused, two), f"{shape} in64={in64} scaled={scales[0] is not None}"
@@ -85,20 +87,22 @@ def test_fused_equals_two_phase_and_oracle(sig, oracle, monkeypatch, shape, in64
 
 
 def test_fused_route_is_taken_and_small(sig):
-    """The fused route's workspace holds only the operand images (no increment
-    matrix): 256 x 256 paths of length 128 in 8 dims need ~2.2 MB, against
-    4.26 GB for the two-phase matrix."""
+    """By default a tc64 Gram at order 2 takes the fused route, whose workspace
+    holds only the operand images (no increment matrix): 256 x 256 paths of
+    length 128 in 8 dims need ~4 MB, against 4.26 GB for the two-phase matrix."""
     import os
     from sigpde_b200 import _lib
     lib = _lib.lib()
-    os.environ["SIGK_FUSED_TC"] = "1"
+    os.environ.pop("SIGK_FUSED_TC", None)
+    default = lib.sigk_workspace_size(_lib.SIGK_OP_GRAM, 256, 256, 128, 128, 8, 2, _lib.SIGK_F32,
+                                      _lib.SIGK_PREC_TC64)
+    os.environ["SIGK_FUSED_TC"] = "0"
     try:
-        fused = lib.sigk_workspace_size(_lib.SIGK_OP_GRAM, 256, 256, 128, 128, 8, 2, _lib.SIGK_F32,
-                                        _lib.SIGK_PREC_TC64)
+        two = lib.sigk_workspace_size(_lib.SIGK_OP_GRAM, 256, 256, 128, 128, 8, 2, _lib.SIGK_F32,
+                                      _lib.SIGK_PREC_TC64)
     finally:
         os.environ.pop("SIGK_FUSED_TC", None)
-    two = lib.sigk_workspace_size(_lib.SIGK_OP_GRAM, 256, 256, 128, 128, 8, 2, _lib.SIGK_F32, _lib.SIGK_PREC_TC64)
-    assert fused < 8 << 20 < (1 << 30) < two
+    assert default < 8 << 20 < (1 << 30) < two
 
 
 def test_fused_config2_size(sig, oracle, monkeypatch):
@@ -111,7 +115,7 @@ def test_fused_config2_size(sig, oracle, monkeypatch):
     k = sig.SigPDE(sig.kernels.LinearKernel(), 2, precision="tc64")
     monkeypatch.setenv("SIGK_FUSED_TC", "1")
     fused = k.gram(X, Y)
-    monkeypatch.delenv("SIGK_FUSED_TC", raising=False)
+    monkeypatch.setenv("SIGK_FUSED_TC", "0")
     two = k.gram(X, Y)
     torch.cuda.synchronize()
     assert torch.equal(fused, two)
