@@ -26,13 +26,15 @@
 // 32 q + t belongs to exactly one of the two warps of quarter q:
 //     LO rows: t < 16 -> set 0, lane t;       t >= 16 -> set 1, lane t - 16
 //     HI rows: t >= 16 -> set 0, lane t;      t < 16 -> set 1, lane t + 16
-// and both sets share the same columns.  Each warp loads the LO and HI
-// columns and keeps the one its thread needs.  TMEM: 2 slots x 2 y paths x
+// and both sets share the same columns.  TMEM: 2 slots x 2 y paths x
 // {LO, HI} x RC tiles x 16 columns = 128 RC columns (512 at RC = 4).
 //
-// At chunk boundary kb a warp waits for chunk kb's MMAs, moves its increments
-// of chunks kb - 1 and kb into its own shared-memory ring, skewed so that
-// slot s % 16 holds what each thread needs at step s, and arrives on a
+// At chunk boundary kb the two warps of a quarter wait for chunk kb's MMAs
+// and split the copy of chunks kb - 1 and kb out of TMEM: set 0 loads the LO
+// family, set 1 the HI family, and thread t writes lane 32 q + t into the
+// shared-memory ring of the warp that owns the row, skewed so that slot
+// s % 16 holds what each thread needs at step s (one 16-byte store per slot,
+// between two 64-thread barriers of the pair).  Then each warp arrives on a
 // counter.  The last of the 8 warps to arrive issues chunk kb + 1's MMAs
 // (into the slot of chunk kb - 1, which every warp has now read) and stages
 // the y rows of chunk kb + 2: no producer warp, no block-wide barrier.  The
@@ -108,7 +110,8 @@ __host__ __forceinline__ size_t fused_tc_smem(int rc, int kp) { return ft_smem_l
 struct FtState {
     uint32_t tmem;       // TMEM base address
     int err;             // a wait ran out in this CTA
-    uint32_t arrive[2];  // [0]: arrivals at boundaries so far; [1]: an HI-only commit is in flight
+    uint32_t arrive;     // arrivals at boundaries so far
+    uint32_t aux_pending; // an HI-only commit (x block change) is in flight
     int64_t a_block;     // x block held in the A stage
     uint32_t a_phase;    // completed stagings of A (mbarrier phases)
     uint32_t aux_phase;  // completed HI-only commits (x block changes)
@@ -219,10 +222,10 @@ struct FtIssuer {
         if (blk != st->a_block) {
             // the HI family still reads the old x block: complete it, then stage the new block
             mma_family(k, 1);
-            st->arrive[1] = 1; // an HI-only commit in flight
+            st->aux_pending = 1;
             mma_commit(bar_aux);
             if (!mbar_wait(bar_aux, st->aux_phase & 1)) return fail();
-            st->arrive[1] = 0;
+            st->aux_pending = 0;
             ++st->aux_phase;
             stage_a(blk);
             ++st->a_phase;
@@ -308,7 +311,8 @@ __global__ void __launch_bounds__(kFtWarps * 32, 1) fused_tc_kernel(FusedTcParam
     if (tid == 32) {
         for (int i = 0; i < 4 + kFtBSlots; ++i) mbar_init(bar_a + 8 * i, 1); // a, aux, b[], mma[2]
         st->err = 0;
-        st->arrive[0] = st->arrive[1] = 0;
+        st->arrive = 0;
+        st->aux_pending = 0;
         st->a_block = -1;
         st->a_phase = 0;
         st->aux_phase = 0;
@@ -352,7 +356,7 @@ __global__ void __launch_bounds__(kFtWarps * 32, 1) fused_tc_kernel(FusedTcParam
     // ring slot j, y path r of this thread: myring[j * kSlotF + r * 32 * RC .. + RC)
     float *myring = reinterpret_cast<float *>(smem + L.ring) + (size_t)warp * kFtRing * kSlotF + lane * RC;
     const uint32_t tq = tmem + ((uint32_t)(q * 32) << 16); // this warp's TMEM lane quarter
-    const uint32_t arrive_addr = smem_u32(&st->arrive[0]);
+    const uint32_t arrive_addr = smem_u32(&st->arrive);
 
     // Boundary kb: chunk kb's MMAs are done; the increments for steps [16 kb, 16 kb + 16) come from chunks
     // kb - 1 and kb (column c of chunk a is step 16 a + c + ii of the thread that plays the row's lane).
@@ -496,7 +500,7 @@ __global__ void __launch_bounds__(kFtWarps * 32, 1) fused_tc_kernel(FusedTcParam
             const int64_t sb = st->staged_b;
             for (int64_t k = (sb > 3 ? sb - 3 : 0); k <= sb; ++k) I.wait_b(k);
             if (st->a_phase > 0) mbar_wait(bar_a, (st->a_phase - 1) & 1);
-            if (st->arrive[1]) mbar_wait(bar_aux, st->aux_phase & 1);
+            if (st->aux_pending) mbar_wait(bar_aux, st->aux_phase & 1);
             if (st->issued >= 0) mbar_wait(bar_mma + 8 * (uint32_t)(st->issued & 1), (uint32_t)((st->issued >> 1) & 1));
             atomicOr(p.err, 1u);
         }
