@@ -184,3 +184,41 @@ def test_gradient_routing():
             k.gram(x, x)
         with pytest.raises(ValueError, match="CUDA"):
             k.pairwise(x)
+
+
+def test_route_choices_by_workspace(built_lib, monkeypatch):
+    """Route choices visible through sigk_workspace_size (host-only planning).
+
+    A tc64 Gram of order >= 2 takes the fused tensor-core kernel (operand
+    images only: no increment matrix) unless SIGK_FUSED_TC=0; order 1 keeps the
+    two-phase matrix unless SIGK_FUSED_TC=1.  An fp64 Gram of d >= 16 writes the
+    float64 increment matrix, except at order 2-3 when the lanes' dx tile fits
+    registers (then it needs only the path differences, as with
+    SIGK_NO_DGEMM_INC=1); its symmetric Gram keeps the matrix."""
+    from sigpde_b200 import _lib
+    lib = _lib.lib()
+    G, S, F32 = _lib.SIGK_OP_GRAM, _lib.SIGK_OP_GRAM_SYM, _lib.SIGK_F32
+    TC64, FP64 = _lib.SIGK_PREC_TC64, _lib.SIGK_PREC_FP64
+
+    def ws(op, nx, ny, lx, ly, d, o, prec, **env):
+        for k in ("SIGK_FUSED_TC", "SIGK_NO_DGEMM_INC"):
+            monkeypatch.delenv(k, raising=False)
+        for k, v in env.items():
+            monkeypatch.setenv(k, v)
+        n = lib.sigk_workspace_size(op, nx, ny, lx, ly, d, o, F32, prec)
+        for k in env:
+            monkeypatch.delenv(k)
+        return n
+
+    # tc64, order 2: fused by default (~4 MB), two-phase when disabled (the 4.26 GB matrix, chunked)
+    fused = ws(G, 256, 256, 128, 128, 8, 2, TC64)
+    two = ws(G, 256, 256, 128, 128, 8, 2, TC64, SIGK_FUSED_TC="0")
+    assert fused < 8 << 20 < 1 << 30 < two
+    # tc64, order 1: two-phase by default, fused on request
+    assert ws(G, 256, 256, 128, 128, 8, 1, TC64) > 1 << 30 > ws(G, 256, 256, 128, 128, 8, 1, TC64, SIGK_FUSED_TC="1")
+    # fp64, d = 16, order 2, 156 rows (8 a lane, 2 coarse rows x 16 dims in registers): no matrix
+    g = ws(G, 7, 6, 40, 47, 16, 2, FP64)
+    assert g == ws(G, 7, 6, 40, 47, 16, 2, FP64, SIGK_NO_DGEMM_INC="1")
+    assert ws(S, 7, 7, 40, 40, 16, 2, FP64) > ws(S, 7, 7, 40, 40, 16, 2, FP64, SIGK_NO_DGEMM_INC="1")
+    # fp64, d = 24 (a 32-wide padded tile: too wide for registers) keeps the matrix at order 2
+    assert ws(G, 7, 6, 40, 47, 24, 2, FP64) > ws(G, 7, 6, 40, 47, 24, 2, FP64, SIGK_NO_DGEMM_INC="1")

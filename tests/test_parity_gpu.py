@@ -397,11 +397,14 @@ def test_robust_normalization_increment_sources(sig, oracle, L, d, order, monkey
     np.testing.assert_array_equal(host(rk.normalization(X)), lam)
 
 
-@pytest.mark.parametrize("shape", [(7, 6, 40, 16, 2), (9, 9, 64, 32, 0), (5, 4, 300, 24, 1), (6, 6, 12, 16, 4)])
+@pytest.mark.parametrize("shape", [(7, 6, 40, 24, 2), (9, 9, 64, 32, 0), (5, 4, 300, 24, 1), (6, 6, 12, 16, 4),
+                                   (7, 6, 40, 16, 2)])
 def test_fp64_wide_paths_use_a_float64_increment_matrix(sig, oracle, shape, monkeypatch):
     """fp64 Grams with d >= 16 first write the float64 increments of all pairs with one GEMM on the
     CUDA cores and the wavefront reads them; each increment is summed in the fused kernels' order, so
-    the results are bitwise those of the fused path (SIGK_NO_DGEMM_INC=1), and meet the fp64 bound."""
+    the results are bitwise those of the fused path (SIGK_NO_DGEMM_INC=1), and meet the fp64 bound.
+    (A Gram of order 2-3 whose lanes hold dx in registers, like the Gram of (7, 6, 40, 16, 2), takes
+    the register kernel instead; its symmetric Gram keeps the matrix.)"""
     nx, ny, L, d, o = shape
     X = cuda(oracle.brownian(nx, L, d, 71 + L), torch.float64)
     Y = cuda(oracle.brownian(ny, L + 7, d, 72 + L), torch.float64)
