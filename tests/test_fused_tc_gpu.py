@@ -35,6 +35,8 @@ SHAPES = [
     (33, 3, 17, 129, 16, 0),    # one y block of 3 paths, ncy = 128
     (4, 9, 66, 64, 8, 2),       # 260 rows: 16 a lane, 4 coarse rows (one row of padding)
     (64, 81, 40, 35, 4, 1),     # 328 groups on 148 CTAs: runs cross x blocks; last y pair of one path
+    (5, 1, 40, 41, 8, 2),       # a single y path: every y pair has one path
+    (1, 6, 33, 30, 2, 2),       # a single x path: 7 of the block's 8 rows are absent
 ]
 
 
