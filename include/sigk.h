@@ -41,7 +41,7 @@
  *                   the increment matrix: up to 6 GiB per call (the x paths
  *                   are processed in chunks beyond that; SIGK_TC_CHUNK_MB
  *                   sets the chunk size).  Exception: sigk_gram with TC64 at
- *                   order 2 or 3, x paths of one band and dim <= 8 (<= 16 at
+ *                   order 2 or 3, x paths of one band and dim <= 8 (<= 32 at
  *                   up to 2 coarse rows a lane) runs one fused kernel that
  *                   hands the increments from TMEM through shared memory to
  *                   the wavefront; its workspace holds only the operand

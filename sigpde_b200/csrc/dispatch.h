@@ -110,6 +110,6 @@ StreamIncFn get_stream_inc_kernel(bool f64cells, int R, int O, bool mat64, int W
 // Fused tensor-core Gram (fused_tc.cuh): tcgen05 increments handed to the wavefront through shared
 // memory; R rows a lane at order O (R >= 2^O, R >> O <= 4), null where not built
 using FusedTcFn = void (*)(FusedTcParams);
-FusedTcFn get_fused_tc_kernel(int R, int O);
+FusedTcFn get_fused_tc_kernel(int R, int O, int ring); // ring: 16 or 8 steps between boundaries
 
 } // namespace sigk

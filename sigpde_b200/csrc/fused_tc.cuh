@@ -18,7 +18,8 @@
 // each chunk k is two MMA families: LO, against the y rows of times
 // [16k, 16k + 16), for wavefront lanes 0..15, and HI, against times
 // [16k - 16, 16k), for lanes 16..31.  Within each half the skew is at most 15
-// steps, and boundary kb reads only chunks kb - 1 and kb: 2 TMEM slots.
+// steps, so the 16 steps after a chunk boundary read only 2 chunks: 2 TMEM
+// slots.
 //
 // Lane sharing.  A 32x32b TMEM load gives thread t of warp w lane
 // 32 (w % 4) + t.  Set h = 0 plays wavefront lane t on thread t, set h = 1
@@ -29,15 +30,17 @@
 // and both sets share the same columns.  TMEM: 2 slots x 2 y paths x
 // {LO, HI} x RC tiles x 16 columns = 128 RC columns (512 at RC = 4).
 //
-// At chunk boundary kb the two warps of a quarter wait for chunk kb's MMAs
-// and split the copy of chunks kb - 1 and kb out of TMEM: set 0 loads the LO
+// Every RING steps (16, or 8 where a wide dimension leaves shared memory for
+// only 8 ring slots) the two warps of a quarter wait for the current chunk's
+// MMAs and split the copy of it and the chunk before out of TMEM: set 0 loads the LO
 // family, set 1 the HI family, and thread t writes lane 32 q + t into the
 // shared-memory ring of the warp that owns the row, skewed so that slot
 // s % 16 holds what each thread needs at step s (one 16-byte store per slot,
 // between two 64-thread barriers of the pair).  Then each warp arrives on a
-// counter.  The last of the 8 warps to arrive issues chunk kb + 1's MMAs
-// (into the slot of chunk kb - 1, which every warp has now read) and stages
-// the y rows of chunk kb + 2: no producer warp, no block-wide barrier.  The
+// counter.  At the last boundary that reads chunk m - 1, the last of the 8
+// warps to arrive issues chunk m + 1's MMAs (into the slot of chunk m - 1)
+// and stages the y rows of chunk m + 2: no producer warp, no block-wide
+// barrier.  The
 // A operand (the x block's rows) changes only where the run moves to another
 // x block; there the HI MMAs of that chunk, which still read the old block,
 // are completed before the new block is staged.
@@ -49,7 +52,8 @@
 //
 // Scope: Gram (x != y), tc64 (float64 cells), dyadic order <= 3, x paths of
 // one band with R = RC 2^order rows a lane, RC <= 4, shared memory within the
-// device limit (dimension <= 8 at RC = 4, <= 16 below).  Every wait is
+// device limit (RING = 16: dimension <= 8 at RC = 4, <= 16 below; RING = 8:
+// dimension <= 16 at RC = 4, <= 32 at RC <= 2).  Every wait is
 // bounded: a wait that runs out sets the error word and the CTA's entries
 // become NaN.
 #pragma once
@@ -60,7 +64,9 @@ namespace sigk {
 
 constexpr int kFtWarps = 8;      // two sets of four wavefront warps (one per TMEM lane quarter)
 constexpr int kFtChunk = 16;     // times per MMA chunk (the MMA's N)
-constexpr int kFtRing = 16;      // ring slots per thread and y path: the 16 steps after a boundary
+// Ring slots per thread and y path (the steps between two boundaries): 16, or 8 where the operands
+// of a wide dimension leave no room for 16 (a boundary every 8 steps; each chunk is then read at two).
+constexpr int kFtRingMax = 16;
 constexpr int kFtBSlots = 4;     // y-row stages: chunks k - 1, k (MMA k), k + 1 (next MMA), k + 2 (staging)
 
 struct FusedTcParams {
@@ -87,15 +93,15 @@ struct FtSmem {
 
 __host__ __device__ __forceinline__ uint32_t ft_align(uint32_t v, uint32_t a) { return (v + a - 1) / a * a; }
 
-// Shared memory: the rings (per warp: kFtRing slots x 2 y paths x 32 threads x
+// Shared memory: the rings (per warp: `ring` slots x 2 y paths x 32 threads x
 // RC floats), the A block (2 RC tiles, hi then lo), kFtBSlots y-row stages
 // (2 y paths x {hi, lo} x 16 rows), mbarriers (a, aux, b[kFtBSlots], mma[2])
 // and the issuers' shared state.
-__host__ __device__ __forceinline__ FtSmem ft_smem_layout(int rc, int kp)
+__host__ __device__ __forceinline__ FtSmem ft_smem_layout(int rc, int kp, int ring)
 {
     FtSmem s{};
     s.ring = 0;
-    s.a = ft_align((uint32_t)kFtWarps * kFtRing * 2 * 32 * rc * 4, 1024);
+    s.a = ft_align((uint32_t)kFtWarps * ring * 2 * 32 * rc * 4, 1024);
     s.b = s.a + 2u * 2u * (uint32_t)rc * kTcM * kp * 4;
     s.bars = s.b + (uint32_t)kFtBSlots * 2u * 2u * (uint32_t)kFtChunk * kp * 4;
     s.misc = s.bars + (4 + kFtBSlots) * 8;
@@ -103,7 +109,7 @@ __host__ __device__ __forceinline__ FtSmem ft_smem_layout(int rc, int kp)
     return s;
 }
 
-__host__ __forceinline__ size_t fused_tc_smem(int rc, int kp) { return ft_smem_layout(rc, kp).total; }
+__host__ __forceinline__ size_t fused_tc_smem(int rc, int kp, int ring) { return ft_smem_layout(rc, kp, ring).total; }
 
 // State shared by the threads that take turns issuing (shared memory; each
 // issuer acquires it through the arrival counter, see FtIssuer).
@@ -273,13 +279,14 @@ __device__ __forceinline__ void ft_ring_write(float *dst, const float (&v)[RC][k
         dst[0] = v[0][c];
 }
 
-template <int R, int O>
+template <int R, int O, int RING>
 __global__ void __launch_bounds__(kFtWarps * 32, 1) fused_tc_kernel(FusedTcParams p)
 {
     using BS = BlockShape<R, O>;
     constexpr int C = BS::C;
     constexpr int RC = BS::RC;
     static_assert(O <= 3 && (R >> O) == RC && RC <= 4, "one coarse column a step, whole coarse rows a lane");
+    static_assert(RING == 16 || RING == 8, "a boundary every 16 or 8 steps");
     constexpr uint32_t kCols = ft_tmem_cols(RC);
     constexpr int kSlotF = 2 * 32 * RC; // floats per ring slot (2 y paths x 32 threads x RC)
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -293,9 +300,10 @@ __global__ void __launch_bounds__(kFtWarps * 32, 1) fused_tc_kernel(FusedTcParam
     const int Tp = p.T;
     const int64_t nlocal = ng * Tp;            // time slots of each warp's run
     const int64_t S = nlocal + 31;             // steps: lane 31 runs 31 behind lane 0
-    const int64_t nbound = (S + kFtChunk - 1) / kFtChunk;
+    const int64_t nbound = (S + RING - 1) / RING;             // boundaries: one every RING steps
+    const int64_t nmma = (RING * (nbound - 1)) / kFtChunk + 1; // chunks read: up to the last boundary's
 
-    const FtSmem L = ft_smem_layout(RC, p.kp);
+    const FtSmem L = ft_smem_layout(RC, p.kp, RING);
     const uint32_t sbase = smem_u32(smem);
     FtState *st = reinterpret_cast<FtState *>(smem + L.misc);
     volatile int *cta_err = &st->err;
@@ -348,38 +356,42 @@ __global__ void __launch_bounds__(kFtWarps * 32, 1) fused_tc_kernel(FusedTcParam
         ++st->a_phase;
         I.stage_b(0);
         I.stage_b(1);
-        if (I.issue(0) && I.issue(1) && nbound > 2) I.stage_b(2);
+        if (I.issue(0) && I.issue(1) && nmma > 2) I.stage_b(2);
     }
     __syncwarp();
 
     // ---------------------------------------------------------------- the wavefront
     // ring slot j, y path r of this thread: myring[j * kSlotF + r * 32 * RC .. + RC)
-    float *myring = reinterpret_cast<float *>(smem + L.ring) + (size_t)warp * kFtRing * kSlotF + lane * RC;
+    float *myring = reinterpret_cast<float *>(smem + L.ring) + (size_t)warp * RING * kSlotF + lane * RC;
     const uint32_t tq = tmem + ((uint32_t)(q * 32) << 16); // this warp's TMEM lane quarter
     const uint32_t arrive_addr = smem_u32(&st->arrive);
 
-    // Boundary kb: chunk kb's MMAs are done; the increments for steps [16 kb, 16 kb + 16) come from chunks
-    // kb - 1 and kb (column c of chunk a is step 16 a + c + ii of the thread that plays the row's lane).
-    // The two warps of a lane quarter share the work: set 0 loads the LO family, set 1 the HI family, and
-    // thread t writes the value of TMEM lane 32 q + t into the ring of the warp that owns the row (its own
-    // for t < 16, its partner's for t >= 16; thread t of either warp plays a lane congruent to t mod 16,
-    // so the ring offset and the skew ii are the same).  A 64-thread barrier of the pair before the copy
+    // Boundary b, before steps [RING b, RING b + RING): chunk m = RING b / 16 is done (its MMAs waited for);
+    // the increments of these steps come from chunks m - 1 and m (column c of chunk a is step
+    // 16 a + c + ii of the thread that plays the row's lane, ring slot 16 a + c + ii - RING b).  The two
+    // warps of a lane quarter share the copy: set 0 loads the LO family, set 1 the HI family, and thread t
+    // writes the value of TMEM lane 32 q + t into the ring of the warp that owns the row (its own for
+    // t < 16, its partner's for t >= 16; thread t of either warp plays a lane congruent to t mod 16, so
+    // the ring offset and the skew ii are the same).  A 64-thread barrier of the pair before the copy
     // (both warps are done reading the previous period's slots) and one after it (the slots are written)
-    // orders the cross-warp stores.  Then the arrival, and the last arrival issues chunk kb + 1 into the
-    // TMEM slot of chunk kb - 1.  Arrivals are totally ordered by boundary once past boundary 1 (a warp
-    // passes boundary kb + 1 only after chunk kb + 1 was issued), so the arrival that brings the count to
-    // 8 (kb + 1) is the last one of boundary kb.
-    float *dstring = lane < 16 ? myring : myring + (h ? -4 : 4) * kFtRing * kSlotF; // the row owner's ring
+    // orders the cross-warp stores.  Then the arrival.  Chunk m - 1 is read for the last time at the
+    // boundary whose period ends at step 16 m + 15 (b = m at RING = 16, b = 2m + 1 at RING = 8); the last
+    // arrival there issues chunk m + 1 into its TMEM slot and stages the y rows of chunk m + 2.  No warp
+    // arrives at a boundary before every warp has arrived at the previous one past the first chunk (the
+    // next boundary's chunk is issued only at that last arrival), so the arrival that brings the count to
+    // 8 (b + 1) is the last one of boundary b.
+    float *dstring = lane < 16 ? myring : myring + (h ? -4 : 4) * RING * kSlotF; // the row owner's ring
     const int pair_bar = 1 + q; // named barrier of warps q and q + 4
-    auto boundary = [&](int64_t kb) {
-        if (!*cta_err && !mbar_wait(bar_mma + 8 * (uint32_t)(kb & 1), (uint32_t)((kb >> 1) & 1))) *cta_err = 1;
+    auto boundary = [&](int64_t b) {
+        const int64_t m = (RING * b) / kFtChunk;
+        if (!*cta_err && !mbar_wait(bar_mma + 8 * (uint32_t)(m & 1), (uint32_t)((m >> 1) & 1))) *cta_err = 1;
         tc_fence_after();
         named_bar(pair_bar, 64);
         // tcgen05.ld is warp-collective: decide for the whole warp (another thread may set the flag)
         if (!__any_sync(kFullMask, *cta_err != 0)) {
 #pragma unroll 1
-            for (int64_t a = (kb > 0 ? kb - 1 : 0); a <= kb; ++a) {
-                const int base = (int)(kFtChunk * (a - kb)) + ii;
+            for (int64_t a = (m > 0 ? m - 1 : 0); a <= m; ++a) {
+                const int base = (int)(kFtChunk * a - RING * b) + ii;
 #pragma unroll 1
                 for (int r = 0; r < 2; ++r) {
                     float v[RC][kFtChunk]; // TMEM lane 32 q + lane of this warp's family, all RC tiles
@@ -406,7 +418,7 @@ __global__ void __launch_bounds__(kFtWarps * 32, 1) fused_tc_kernel(FusedTcParam
 #pragma unroll
                     for (int c = 0; c < kFtChunk; ++c) {
                         const int j = base + c;
-                        if ((unsigned)j < (unsigned)kFtRing) ft_ring_write<RC>(dstring + j * kSlotF + r * 32 * RC, v, c);
+                        if ((unsigned)j < (unsigned)RING) ft_ring_write<RC>(dstring + j * kSlotF + r * 32 * RC, v, c);
                     }
                 }
             }
@@ -416,9 +428,10 @@ __global__ void __launch_bounds__(kFtWarps * 32, 1) fused_tc_kernel(FusedTcParam
         __syncwarp();
         if (lane == 0) {
             const uint32_t old = atomic_add_acq_rel(arrive_addr, 1u);
-            if (old + 1 == (uint32_t)(kFtWarps * (kb + 1))) {
+            if (old + 1 == (uint32_t)(kFtWarps * (b + 1))) {
                 tc_fence_after();
-                if (kb >= 1 && kb + 1 < nbound && I.issue(kb + 1) && kb + 2 < nbound) I.stage_b(kb + 2);
+                const bool last_read_of_prev = RING == kFtChunk || (b & 1); // the last boundary reading m - 1
+                if (last_read_of_prev && m >= 1 && m + 1 < nmma && I.issue(m + 1) && m + 2 < nmma) I.stage_b(m + 2);
             }
         }
         __syncwarp();
@@ -444,10 +457,10 @@ __global__ void __launch_bounds__(kFtWarps * 32, 1) fused_tc_kernel(FusedTcParam
     Dbl2 corner_next = one;
     int col = 0;
     int64_t grp = 0, xi = 0, ya = 0;
-    for (int64_t kb = 0; kb < nbound; ++kb) {
-        boundary(kb);
-        const int64_t s1 = (kb + 1) * kFtChunk < S ? (kb + 1) * kFtChunk : S;
-        for (int64_t s = kb * kFtChunk; s < s1; ++s) {
+    for (int64_t b = 0; b < nbound; ++b) {
+        boundary(b);
+        const int64_t s1 = (b + 1) * RING < S ? (b + 1) * RING : S;
+        for (int64_t s = b * RING; s < s1; ++s) {
             Dbl2 top[C];
 #pragma unroll
             for (int c = 0; c < C; ++c) {
@@ -471,7 +484,7 @@ __global__ void __launch_bounds__(kFtWarps * 32, 1) fused_tc_kernel(FusedTcParam
                     const Dbl2 corner = (col == 0) ? one : corner_next;
                     corner_next = top[C - 1];
                     float ca[RC], cb[RC];
-                    const float *rs = myring + (int)(s & (kFtRing - 1)) * kSlotF;
+                    const float *rs = myring + (int)(s & (RING - 1)) * kSlotF;
                     ft_ring_read<RC>(rs, ca);
                     ft_ring_read<RC>(rs + 32 * RC, cb);
                     Dbl2 A[RC], B[RC];

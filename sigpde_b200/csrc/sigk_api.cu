@@ -581,7 +581,7 @@ int consume_matrix(const TcPlan &t, int op, const void *mat, bool mat64, int64_t
 constexpr size_t kFtMaxSmem = 227 * 1024; // the B200's per-block opt-in limit
 struct FtPlan {
     bool ok = false;
-    int R = 0, O = 0, kp = 0, T = 0;
+    int R = 0, O = 0, kp = 0, T = 0, ring = 16;
     size_t err_off = 0, a_off = 0, a_bytes = 0, b_off = 0, b_bytes = 0, ws_bytes = 0;
 };
 
@@ -593,17 +593,23 @@ FtPlan make_fused_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy,
     // takes it at every eligible order, SIGK_FUSED_TC=0 never.
     const char *force = getenv("SIGK_FUSED_TC");
     const int mode = (force && force[0]) ? (force[0] != '0' ? 1 : 0) : -1;
-    if (op != kOpGram || precision != SIGK_PREC_TC64 || d > 16 || order > 3 || mode == 0 || (mode < 0 && order < 2))
+    if (op != kOpGram || precision != SIGK_PREC_TC64 || d > 32 || order > 3 || mode == 0 || (mode < 0 && order < 2))
         return f;
     const int64_t n = ncx << order;
     if (n > 32 * 16) return f; // one band
     const int R = pick_rows(n);
     const int rc = R >> order;
     if (rc < 1 || (rc << order) != R || rc > 4 || 32 * R < n) return f;
-    if (fused_tc_smem(rc, (int)((d + 7) / 8 * 8)) > kFtMaxSmem) return f;
-    if (!get_fused_tc_kernel(R, order)) return f;
+    // a boundary every 16 steps, or every 8 (half the ring) where the operands of a wide dimension need the room
+    const int kpd = (int)((d + 7) / 8 * 8);
+    const int ring = fused_tc_smem(rc, kpd, 16) <= kFtMaxSmem ? 16 : fused_tc_smem(rc, kpd, 8) <= kFtMaxSmem ? 8 : 0;
+    if (!ring || !get_fused_tc_kernel(R, order, ring)) return f;
+    // at 4 coarse rows a lane the 8-step boundary's copy outweighs the matrix round trip (256 x 256, L = 128,
+    // d = 16, order 2: 5.93 vs 5.63 ms two-phase); at 2 it wins (L = 64, d = 32, order 3: 4.30 vs 4.44 ms)
+    if (mode < 0 && ring == 8 && rc > 2) return f;
     f.ok = true;
     f.R = R;
+    f.ring = ring;
     f.O = order;
     f.kp = (int)((d + 7) / 8 * 8);
     f.T = (int)((ncy + kFtChunk - 1) / kFtChunk * kFtChunk);
@@ -633,8 +639,8 @@ int run_pairs_fused(const FtPlan &f, const void *x, const void *y, int64_t nx, i
     if ((st = tc_image(in64, x, nx, lx, d, kTcM, kTcM, (nx + 7) / 8 * 2 * rc, f.kp, fs, sx, a_hi, a_lo, stream, rc)))
         return st;
     if ((st = tc_image(in64, y, ny, ly, d, f.T, f.T, ny, f.kp, 1.0, sy, b_hi, b_lo, stream))) return st;
-    FusedTcFn fn = get_fused_tc_kernel(f.R, f.O);
-    const size_t smem = fused_tc_smem(rc, f.kp);
+    FusedTcFn fn = get_fused_tc_kernel(f.R, f.O, f.ring);
+    const size_t smem = fused_tc_smem(rc, f.kp, f.ring);
     int dev = 0;
     e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");

@@ -190,8 +190,9 @@ def test_route_choices_by_workspace(built_lib, monkeypatch):
     """Route choices visible through sigk_workspace_size (host-only planning).
 
     A tc64 Gram of order >= 2 takes the fused tensor-core kernel (operand
-    images only: no increment matrix) unless SIGK_FUSED_TC=0; order 1 keeps the
-    two-phase matrix unless SIGK_FUSED_TC=1.  An fp64 Gram of d >= 16 writes the
+    images only: no increment matrix) unless SIGK_FUSED_TC=0, except where its
+    operands leave room for only an 8-slot ring at 4 coarse rows a lane; order
+    1 keeps the two-phase matrix unless SIGK_FUSED_TC=1.  An fp64 Gram of d >= 16 writes the
     float64 increment matrix, except at order 2-3 when the lanes' dx tile fits
     registers (then it needs only the path differences, as with
     SIGK_NO_DGEMM_INC=1); its symmetric Gram keeps the matrix."""
@@ -216,6 +217,12 @@ def test_route_choices_by_workspace(built_lib, monkeypatch):
     assert fused < 8 << 20 < 1 << 30 < two
     # tc64, order 1: two-phase by default, fused on request
     assert ws(G, 256, 256, 128, 128, 8, 1, TC64) > 1 << 30 > ws(G, 256, 256, 128, 128, 8, 1, TC64, SIGK_FUSED_TC="1")
+    # tc64, d = 16 at 4 coarse rows a lane (the 8-slot ring): two-phase by default, fused on request
+    assert ws(G, 256, 256, 128, 128, 16, 2, TC64) > 1 << 30 > ws(G, 256, 256, 128, 128, 16, 2, TC64, SIGK_FUSED_TC="1")
+    # tc64, d = 32 at 2 coarse rows a lane (8-slot ring): fused by default
+    assert ws(G, 256, 256, 64, 64, 32, 3, TC64) < 16 << 20 < ws(G, 256, 256, 64, 64, 32, 3, TC64, SIGK_FUSED_TC="0")
+    # tc64, d = 32 at 4 coarse rows a lane: the operands do not fit shared memory, two-phase even on request
+    assert ws(G, 256, 256, 128, 128, 32, 2, TC64, SIGK_FUSED_TC="1") == ws(G, 256, 256, 128, 128, 32, 2, TC64)
     # fp64, d = 16, order 2, 156 rows (8 a lane, 2 coarse rows x 16 dims in registers): no matrix
     g = ws(G, 7, 6, 40, 47, 16, 2, FP64)
     assert g == ws(G, 7, 6, 40, 47, 16, 2, FP64, SIGK_NO_DGEMM_INC="1")

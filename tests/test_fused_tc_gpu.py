@@ -11,8 +11,9 @@ oracle the tc64 bound applies: error normalised by sqrt(k(x,x) k(y,y)) at most
 1e-5.  Shapes cover every instantiated (rows per lane, order), time lines
 padded to 16 columns, odd numbers of x and y paths (a last x block of fewer
 than 8 paths, a last y pair of one path), fewer groups than CTAs, runs that
-cross x blocks (the A operand restaged mid-run), scales, float64 inputs and
-dimensions 1..16.  Each case first checks that the fused route is the one
+cross x blocks (the A operand restaged mid-run), both ring sizes (a boundary
+every 16 steps, or every 8 where the operands of dimensions up to 32 need the
+shared memory), scales, float64 inputs and dimensions 1..32.  Each case first checks that the fused route is the one
 taken (its workspace has no increment matrix).
 """
 import numpy as np
@@ -37,6 +38,9 @@ SHAPES = [
     (64, 81, 40, 35, 4, 1),     # 328 groups on 148 CTAs: runs cross x blocks; last y pair of one path
     (5, 1, 40, 41, 8, 2),       # a single y path: every y pair has one path
     (1, 6, 33, 30, 2, 2),       # a single x path: 7 of the block's 8 rows are absent
+    (24, 37, 128, 128, 16, 2),  # d = 16 at 4 coarse rows a lane: 8-slot ring (taken when forced)
+    (9, 11, 60, 57, 32, 2),     # d = 32 at 2 coarse rows a lane: 8-slot ring
+    (7, 5, 60, 50, 12, 3),      # d = 12 at order 3 (16-slot ring)
 ]
 
 
