@@ -134,3 +134,31 @@ def test_fused_config2_size(sig, oracle, monkeypatch):
     kxx = oracle.pairwise(x[i], None, 2)
     kyy = oracle.pairwise(y[j], None, 2)
     assert float(np.max(np.abs(G.reshape(-1)[flat] - want) / np.sqrt(kxx * kyy))) <= CS_TC64
+
+
+def test_fused_random_shapes_bitwise(sig, oracle, monkeypatch):
+    """40 seeded random Gram shapes (paths 1..40, lengths 5..130, dimensions
+    1..32, orders 0..3): wherever the fused route is eligible (forced with
+    SIGK_FUSED_TC=1) its results equal the two-phase route's bitwise."""
+    from sigpde_b200 import _lib
+    rng = np.random.default_rng(2024)
+    taken = 0
+    for _ in range(40):
+        nx, ny = int(rng.integers(1, 41)), int(rng.integers(1, 41))
+        lx, ly = int(rng.integers(5, 131)), int(rng.integers(5, 131))
+        d, o = int(rng.integers(1, 33)), int(rng.integers(0, 4))
+        if not _fused_taken(monkeypatch, nx, ny, lx, ly, d, o, False):
+            continue
+        taken += 1
+        X = torch.tensor(oracle.brownian(nx, lx, d, int(rng.integers(1 << 30))), dtype=torch.float32, device="cuda")
+        Y = torch.tensor(oracle.brownian(ny, ly, d, int(rng.integers(1 << 30))), dtype=torch.float32, device="cuda")
+        k = sig.SigPDE(sig.kernels.LinearKernel(), o, precision="tc64")
+        monkeypatch.setenv("SIGK_FUSED_TC", "1")
+        fused = k.gram(X, Y)
+        monkeypatch.setenv("SIGK_FUSED_TC", "0")
+        two = k.gram(X, Y)
+        monkeypatch.delenv("SIGK_FUSED_TC", raising=False)
+        torch.cuda.synchronize()
+        assert torch.equal(fused, two), (nx, ny, lx, ly, d, o)
+        assert bool(torch.all(torch.isfinite(fused)))
+    assert taken >= 10, f"only {taken} of 40 random shapes were eligible"
