@@ -32,18 +32,17 @@
 //
 // Every RING steps (16, or 8 where a wide dimension leaves shared memory for
 // only 8 ring slots) the two warps of a quarter wait for the current chunk's
-// MMAs and split the copy of it and the chunk before out of TMEM: set 0 loads the LO
-// family, set 1 the HI family, and thread t writes lane 32 q + t into the
-// shared-memory ring of the warp that owns the row, skewed so that slot
-// s % 16 holds what each thread needs at step s (one 16-byte store per slot,
-// between two 64-thread barriers of the pair).  Then each warp arrives on a
-// counter.  At the last boundary that reads chunk m - 1, the last of the 8
-// warps to arrive issues chunk m + 1's MMAs (into the slot of chunk m - 1)
+// MMAs and split the copy of it and the chunk before out of TMEM: set 0 loads
+// the LO family, set 1 the HI family, and thread t writes lane 32 q + t into
+// the shared-memory ring of the warp that owns the row, skewed so that slot
+// s % RING holds what each thread needs at step s (one 16-byte store per
+// slot, between two 64-thread barriers of the pair).  Then each warp arrives
+// on a counter.  At the last boundary that reads chunk m - 1, the last of the
+// 8 warps to arrive issues chunk m + 1's MMAs (into the slot of chunk m - 1)
 // and stages the y rows of chunk m + 2: no producer warp, no block-wide
-// barrier.  The
-// A operand (the x block's rows) changes only where the run moves to another
-// x block; there the HI MMAs of that chunk, which still read the old block,
-// are completed before the new block is staged.
+// barrier.  The A operand (the x block's rows) changes only where the run
+// moves to another x block; there the HI MMAs of that chunk, which still read
+// the old block, are completed before the new block is staged.
 //
 // The arithmetic is that of the two-phase path exactly: the same MMAs (lo*hi,
 // hi*lo, hi*hi per K step, float32 accumulation) for each increment and the
@@ -64,9 +63,6 @@ namespace sigk {
 
 constexpr int kFtWarps = 8;      // two sets of four wavefront warps (one per TMEM lane quarter)
 constexpr int kFtChunk = 16;     // times per MMA chunk (the MMA's N)
-// Ring slots per thread and y path (the steps between two boundaries): 16, or 8 where the operands
-// of a wide dimension leave no room for 16 (a boundary every 8 steps; each chunk is then read at two).
-constexpr int kFtRingMax = 16;
 constexpr int kFtBSlots = 4;     // y-row stages: chunks k - 1, k (MMA k), k + 1 (next MMA), k + 2 (staging)
 
 struct FusedTcParams {
