@@ -82,6 +82,9 @@ def parse():
                     help="skip timing the reference's Numba GPU path beside the default Gram")
     ap.add_argument("--autotune", action="store_true", help="uneven batches: measure rows per lane per bucket "
                     "before timing (sigpde_b200.torch.autotune)")
+    ap.add_argument("--resident", action="store_true",
+                    help="serving traces: requests draw their paths from a pool of 40 path sets kept resident on "
+                         "the device (GramServer.put); the per-request baseline copies them from the host")
     ap.add_argument("--burst", action="store_true", help="serving traces: every request arrives at t=0 "
                     "(saturated throughput) instead of Poisson arrivals")
     return ap.parse_args()
@@ -1186,8 +1189,10 @@ def run_reference_gpu_robust(args, w):
 
 
 # ----------------------------------------------------------------------------- serving trace
-def serve_trace(w, nreq=None):
-    """Seeded request trace: (arrival offsets in s, list of GramRequest with pinned host paths)."""
+def serve_trace(w, nreq=None, pool=0):
+    """Seeded request trace: (arrival offsets in s, list of GramRequest with pinned host paths).
+    pool > 0: the paths come from `pool` path sets drawn like the requests' (each request takes one
+    at random, so sets recur); returns (arrivals, requests, sets, set index of each request)."""
     import numpy as np
     import torch
     from sigpde_b200 import synthetic
@@ -1196,6 +1201,18 @@ def serve_trace(w, nreq=None):
     rng = np.random.Generator(np.random.PCG64(w["seed"]))
     gaps = rng.exponential(1.0 / w["rate"], nreq)
     arrivals = np.cumsum(gaps) - gaps[0]
+    if pool:
+        sets = []
+        for _ in range(pool):
+            N = int(round(np.exp(rng.uniform(np.log(w["nmin"]), np.log(w["nmax"])))))
+            L = int(round(np.exp(rng.uniform(np.log(w["lmin"]), np.log(w["lmax"])))))
+            d = int(rng.choice(w["dims"]))
+            x = synthetic.brownian_np(N, L, d, int(rng.integers(1 << 31)))
+            sets.append(torch.tensor(x, dtype=torch.float32).pin_memory())
+        idx = [int(rng.integers(pool)) for _ in range(nreq)]
+        reqs = [GramRequest(x=sets[k], order=int(rng.choice(w["orders"])),
+                            kind="robust" if rng.random() < w["robust"] else "gram", rid=i) for i, k in enumerate(idx)]
+        return arrivals, reqs, sets, idx
     reqs = []
     for i in range(nreq):
         N = int(round(np.exp(rng.uniform(np.log(w["nmin"]), np.log(w["nmax"])))))
@@ -1220,7 +1237,10 @@ def run_serve(args, w):
     from sigpde_b200 import _lib
     from sigpde_b200.serving import GramServer, serve_sequential
     torch.cuda.set_device(0)
-    arrivals, reqs = serve_trace(w)
+    if args.resident:
+        arrivals, reqs, pool, pool_idx = serve_trace(w, pool=40)
+    else:
+        arrivals, reqs = serve_trace(w)
     if args.burst:
         arrivals = np.zeros_like(arrivals)
     cells = sum(_req_cells(r) for r in reqs)
@@ -1240,6 +1260,10 @@ def run_serve(args, w):
     clocks = ClockSampler(0)
     clocks.start()
     with GramServer(max_inflight=8, precision=args.precision) as srv:
+        if args.resident:  # stored before the clock starts: residency is the point
+            stored = [srv.put(f"p{i}", t) for i, t in enumerate(pool)]
+            for r, k in zip(reqs, pool_idx):
+                r.x = stored[k]
         t0 = time.perf_counter()
         handles = []
         for i, r in enumerate(reqs):
@@ -1252,10 +1276,15 @@ def run_serve(args, w):
             h.wait(timeout=600)
         peak = srv.peak_inflight
         batching = {"batches": srv.batches, "batched_requests": srv.batched_requests}
+        store = srv.store_stats()
     clk = clocks.stop()
     served = summarize(handles, t0, max(h.t_done for h in handles))
     served["peak_inflight"] = peak
     served["kernel_level_batching"] = batching
+    if args.resident:
+        served["path_store"] = {"sets": len(store), "bytes": sum(v["bytes"] for v in store.values()),
+                                "scale_hits": sum(v["scale_hits"] for v in store.values()),
+                                "scale_misses": sum(v["scale_misses"] for v in store.values())}
     # per-request plain launches, same arrivals
     for r in reqs:
         r.arrival = 0.0
@@ -1275,7 +1304,7 @@ def run_serve(args, w):
         for k in picks:
             r, h = reqs[k], handles[k]
             N = r.x.shape[0]
-            x = r.x.double().numpy()
+            x = (r.x.host if hasattr(r.x, "host") else r.x).double().numpy()
             if r.kind == "robust":
                 lam = oracle.normalization(x, r.order)
                 npick = 2
@@ -1299,7 +1328,9 @@ def run_serve(args, w):
         "data": "synthetic Brownian paths (seeded PCG64), float32, pinned host memory",
         "config": {"workload": f"serving trace: {len(reqs)} Gram requests, Poisson {w['rate']}/s, "
                                f"N~logU[{w['nmin']},{w['nmax']}], L~logU[{w['lmin']},{w['lmax']}], d in {{2,8,32}}, "
-                               "order in {0,1,2}, 30% robust" + (" (burst: all at t=0)" if args.burst else ""),
+                               "order in {0,1,2}, 30% robust" + (" (burst: all at t=0)" if args.burst else "")
+                               + (", paths from 40 path sets kept resident by the server (the per-request "
+                                  "baseline copies each request's paths in)" if args.resident else ""),
                    "parallelism": "single GPU, 8 in-flight streams, HBM-footprint admission"},
         "served": served, "per_request_plain_launches": plain,
         "throughput_ratio_vs_plain": served["requests_per_s"] / plain["requests_per_s"],

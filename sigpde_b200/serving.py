@@ -33,8 +33,16 @@ running execute concurrently on the device, and copies overlap compute.  Complet
 is detected with CUDA events; the result, the timestamps (arrival, admission,
 completion) and any error are delivered on the request's handle.
 
+Paths can be kept resident: `put(name, paths)` copies a path set to the
+device once and returns a PathSet that requests name as x or y.  Such
+requests skip the copy-in, are not charged for the paths (the store's bytes
+come out of the budget once), and robust requests on the set compute its
+normalisation scales once per (dyadic order, precision): later requests wait
+for the event of the stream that wrote them and reuse them.
+
 Every solve is deterministic and a request's kernels only read its own
-buffers, so a request's result does not depend on what else is in flight.
+buffers (and stored paths and scales, which nothing overwrites), so a
+request's result does not depend on what else is in flight.
 
 `serve_sequential` runs the same requests one at a time (copy in, solve, copy
 out, synchronise) -- the per-request plain-launch baseline.
@@ -54,16 +62,85 @@ from . import _lib
 from .torch import kernel as _k
 from .torch import static_kernels as _sk
 
-__all__ = ["GramRequest", "RequestHandle", "GramServer", "serve_sequential", "footprint_bytes", "request_cells",
-           "request_pairs", "batch_footprint_bytes"]
+__all__ = ["GramRequest", "RequestHandle", "GramServer", "PathSet", "serve_sequential", "footprint_bytes",
+           "request_cells", "request_pairs", "batch_footprint_bytes"]
+
+
+class PathSet:
+    """Paths resident on the server's device (GramServer.put).  A request names
+    a PathSet as its x or y instead of a tensor: the paths are not copied per
+    request and not charged to the request's footprint (the store holds them
+    once), and robust requests reuse the set's normalisation scales per
+    (dyadic order, precision) -- computed by the first robust request that
+    needs them, on its stream, and read by later ones after waiting for that
+    stream's event.  `host` keeps a pinned copy for per-request baselines."""
+
+    def __init__(self, name, tensor: torch.Tensor, host: torch.Tensor):
+        self.name = name
+        self.tensor = tensor
+        self.host = host
+        self.nbytes = tensor.numel() * tensor.element_size()
+        self.lam_hits = 0
+        self.lam_misses = 0
+        self._lam = {}  # (order, precision) -> (scales, event recorded after they were written)
+        self._lock = threading.Lock()
+
+    @property
+    def shape(self):
+        return self.tensor.shape
+
+    @property
+    def dtype(self):
+        return self.tensor.dtype
+
+    def dim(self):
+        return self.tensor.dim()
+
+    def element_size(self):
+        return self.tensor.element_size()
+
+    def numel(self):
+        return self.tensor.numel()
+
+    def scales(self, rk, order: int, precision: str, stream, use_cache: bool = True):
+        """Normalisation scales of the set (RobustSigPDE.normalization), enqueued on `stream`."""
+        if not use_cache:
+            return rk.normalization(self.tensor)
+        key = (int(order), precision)
+        with self._lock:
+            hit = self._lam.get(key)
+        if hit is not None:
+            lam, ev = hit
+            stream.wait_event(ev)
+            self.lam_hits += 1
+            return lam
+        lam = rk.normalization(self.tensor)
+        ev = torch.cuda.Event()
+        ev.record(stream)
+        with self._lock:
+            self._lam.setdefault(key, (lam, ev))
+            self.lam_misses += 1
+        return lam
+
+
+def _resident(t) -> bool:
+    return isinstance(t, PathSet)
+
+
+def _on_device(t, device, use_host: bool = False):
+    """The request operand on the device: a PathSet's resident tensor (or, for a baseline that copies
+    per request, its pinned host copy sent over), else the tensor copied in (no copy if already there)."""
+    if _resident(t):
+        return t.host.to(device, non_blocking=True) if use_host else t.tensor
+    return t.to(device, non_blocking=True)
 
 
 @dataclasses.dataclass
 class GramRequest:
     """One request.  x (and y) are (N, L, d) float32/float64 tensors, on the
-    host (pinned or pageable) or on the device.  kind: "gram" (k(x_i, y_j),
-    or the symmetric Gram when y is None) or "robust" (RobustSigPDE.gram with
-    the default normaliser)."""
+    host (pinned or pageable) or on the device, or PathSets resident in the
+    server's store.  kind: "gram" (k(x_i, y_j), or the symmetric Gram when y
+    is None) or "robust" (RobustSigPDE.gram with the default normaliser)."""
 
     x: torch.Tensor
     y: Optional[torch.Tensor] = None
@@ -118,7 +195,9 @@ def footprint_bytes(req: GramRequest, precision: str = "fp64") -> int:
     sym = req.y is None
     op = _lib.SIGK_OP_GRAM_SYM if sym else _lib.SIGK_OP_GRAM
     ws = _lib.lib().sigk_workspace_size(op, nx, ny, lx, ly, d, req.order, dt, prec)
-    total = x.numel() * es + (0 if sym else y.numel() * es) + nx * ny * es + ws
+    # resident paths are held by the server's store, not by the request
+    paths = (0 if _resident(x) else x.numel() * es) + (0 if sym or _resident(y) else y.numel() * es)
+    total = paths + nx * ny * es + ws
     if req.kind == "robust":
         nws = _lib.lib().sigk_workspace_size(_lib.SIGK_OP_NORMALIZE, nx, nx, lx, lx, d, req.order, dt, prec)
         total += nws + (nx + ny) * (8 + es)
@@ -179,11 +258,12 @@ def _solve_batch_on_stream(reqs, precision: str, device, stream):
         for r in reqs:
             if r.kind not in ("gram", "robust") or r.y is not None:
                 raise ValueError("only symmetric gram / robust requests are batched")
-            x = r.x.to(device, non_blocking=True)
+            x = _on_device(r.x, device)
             N, L, d = x.shape
             ii, jj = torch.tril_indices(N, N, device=device)  # i >= j: x_i on the rows, as the symmetric Gram
             if r.kind == "robust":
-                lam = _k.RobustSigPDE(_sk.LinearKernel(), r.order, precision=precision).normalization(x)
+                rk = _k.RobustSigPDE(_sk.LinearKernel(), r.order, precision=precision)
+                lam = r.x.scales(rk, r.order, precision, stream) if _resident(r.x) else rk.normalization(x)
                 sx_parts.append(lam.index_select(0, ii))
                 sy_parts.append(lam.index_select(0, jj))
             else:
@@ -226,14 +306,17 @@ def request_cells(req: GramRequest) -> int:
     return int(x.shape[0]) * int(y.shape[0]) * n * m
 
 
-def _solve_on_stream(req: GramRequest, precision: str, device, stream, chunk_cells: int = 0, staging=None):
+def _solve_on_stream(req: GramRequest, precision: str, device, stream, chunk_cells: int = 0, staging=None,
+                     use_store: bool = True):
     """Enqueue copy-in, solve and copy-out of one request on `stream`.
     Returns (pinned host result, tensors to keep alive until the event).
     chunk_cells > 0 splits a large (non-symmetric or robust) Gram into row
-    blocks of about that many cells, one launch each."""
+    blocks of about that many cells, one launch each.  use_store=False treats
+    a PathSet operand like a host tensor (copied in, scales recomputed): the
+    per-request baseline."""
     with torch.cuda.stream(stream):
-        x = req.x.to(device, non_blocking=True)
-        y = None if req.y is None else req.y.to(device, non_blocking=True)
+        x = _on_device(req.x, device, use_host=not use_store)
+        y = None if req.y is None else _on_device(req.y, device, use_host=not use_store)
         lin = _sk.LinearKernel()
         if req.kind not in ("gram", "robust"):
             raise ValueError(f"unknown request kind {req.kind!r}")
@@ -241,8 +324,14 @@ def _solve_on_stream(req: GramRequest, precision: str, device, stream, chunk_cel
         sx = sy = None
         if req.kind == "robust":
             rk = _k.RobustSigPDE(lin, req.order, precision=precision)
-            sx = rk.normalization(x)
-            sy = sx if y is None else rk.normalization(y)
+
+            def scales(operand, dev_paths):
+                if _resident(operand) and use_store:
+                    return operand.scales(rk, req.order, precision, stream)
+                return rk.normalization(dev_paths)
+
+            sx = scales(req.x, x)
+            sy = sx if y is None else scales(req.y, y)
         cells = request_cells(req)
         rows = x.shape[0]
         if chunk_cells > 0 and cells > chunk_cells and rows > 1:
@@ -316,6 +405,8 @@ class GramServer:
         # allocating page-locked memory per request (cudaHostAlloc) can stall behind work in flight
         self._staging = {id(st): None for st in self._streams}
         self._used = 0
+        self._store = {}       # name -> PathSet resident on the device
+        self._store_bytes = 0  # held by the store, outside the requests' share of the budget
         self._stop = threading.Event()
         self._ids = 0
         self._lock = threading.Lock()
@@ -339,6 +430,41 @@ class GramServer:
             h.cost = 0
         self._q.put(h)
         return h
+
+    def put(self, name, paths) -> PathSet:
+        """Keep `paths` ((N, L, d) float32/float64) resident on the server's device
+        under `name` and return the PathSet that requests can name as x or y.
+        The store's bytes come out of the HBM budget the requests share."""
+        t = torch.as_tensor(paths)
+        if t.dim() != 3:
+            raise ValueError("paths must be (N, L, d)")
+        nbytes = t.numel() * t.element_size()
+        with self._lock:
+            if name in self._store:
+                raise KeyError(f"a path set named {name!r} is already stored")
+            if self._store_bytes + nbytes > self.budget:
+                raise MemoryError(f"storing {nbytes} bytes would exceed the budget of {self.budget}")
+            self._store_bytes += nbytes
+        host = t.detach().to("cpu").pin_memory()
+        with torch.cuda.device(self.device):
+            dev = host.to(self.device)
+            torch.cuda.synchronize(self.device)  # resident before any request stream reads it
+        ps = PathSet(name, dev, host)
+        with self._lock:
+            self._store[name] = ps
+        return ps
+
+    def drop(self, name):
+        """Release a stored path set (requests in flight keep their references until they finish)."""
+        with self._lock:
+            ps = self._store.pop(name)
+            self._store_bytes -= ps.nbytes
+
+    def store_stats(self):
+        """Per stored set: bytes and hits / misses of its cached normalisation scales."""
+        with self._lock:
+            return {n: {"bytes": p.nbytes, "scale_hits": p.lam_hits, "scale_misses": p.lam_misses}
+                    for n, p in self._store.items()}
 
     def close(self, wait: bool = True):
         self._stop.set()
@@ -381,11 +507,12 @@ class GramServer:
                 continue
             group.append(h)
             pairs += p
+        budget = self.budget - self._store_bytes
         need = batch_footprint_bytes([h.req for h in group], self.precision)
-        while len(group) > 1 and need > self.budget:
+        while len(group) > 1 and need > budget:
             group.pop()
             need = batch_footprint_bytes([h.req for h in group], self.precision)
-        if len(group) == 1 or self._used + need > self.budget:
+        if len(group) == 1 or self._used + need > budget:
             return False
         for h in group:
             self._pending.remove(h)
@@ -422,11 +549,12 @@ class GramServer:
                 self._pending.remove(h)
                 h._finish(error=e)
                 continue
-            if need > self.budget:
+            budget = self.budget - self._store_bytes
+            if need > budget:
                 self._pending.remove(h)
-                h._finish(error=MemoryError(f"request {h.req.rid} needs {need} bytes, budget is {self.budget}"))
+                h._finish(error=MemoryError(f"request {h.req.rid} needs {need} bytes, budget is {budget}"))
                 continue
-            if self._used + need > self.budget:
+            if self._used + need > budget:
                 return  # wait for memory to free up
             self._pending.remove(h)
             stream = self._free_streams.pop()
@@ -494,7 +622,9 @@ class GramServer:
 def serve_sequential(requests, precision: str = "fp64", device="cuda", arrivals=None):
     """The per-request plain-launch baseline: each request alone (copy in,
     solve, copy out, synchronise), in arrival order, starting no earlier than
-    its arrival.  Returns a list of RequestHandle."""
+    its arrival; PathSet operands are copied in from their host copies and
+    their scales recomputed, as a plain call would.  Returns a list of
+    RequestHandle."""
     device = torch.device(device)
     stream = torch.cuda.Stream(device)
     handles = []
@@ -510,7 +640,7 @@ def serve_sequential(requests, precision: str = "fp64", device="cuda", arrivals=
         h = RequestHandle(req)
         h.t_admit = time.perf_counter()
         try:
-            host, _ = _solve_on_stream(req, precision, device, stream)
+            host, _ = _solve_on_stream(req, precision, device, stream, use_store=False)
             stream.synchronize()
             h._finish(result=host)
         except Exception as e:

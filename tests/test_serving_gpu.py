@@ -141,3 +141,62 @@ def test_sequential_baseline_gives_the_same_results(oracle):
     handles = serve_sequential(reqs)
     for h, r in zip(handles, reqs):
         np.testing.assert_array_equal(h.wait().numpy(), _alone(r).numpy())
+
+
+def test_resident_path_sets(oracle):
+    """Path sets kept on the device (GramServer.put): requests naming them as x or
+    y give bitwise the results of the same paths sent from the host, robust
+    requests on a set compute its scales once per (order, precision) and reuse
+    them (hits counted), the store's bytes come out of the budget and the
+    requests' footprints leave the stored paths out, and the per-request
+    baseline (serve_sequential) recomputes from the host copies."""
+    import sigpde_b200.torch as sig
+    from sigpde_b200.serving import GramRequest, GramServer, footprint_bytes, serve_sequential
+    rng = np.random.default_rng(7)
+    sets = {}
+    for i in range(4):
+        N, L = int(rng.integers(4, 30)), int(rng.integers(10, 60))
+        sc = np.exp(rng.uniform(np.log(0.5), np.log(4.0), N))
+        sets[f"s{i}"] = torch.tensor(oracle.brownian(N, L, 8, 100 + i, scale=sc), dtype=torch.float32)
+    with GramServer(max_inflight=4) as srv:
+        budget0 = srv.budget - srv._store_bytes
+        stored = {k: srv.put(k, v) for k, v in sets.items()}
+        assert srv.budget - srv._store_bytes == budget0 - sum(v.numel() * 4 for v in sets.values())
+        with pytest.raises(KeyError):
+            srv.put("s0", sets["s0"])
+        reqs = []
+        for i in range(24):
+            a = f"s{int(rng.integers(0, 4))}"
+            kind = "robust" if i % 2 == 0 else "gram"
+            o = int(rng.integers(0, 3))
+            y = None
+            if kind == "gram" and i % 4 == 1:
+                b = f"s{int(rng.integers(0, 4))}"
+                y = stored[b]
+            reqs.append(GramRequest(x=stored[a], y=y, order=o, kind=kind))
+        # footprints leave the resident paths out
+        for r in reqs[:4]:
+            host_req = GramRequest(x=r.x.host, y=None if r.y is None else r.y.host, order=r.order, kind=r.kind)
+            paths = r.x.nbytes + (0 if r.y is None else r.y.nbytes)
+            assert footprint_bytes(host_req) - footprint_bytes(r) == paths
+        handles = [srv.submit(r) for r in reqs]
+        results = [h.wait(timeout=120) for h in handles]
+        stats = srv.store_stats()
+    for r, got in zip(reqs, results):
+        x = r.x.host.cuda()
+        y = None if r.y is None else r.y.host.cuda()
+        if r.kind == "robust":
+            want = sig.RobustSigPDE(sig.kernels.LinearKernel(), r.order).gram(x, y).cpu()
+        else:
+            want = sig.SigPDE(sig.kernels.LinearKernel(), r.order).gram(x, y).cpu()
+        np.testing.assert_array_equal(got.numpy(), want.numpy())
+    robust_keys = {(r.x.name, r.order) for r in reqs if r.kind == "robust"}
+    robust_reqs = sum(r.kind == "robust" for r in reqs)
+    hits = sum(v["scale_hits"] for v in stats.values())
+    misses = sum(v["scale_misses"] for v in stats.values())
+    assert hits + misses == robust_reqs
+    assert misses >= len(robust_keys) and hits >= robust_reqs - 2 * len(robust_keys) and hits > 0
+    # the per-request baseline copies the host paths and recomputes: the same results
+    seq = serve_sequential(reqs[:6])
+    for h, got in zip(seq, results[:6]):
+        np.testing.assert_array_equal(h.result.numpy(), got.numpy())
