@@ -137,8 +137,9 @@ def other_workloads(args):
     default Gram's timed region, so that one bench line records them too: the
     robust Gram (robust512), the uneven batch (uneven4096) and the serving trace
     (serve_light, burst arrivals: served stream against per-request plain
-    launches).  Each runner prints its own line; the figures kept here are its
-    times, with 5 timed steps after 3 warm-ups and no CPU baselines."""
+    launches; the median of three runs).  Each runner prints its own line; the
+    figures kept here are its times, with 5 timed steps after 3 warm-ups and no
+    CPU baselines."""
     import argparse
     import contextlib
     import io
@@ -163,8 +164,13 @@ def other_workloads(args):
                                     if k in r}
         r = run(run_ours_ragged, "uneven4096", precision=prec)
         out[f"uneven4096_{prec}"] = {k: r.get(k) for k in ("ms_per_step", "value", "unit", "error") if k in r}
-    r = run(run_serve, "serve_light", precision="tc64", burst=True)
+    # the served stream is a host-side Python loop, so one short run moves with the host's load:
+    # three runs, the one of median ratio reported, all three ratios listed
+    runs = [run(run_serve, "serve_light", precision="tc64", burst=True) for _ in range(3)]
+    ok = [x for x in runs if "error" not in x]
+    r = sorted(ok, key=lambda x: x["throughput_ratio_vs_plain"])[len(ok) // 2] if ok else runs[0]
     out["serve_light_tc64_burst"] = {
+        "runs": 3, "ratios_of_the_runs": [round(x.get("throughput_ratio_vs_plain", float("nan")), 3) for x in runs],
         "served_requests_per_s": r.get("served", {}).get("requests_per_s"),
         "plain_requests_per_s": r.get("per_request_plain_launches", {}).get("requests_per_s"),
         "throughput_ratio_vs_plain": r.get("throughput_ratio_vs_plain"),
