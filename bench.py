@@ -170,7 +170,8 @@ def other_workloads(args):
     ok = [x for x in runs if "error" not in x]
     r = sorted(ok, key=lambda x: x["throughput_ratio_vs_plain"])[len(ok) // 2] if ok else runs[0]
     out["serve_light_tc64_burst"] = {
-        "runs": 3, "ratios_of_the_runs": [round(x.get("throughput_ratio_vs_plain", float("nan")), 3) for x in runs],
+        "runs": 3, "ratios_of_the_runs": [round(x["throughput_ratio_vs_plain"], 3) if "throughput_ratio_vs_plain" in x
+                               else None for x in runs],
         "served_requests_per_s": r.get("served", {}).get("requests_per_s"),
         "plain_requests_per_s": r.get("per_request_plain_launches", {}).get("requests_per_s"),
         "throughput_ratio_vs_plain": r.get("throughput_ratio_vs_plain"),
