@@ -368,7 +368,8 @@ class GramServer:
     """Continuous-batching server (see the module docstring).
 
     hbm_budget_bytes: device memory the in-flight requests may hold together
-    (default: 80% of the free memory at start).  A request larger than the
+    (default: 80% of the memory free at start, counting blocks that the
+    caching allocator holds but does not use).  A request larger than the
     whole budget fails at admission with MemoryError instead of waiting
     forever.
     """
@@ -382,9 +383,20 @@ class GramServer:
             self.device = torch.device("cuda", torch.cuda.current_device())
         self.precision = precision
         self.max_inflight = int(max_inflight)
+        # Start from a clean allocator pool: blocks cached by earlier work in the process (an earlier
+        # server's requests, say) are released, so that this server's requests are not carved out of a
+        # pool shaped by other sizes.  Measured: a second and third server in one process (light trace,
+        # burst) served 764-790 requests/s from the pool the first left, 1151-1610 from a clean one.
+        with torch.cuda.device(self.device):
+            torch.cuda.empty_cache()
         if hbm_budget_bytes is None:
+            # memory this process can use: what the driver has free plus what the caching allocator holds
+            # without using (blocks cached by earlier work, which the driver counts as taken); from the
+            # driver's figure alone, a second server in a process that already served would get only the
+            # scraps the first one left
             free, _ = torch.cuda.mem_get_info(self.device)
-            hbm_budget_bytes = int(0.8 * free)
+            cached = torch.cuda.memory_reserved(self.device) - torch.cuda.memory_allocated(self.device)
+            hbm_budget_bytes = int(0.8 * (free + max(cached, 0)))
         self.budget = int(hbm_budget_bytes)
         self.poll = poll_interval_s
         self.chunk_cells = int(chunk_cells)

@@ -200,3 +200,21 @@ def test_resident_path_sets(oracle):
     seq = serve_sequential(reqs[:6])
     for h, got in zip(seq, results[:6]):
         np.testing.assert_array_equal(h.result.numpy(), got.numpy())
+
+
+def test_default_budget_counts_the_allocator_cache():
+    """Memory the caching allocator holds without using (left by earlier work in
+    the process) is usable by a new server: its default budget must not shrink
+    by it (a second server in a process that already served once used to get
+    only the scraps, and refused ordinary requests)."""
+    import gc
+    from sigpde_b200.serving import GramServer
+    gc.collect()
+    torch.cuda.empty_cache()
+    with GramServer(max_inflight=2) as srv:
+        b0 = srv.budget
+    block = torch.empty(4 << 30, dtype=torch.uint8, device="cuda")
+    del block  # cached by the allocator, free for this process
+    with GramServer(max_inflight=2) as srv:
+        b1 = srv.budget
+    assert b1 > b0 - (256 << 20), (b0, b1)
