@@ -109,10 +109,11 @@ class PathSet:
         key = (int(order), precision)
         with self._lock:
             hit = self._lam.get(key)
+            if hit is not None:
+                self.lam_hits += 1
         if hit is not None:
             lam, ev = hit
             stream.wait_event(ev)
-            self.lam_hits += 1
             return lam
         lam = rk.normalization(self.tensor)
         ev = torch.cuda.Event()
