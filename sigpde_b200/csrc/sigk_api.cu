@@ -333,14 +333,20 @@ struct TcPlan {
     size_t err_off, a_off, b_off, ct_off, ws_bytes;
 };
 
-size_t tc_chunk_cap()
+// Float matrices read by half-warp pipelines at order 1 (at most 128 refined rows) run faster in
+// chunks of at most 1 GiB: RobustSigPDE.gram N=512, L=64, d=16, tc64 2.23 -> 2.04 ms; a 512 x 512
+// order-1 Gram 3.64 -> 3.33 ms (tc32 symmetric 1.93 -> 1.73 ms).  Orders 0 and 2 and float64
+// matrices measured slower with small chunks, so they keep kTcChunkBytes.
+constexpr size_t kTcChunkBytesHalfWarpO1 = size_t(1) << 30;
+
+size_t tc_chunk_cap(bool half_warp_order1 = false)
 {
     const char *v = getenv("SIGK_TC_CHUNK_MB");
     if (v && v[0]) {
         long long mb = atoll(v);
         if (mb > 0) return (size_t)mb << 20;
     }
-    return kTcChunkBytes;
+    return half_warp_order1 ? kTcChunkBytesHalfWarpO1 : kTcChunkBytes;
 }
 
 TcPlan make_tc_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, int64_t d, int order, size_t tsize)
@@ -365,7 +371,7 @@ TcPlan make_tc_plan(int op, int64_t nx, int64_t ny, int64_t ncx, int64_t ncy, in
     t.rows_y = ncy;
     const int64_t width = op == kOpPairwise ? ncy : (op == kOpGram ? ny : nx) * ncy; // matrix rows per x path
     const size_t per_x = (size_t)t.rows_x * (size_t)width * sizeof(float);
-    int64_t chunk = (int64_t)(tc_chunk_cap() / per_x);
+    int64_t chunk = (int64_t)(tc_chunk_cap(order == 1 && n <= 128) / per_x);
     if (chunk < 1) chunk = 1;
     if (chunk > nx) chunk = nx;
     t.chunk = chunk;
