@@ -195,14 +195,15 @@ def test_route_choices_by_workspace(built_lib, monkeypatch):
     1 keeps the two-phase matrix unless SIGK_FUSED_TC=1.  An fp64 Gram of d >= 16 writes the
     float64 increment matrix, except at order 2-3 when the lanes' dx tile fits
     registers (then it needs only the path differences, as with
-    SIGK_NO_DGEMM_INC=1); its symmetric Gram keeps the matrix."""
+    SIGK_NO_DGEMM_INC=1); its symmetric Gram keeps the matrix.  Float32 matrices
+    read at order 1 by half-warp pipelines are chunked at 1 GiB."""
     from sigpde_b200 import _lib
     lib = _lib.lib()
     G, S, F32 = _lib.SIGK_OP_GRAM, _lib.SIGK_OP_GRAM_SYM, _lib.SIGK_F32
     TC64, FP64 = _lib.SIGK_PREC_TC64, _lib.SIGK_PREC_FP64
 
     def ws(op, nx, ny, lx, ly, d, o, prec, **env):
-        for k in ("SIGK_FUSED_TC", "SIGK_NO_DGEMM_INC"):
+        for k in ("SIGK_FUSED_TC", "SIGK_NO_DGEMM_INC", "SIGK_TC_CHUNK_MB"):
             monkeypatch.delenv(k, raising=False)
         for k, v in env.items():
             monkeypatch.setenv(k, v)
@@ -229,3 +230,10 @@ def test_route_choices_by_workspace(built_lib, monkeypatch):
     assert ws(S, 7, 7, 40, 40, 16, 2, FP64) > ws(S, 7, 7, 40, 40, 16, 2, FP64, SIGK_NO_DGEMM_INC="1")
     # fp64, d = 24 (a 32-wide padded tile: too wide for registers) keeps the matrix at order 2
     assert ws(G, 7, 6, 40, 47, 24, 2, FP64) > ws(G, 7, 6, 40, 47, 24, 2, FP64, SIGK_NO_DGEMM_INC="1")
+    # tc64 float32 matrices at order 1 with at most 128 refined rows (half-warp readers): chunks of at
+    # most 1 GiB (the robust workload's 2.08 GB matrix in 3 chunks); a larger SIGK_TC_CHUNK_MB overrides;
+    # order 0 and longer paths keep the 6 GiB cap (one chunk here)
+    c3 = ws(S, 512, 512, 64, 64, 16, 1, TC64)
+    assert c3 < (1 << 30) + (64 << 20) < (2 << 30) < ws(S, 512, 512, 64, 64, 16, 1, TC64, SIGK_TC_CHUNK_MB="6144")
+    assert ws(S, 512, 512, 128, 128, 8, 0, TC64) > 4 << 30
+    assert ws(S, 512, 512, 128, 128, 8, 1, TC64) > 4 << 30
