@@ -1,7 +1,8 @@
 """Host-side logic of the request server (sigpde_b200.serving), without a GPU:
 request cost and footprint accounting, including path sets kept resident by
-the server (their bytes are the store's, not the request's), and the cached
-normalisation scales of a path set (computed once per (order, precision))."""
+the server (their bytes are the store's, not the request's), the cached
+normalisation scales of a path set (computed once per (order, precision)),
+and the admission order (cheapest first, oldest first past the wait limit)."""
 import numpy as np
 import pytest
 import torch
@@ -69,3 +70,41 @@ def test_path_set_scales_are_cached_per_order_and_precision(monkeypatch):
     e = ps.scales(rk, 1, "fp64", s1, use_cache=False)
     assert rk.calls == 4 and e is not a
     assert (ps.lam_hits, ps.lam_misses) == (1, 3)
+
+
+class _Req:
+    def __init__(self, arrival):
+        self.arrival = arrival
+
+
+class _Handle:
+    def __init__(self, name, cost, arrival):
+        self.name = name
+        self.cost = cost
+        self.req = _Req(arrival)
+
+
+class _Queue:
+    def __init__(self, handles, max_wait_s):
+        self._pending = handles
+        self.max_wait_s = max_wait_s
+
+
+def test_admission_order_cheapest_first_with_aging():
+    """The next request admitted is the cheapest waiting one, unless some waited longer than
+    max_wait_s: then the oldest of those (so that large requests are not starved)."""
+    import time
+    from sigpde_b200.serving import GramServer
+    now = time.perf_counter()
+    a, b, c = _Handle("a", 50.0, now - 0.01), _Handle("b", 5.0, now - 0.02), _Handle("c", 20.0, now)
+    assert GramServer._next(_Queue([a, b, c], max_wait_s=10.0)).name == "b"
+    old1, old2 = _Handle("old1", 900.0, now - 30.0), _Handle("old2", 100.0, now - 20.0)
+    assert GramServer._next(_Queue([a, b, old2, old1, c], max_wait_s=10.0)).name == "old1"
+    assert GramServer._next(_Queue([a, b, old2, c], max_wait_s=10.0)).name == "old2"
+
+
+def test_request_pairs_count_the_lower_triangle_of_a_symmetric_gram():
+    from sigpde_b200.serving import GramRequest, request_pairs
+    x, y = _paths(9, 12, 3, 3), _paths(4, 15, 3, 4)
+    assert request_pairs(GramRequest(x=x, y=y, order=1)) == 36
+    assert request_pairs(GramRequest(x=x, order=1)) == 45
