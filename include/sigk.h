@@ -38,9 +38,11 @@
  *                   sigk_pairwise_ragged and normalisation entry points form
  *                   increments on the CUDA cores with the same cell
  *                   precision.  The workspace holds
- *                   the increment matrix: up to 6 GiB per call (the x paths
- *                   are processed in chunks beyond that; SIGK_TC_CHUNK_MB
- *                   sets the chunk size).  Exception: sigk_gram with TC64 at
+ *                   the increment matrix: up to 6 GiB per call (1 GiB at
+ *                   order 1 with at most 128 refined rows, where smaller
+ *                   chunks read faster; the x paths are processed in chunks
+ *                   beyond that; SIGK_TC_CHUNK_MB sets the chunk size).
+ *                   Exception: sigk_gram with TC64 at
  *                   order 2 or 3, x paths of one band and dim <= 8 (<= 32 at
  *                   up to 2 coarse rows a lane) runs one fused kernel that
  *                   hands the increments from TMEM through shared memory to
